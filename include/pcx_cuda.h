@@ -1,0 +1,140 @@
+/*
+ * pcx_cuda.h — C ABI of the B200 (sm_100a) FFT / correlation library
+ * (libpcx_cuda.so).  Plain pointers and sizes only; every call returns an
+ * int status (PCX_OK = 0) and pcx_last_error() gives the message of the last
+ * failing call on the calling thread.
+ *
+ * Data layout everywhere: packed split-complex at pack width P (a power of
+ * two): per pack of P elements, P reals then P imaginaries — the layout of
+ * pcxo::vector<T, P> (reference vector.hpp:26-382, element access
+ * element_access.hpp:8-11).  P = 1 is interleaved complex
+ * (std::vector<std::complex<T>>, reference types.hpp:119-148).
+ * Pointers passed to exec calls are DEVICE pointers (or managed memory),
+ * 16-byte aligned; strides count reals (T) between consecutive rows.
+ *
+ * The reference (Dooez/packed) is a header-only C++ template library with no
+ * FFI of its own; each entry point below names the reference interface whose
+ * behaviour it carries.  include/pcxo/*.hpp wraps these calls in the
+ * reference's own class templates.
+ */
+#ifndef PCX_CUDA_H
+#define PCX_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PCX_OK 0
+#define PCX_ERR_INVALID 1      /* std::invalid_argument in the reference      */
+#define PCX_ERR_CUDA 2         /* CUDA runtime failure                        */
+#define PCX_ERR_UNSUPPORTED 3  /* valid in the reference, not built here      */
+#define PCX_ERR_TIMEOUT 4      /* a bounded device wait gave up               */
+
+/* element types */
+#define PCX_F32 0
+#define PCX_F64 1
+
+/* output / input orders — reference fft_order, fft.hpp:540-544 */
+#define PCX_ORDER_NORMAL 0
+#define PCX_ORDER_BIT_REVERSED 1
+#define PCX_ORDER_UNORDERED 2
+
+/* directions */
+#define PCX_FORWARD 0
+#define PCX_INVERSE 1
+
+typedef struct pcx_plan_s*   pcx_plan;
+typedef struct pcx_fxcorr_s* pcx_fxcorr;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* pcx_last_error(void);
+
+/* Library version string. */
+const char* pcx_version(void);
+
+/*
+ * FFT plan.  Replaces the constructor fft_unit<T, Order>(fft_size, sub_size)
+ * (reference fft.hpp:594-605; size checks check_size 1806-1812 and
+ * check_sub_size 1814-1826, twiddle/sort tables get_twiddles 1969-2050).
+ * n: power of two, 2 <= n <= 2^20.  sub_size: power of two >= 8 (validated as
+ * the reference does; on the GPU it is a hint only).  Twiddles are generated
+ * on the device in FP64 and rounded once to `dtype`.
+ */
+int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, size_t sub_size);
+int pcx_plan_destroy(pcx_plan plan);
+/* fft_unit::size() (fft.hpp:615-617). */
+size_t pcx_plan_size(pcx_plan plan);
+/* Bytes of scratch an exec of this plan uses for `batch` rows (0 for n <= 4096). */
+size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
+
+/*
+ * Batched transform of `batch` rows.  Replaces
+ *   fft_unit::fft_raw<PD,PS>(dest, src[, src_size])     fft.hpp:624-681
+ *   fft_unit::ifft_raw<Norm,PD,PS>(dest, src)           fft.hpp:689-721
+ *   fft_unit::operator()(vec) / operator()(dest, src)   fft.hpp:728-820
+ *   fft_unit::ifft<Norm>(vec) / ifft<Norm>(dest, src)   fft.hpp:828-915
+ * dst == src is the in-place form.  src_len (<= n) source elements per row
+ * are read and the rest taken as zero (fft.hpp:671-681); src_len = 0 means n.
+ * Forward output / inverse input follow the plan's order.  normalize scales
+ * the inverse by 1/n.  The out-of-place inverse computes the mathematically
+ * correct inverse for every order (the reference's differs, fft.hpp:863-915).
+ * stream: a cudaStream_t (NULL = legacy default stream).
+ * Uses the plan's own scratch for n > 4096: concurrent execs of one plan on
+ * different streams must use pcx_fft_exec_ws with separate workspaces.
+ */
+int pcx_fft_exec(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
+                 int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,
+                 void* stream);
+
+/* As pcx_fft_exec with caller-provided scratch (>= pcx_plan_workspace_size). */
+int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
+                    int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Adjoint (vector-Jacobian product) of pcx_fft_exec with the same arguments:
+ * given the cotangent g_out of the transform's output, writes the cotangent
+ * of its input.  The forward DFT's adjoint is the unnormalised inverse read
+ * in the plan's order; the inverse's adjoint is the forward scaled as the
+ * inverse was.  No reference counterpart (the reference has no derivatives).
+ */
+int pcx_fft_vjp(pcx_plan plan, void* g_in, const void* g_out, int pack, int direction, int normalize,
+                size_t batch, size_t stride, void* stream);
+
+/*
+ * Overlap-save cross-correlation.  Replaces fxcorr_unit<T>(g, fft_size)
+ * (reference fxcorr.hpp:62-92): g is a DEVICE pointer to k elements at pack
+ * width pack_g; kernel spectrum K = FFT(g zero-padded to n_fft) / n_fft is
+ * computed on the device.  Requires k <= n_fft - pack + 1 so that step > 0.
+ */
+int pcx_fxcorr_create(pcx_fxcorr* h, const void* g, size_t k, int pack_g, size_t n_fft, int dtype);
+int pcx_fxcorr_destroy(pcx_fxcorr h);
+
+/*
+ * y[n] = sum_{j<k} x[n+j] * conj(g[j]) (x zero past its end) for `channels`
+ * rows of `len` elements at pack width `pack`.  Replaces
+ * fxcorr_unit::operator()(vec) (fxcorr.hpp:102-136, block loop with the
+ * block offset taken as a packed element index) and the empty out-of-place
+ * operator()(dest, src) (fxcorr.hpp:138-140).  dst == src is in place.
+ */
+int pcx_fxcorr_exec(pcx_fxcorr h, void* dst, const void* src, size_t len, int pack, size_t channels,
+                    size_t dst_stride, size_t src_stride, void* stream);
+
+/*
+ * Adjoint of pcx_fxcorr_exec: given gy (cotangent of y), writes gx
+ * (cotangent of x: convolution of gy with g) and, if gg != NULL, accumulates
+ * the cotangent of g over all channels into gg (k elements at pack width
+ * pack_g, overwritten): correlation of gy with x.  x is the forward input.
+ * Cotangents of complex values follow d/dRe + i d/dIm.
+ */
+int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, const void* x, size_t len, int pack,
+                   size_t channels, size_t stride, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCX_CUDA_H */

@@ -1,0 +1,466 @@
+// Host side of the FFT: plans (twiddle tables generated on the device in
+// FP64), the launch schedule for the single-pass and four-step paths, and the
+// FFT entry points of the C ABI (include/pcx_cuda.h).
+#include "pcx_fft_kernels.cuh"
+#include "pcx_host.hpp"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+namespace pcxg {
+
+// ---------------------------------------------------------------- twiddles
+template<class T>
+__global__ void k_twiddles(cpx<T>* out, int count, int log_n, long long mult) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long e = ((long long)i * mult) & ((1LL << log_n) - 1);
+    double          s, c;
+    // exp(-2 pi i e / N): the argument 2e/N is exact, sincospi reduces it exactly.
+    sincospi(2.0 * (double)e / (double)(1LL << log_n), &s, &c);
+    out[i] = {T(c), T(-s)};
+}
+
+template<class T>
+static cudaError_t gen_twiddles(void* out, int count, int log_n, long long mult, cudaStream_t st) {
+    k_twiddles<T><<<(count + 255) / 256, 256, 0, st>>>(reinterpret_cast<cpx<T>*>(out), count, log_n, mult);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------- launch selection
+constexpr int SINGLE_NT = 256;
+
+template<class T>
+struct kcfg {
+    // elements per four-step tile: 64 KB of complex data
+    static constexpr int TILE = 65536 / (int)sizeof(cpx<T>);
+    static constexpr int NT   = TILE / 16;
+    static constexpr int CMIN = 64 / (2 * (int)sizeof(T));    // one 64-byte row segment
+};
+
+template<class T, int LOGL>
+static cudaError_t launch_single(const io_args& a, const void* tw, cudaStream_t st, bool set_attr) {
+    constexpr int M     = SINGLE_NT / splan<LOGL>::TT;
+    constexpr int bytes = single_smem_bytes<T, LOGL, SINGLE_NT>();
+    auto          kern  = k_single<T, LOGL, SINGLE_NT>;
+    if (set_attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    if (a.batch == 0) return cudaSuccess;
+    const long long grid = (a.batch + M - 1) / M;
+    kern<<<(unsigned)grid, SINGLE_NT, bytes, st>>>(a, reinterpret_cast<const cpx<T>*>(tw));
+    return cudaGetLastError();
+}
+
+template<class T>
+static cudaError_t dispatch_single(int log_n, const io_args& a, const void* tw, cudaStream_t st, bool set_attr) {
+    switch (log_n) {
+    case 1: return launch_single<T, 1>(a, tw, st, set_attr);
+    case 2: return launch_single<T, 2>(a, tw, st, set_attr);
+    case 3: return launch_single<T, 3>(a, tw, st, set_attr);
+    case 4: return launch_single<T, 4>(a, tw, st, set_attr);
+    case 5: return launch_single<T, 5>(a, tw, st, set_attr);
+    case 6: return launch_single<T, 6>(a, tw, st, set_attr);
+    case 7: return launch_single<T, 7>(a, tw, st, set_attr);
+    case 8: return launch_single<T, 8>(a, tw, st, set_attr);
+    case 9: return launch_single<T, 9>(a, tw, st, set_attr);
+    case 10: return launch_single<T, 10>(a, tw, st, set_attr);
+    case 11: return launch_single<T, 11>(a, tw, st, set_attr);
+    case 12: return launch_single<T, 12>(a, tw, st, set_attr);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template<class T, int LOGL>
+static cudaError_t launch_col(const pass_args& a, long long rows, const void* tw, cudaStream_t st, bool set_attr) {
+    constexpr int C  = std::max(kcfg<T>::CMIN, kcfg<T>::TILE >> LOGL);
+    constexpr int NT = C * splan<LOGL>::TT;
+    static_assert(NT == kcfg<T>::NT || C == kcfg<T>::CMIN, "tile shape");
+    constexpr int xb    = xch_interleaved<(1 << LOGL), C>::size * (int)sizeof(cpx<T>);
+    constexpr int rb    = (1 << LOGL) * 2 * C * (int)sizeof(T);
+    constexpr int bytes = xb > rb ? xb : rb;
+    auto          kern  = k_colpass<T, LOGL, C, NT>;
+    if (set_attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    if (rows == 0) return cudaSuccess;
+    pass_args b     = a;
+    b.tiles_per_row = (1 << a.log_n2) / C;
+    kern<<<(unsigned)(rows * b.tiles_per_row), NT, bytes, st>>>(b, reinterpret_cast<const cpx<T>*>(tw));
+    return cudaGetLastError();
+}
+
+template<class T, int LOGL>
+static cudaError_t launch_row(const pass_args& a, long long rows, const void* tw, cudaStream_t st, bool set_attr) {
+    constexpr int CR    = std::max(kcfg<T>::CMIN, kcfg<T>::TILE >> LOGL);
+    constexpr int NT    = CR * splan<LOGL>::TT;
+    constexpr int xb    = xch_blocked<(1 << LOGL), CR>::size * (int)sizeof(cpx<T>);
+    constexpr int rb    = CR * 2 * (1 << LOGL) * (int)sizeof(T);
+    constexpr int tb    = (1 << LOGL) * (2 * CR + 1) * (int)sizeof(T);
+    constexpr int b1    = xb > rb ? xb : rb;
+    constexpr int bytes = b1 > tb ? b1 : tb;
+    auto          kern  = k_rowpass<T, LOGL, CR, NT>;
+    if (set_attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    if (rows == 0) return cudaSuccess;
+    pass_args b     = a;
+    b.tiles_per_row = (1 << a.log_n1) / CR;
+    kern<<<(unsigned)(rows * b.tiles_per_row), NT, bytes, st>>>(b, reinterpret_cast<const cpx<T>*>(tw));
+    return cudaGetLastError();
+}
+
+template<class T>
+static cudaError_t dispatch_col(int logl, const pass_args& a, long long rows, const void* tw, cudaStream_t st,
+                                bool set_attr) {
+    switch (logl) {
+    case 6: return launch_col<T, 6>(a, rows, tw, st, set_attr);
+    case 7: return launch_col<T, 7>(a, rows, tw, st, set_attr);
+    case 8: return launch_col<T, 8>(a, rows, tw, st, set_attr);
+    case 9: return launch_col<T, 9>(a, rows, tw, st, set_attr);
+    case 10: return launch_col<T, 10>(a, rows, tw, st, set_attr);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template<class T>
+static cudaError_t dispatch_row(int logl, const pass_args& a, long long rows, const void* tw, cudaStream_t st,
+                                bool set_attr) {
+    switch (logl) {
+    case 6: return launch_row<T, 6>(a, rows, tw, st, set_attr);
+    case 7: return launch_row<T, 7>(a, rows, tw, st, set_attr);
+    case 8: return launch_row<T, 8>(a, rows, tw, st, set_attr);
+    case 9: return launch_row<T, 9>(a, rows, tw, st, set_attr);
+    case 10: return launch_row<T, 10>(a, rows, tw, st, set_attr);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}    // namespace pcxg
+
+using namespace pcxg;
+
+// ------------------------------------------------------------------- plans
+static size_t scratch_cap_bytes() {
+    static size_t cap = [] {
+        const char* e = std::getenv("PCX_SCRATCH_MB");
+        long        v = e ? std::atol(e) : 0;
+        return (size_t)(v > 0 ? v : 40) << 20;
+    }();
+    return cap;
+}
+
+size_t pcx_plan_s::chunk_rows(size_t batch) const {
+    if (!two_pass) return 0;
+    const size_t per = n * elem_bytes();
+    size_t       c   = std::max<size_t>(1, scratch_cap_bytes() / per);
+    return std::min(c, std::max<size_t>(batch, 1));
+}
+
+static int plan_init_tables(pcx_plan_s* p) {
+    const int  log_n = p->log_n;
+    const bool f64   = p->dtype == PCX_F64;
+    auto       gen   = [&](void* out, int count, int lg, long long mult) {
+        return f64 ? gen_twiddles<double>(out, count, lg, mult, 0) : gen_twiddles<float>(out, count, lg, mult, 0);
+    };
+    const size_t eb = p->elem_bytes();
+    if (!p->two_pass) {
+        p->tw_bytes = (size_t)p->n * eb;
+        PCX_CUDA_TRY(cudaMalloc(&p->tw, p->tw_bytes));
+        p->twL = p->tw;
+        PCX_CUDA_TRY(gen(p->twL, (int)p->n, log_n, 1));
+        PCX_CUDA_TRY(f64 ? dispatch_single<double>(log_n, io_args{}, nullptr, 0, true)
+                         : dispatch_single<float>(log_n, io_args{}, nullptr, 0, true));
+    } else {
+        const int n1 = 1 << p->log_n1, n2 = 1 << p->log_n2;
+        p->tw_bytes  = (size_t)(n1 + n2 + n2 + n1) * eb;
+        PCX_CUDA_TRY(cudaMalloc(&p->tw, p->tw_bytes));
+        char* base = static_cast<char*>(p->tw);
+        p->twN1    = base;
+        p->twN2    = base + n1 * eb;
+        p->tw_lo   = base + (n1 + n2) * eb;
+        p->tw_hi   = base + (n1 + 2 * n2) * eb;
+        PCX_CUDA_TRY(gen(p->twN1, n1, p->log_n1, 1));
+        PCX_CUDA_TRY(gen(p->twN2, n2, p->log_n2, 1));
+        PCX_CUDA_TRY(gen(p->tw_lo, n2, log_n, 1));
+        PCX_CUDA_TRY(gen(p->tw_hi, n1, log_n, n2));
+        pass_args z{};
+        z.log_n1 = p->log_n1;
+        z.log_n2 = p->log_n2;
+        for (int lg: {p->log_n1, p->log_n2}) {
+            PCX_CUDA_TRY(f64 ? dispatch_col<double>(lg, z, 0, nullptr, 0, true)
+                             : dispatch_col<float>(lg, z, 0, nullptr, 0, true));
+            PCX_CUDA_TRY(f64 ? dispatch_row<double>(lg, z, 0, nullptr, 0, true)
+                             : dispatch_row<float>(lg, z, 0, nullptr, 0, true));
+        }
+    }
+    PCX_CUDA_TRY(cudaDeviceSynchronize());
+    return PCX_OK;
+}
+
+extern "C" int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, size_t sub_size) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan pointer is null");
+        *plan = nullptr;
+        // reference check_size (fft.hpp:1806-1812)
+        if (n <= 1 || (n & (n - 1)) != 0) {
+            return pcx_fail(PCX_ERR_INVALID, "fft_size (which is " + std::to_string(n) +
+                                                 ") is not a power of two or less than 2");
+        }
+        // reference check_sub_size (fft.hpp:1814-1826)
+        if (sub_size < 8 || (sub_size & (sub_size - 1)) != 0) {
+            return pcx_fail(PCX_ERR_INVALID, "sub_size (which is " + std::to_string(sub_size) +
+                                                 ") is not a power of two or less than 8");
+        }
+        if (dtype != PCX_F32 && dtype != PCX_F64) return pcx_fail(PCX_ERR_INVALID, "unknown dtype");
+        if (order < 0 || order > 2) return pcx_fail(PCX_ERR_INVALID, "unknown fft_order");
+        if (n > (size_t(1) << 20)) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED,
+                            "fft_size (which is " + std::to_string(n) + ") exceeds the largest size built (2^20)");
+        }
+        if (order == PCX_ORDER_UNORDERED && n < 16) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED, "unordered order needs fft_size >= 16");
+        }
+        auto p      = new pcx_plan_s{};
+        p->n        = n;
+        p->dtype    = dtype;
+        p->order    = order;
+        p->sub_size = sub_size;
+        p->log_n    = __builtin_ctzll(n);
+        p->two_pass = p->log_n > 12;
+        p->log_n1   = (p->log_n + 1) / 2;
+        p->log_n2   = p->log_n / 2;
+        cudaGetDevice(&p->device);
+        int rc = plan_init_tables(p);
+        if (rc != PCX_OK) {
+            p->release();
+            delete p;
+            return rc;
+        }
+        *plan = p;
+        return PCX_OK;
+    });
+}
+
+void pcx_plan_s::release() {
+    if (tw) cudaFree(tw);
+    if (scratch) cudaFree(scratch);
+    tw      = nullptr;
+    scratch = nullptr;
+}
+
+extern "C" int pcx_plan_destroy(pcx_plan plan) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return PCX_OK;
+        plan->release();
+        delete plan;
+        return PCX_OK;
+    });
+}
+
+extern "C" size_t pcx_plan_size(pcx_plan plan) { return plan ? plan->n : 0; }
+
+extern "C" size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch) {
+    if (!plan || !plan->two_pass) return 0;
+    return plan->chunk_rows(batch) * plan->n * plan->elem_bytes();
+}
+
+// ------------------------------------------------------------------ exec
+namespace {
+int check_pack(int pack, const char* what) {
+    if (pack < 1 || (pack & (pack - 1)) != 0) {
+        return pcx_fail(PCX_ERR_INVALID, std::string(what) + " pack size (which is " + std::to_string(pack) +
+                                             ") is not a power of two");
+    }
+    return PCX_OK;
+}
+}    // namespace
+
+int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
+                size_t batch, size_t dstride, size_t sstride, void* ws, size_t ws_bytes, cudaStream_t st,
+                double extra_scale) {
+    if (!p) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+    if (int rc = check_pack(pd, "destination")) return rc;
+    if (int rc = check_pack(ps, "source")) return rc;
+    const size_t n = p->n;
+    if (src_len == 0) src_len = n;
+    if (src_len > n) {
+        return pcx_fail(PCX_ERR_INVALID, "source size (which is " + std::to_string(src_len) +
+                                             ") is bigger than fft size (which is " + std::to_string(n) + ")");
+    }
+    if (dir == PCX_INVERSE && src_len != n) {
+        return pcx_fail(PCX_ERR_INVALID, "source size (which is " + std::to_string(src_len) +
+                                             ") is not equal to fft size (which is " + std::to_string(n) + ")");
+    }
+    if (dir != PCX_FORWARD && dir != PCX_INVERSE) return pcx_fail(PCX_ERR_INVALID, "unknown direction");
+    if ((size_t)pd > n || (size_t)ps > n) {
+        return pcx_fail(PCX_ERR_UNSUPPORTED, "pack size larger than fft size is not supported");
+    }
+    const int cmin = p->dtype == PCX_F64 ? kcfg<double>::CMIN : kcfg<float>::CMIN;
+    if (p->two_pass && (pd > cmin || ps > cmin)) {
+        return pcx_fail(PCX_ERR_UNSUPPORTED, "pack sizes above " + std::to_string(cmin) +
+                                                 " are not supported for fft_size > 4096");
+    }
+    if (batch == 0) return PCX_OK;
+    if (!dst || !src) return pcx_fail(PCX_ERR_INVALID, "null data pointer");
+    const size_t vreals = 16 / (p->dtype == PCX_F64 ? sizeof(double) : sizeof(float));
+    if (p->two_pass && batch > 1 && (dstride % vreals != 0 || sstride % vreals != 0)) {
+        return pcx_fail(PCX_ERR_UNSUPPORTED, "row strides must be multiples of 16 bytes for fft_size > 4096");
+    }
+    if ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) % 16 != 0) {
+        return pcx_fail(PCX_ERR_INVALID, "data pointers must be 16-byte aligned");
+    }
+    const size_t row_d = n * 2, row_s = n * 2;
+    if (batch > 1 && (dstride < row_d || sstride < (src_len == n ? row_s : 0))) {
+        return pcx_fail(PCX_ERR_INVALID, "row stride smaller than a row");
+    }
+    const bool   inv   = dir == PCX_INVERSE;
+    const double scale = (inv && norm ? 1.0 / (double)n : 1.0) * extra_scale;
+
+    io_args io{};
+    io.src_stride = (long long)sstride;
+    io.dst_stride = (long long)dstride;
+    io.src_len    = (int)src_len;
+    io.lp_src     = __builtin_ctz(ps);
+    io.lp_dst     = __builtin_ctz(pd);
+    io.order_in   = inv ? p->order : 0;
+    io.order_out  = inv ? 0 : p->order;
+    io.conj_in    = inv;
+    io.conj_out   = inv;
+    io.scale      = scale;
+    const bool f64 = p->dtype == PCX_F64;
+    const size_t eb = p->elem_bytes();
+
+    if (!p->two_pass) {
+        io.src   = src;
+        io.dst   = dst;
+        io.batch = (long long)batch;
+        PCX_CUDA_TRY(f64 ? dispatch_single<double>(p->log_n, io, p->twL, st, false)
+                         : dispatch_single<float>(p->log_n, io, p->twL, st, false));
+        return PCX_OK;
+    }
+
+    // four-step through L2-sized chunks of scratch
+    const size_t chunk = p->chunk_rows(batch);
+    const size_t need  = chunk * n * eb;
+    void*        scr   = ws;
+    if (!scr) {
+        if (p->scratch_bytes < need) {
+            if (p->scratch) cudaFree(p->scratch);
+            p->scratch       = nullptr;
+            p->scratch_bytes = 0;
+            PCX_CUDA_TRY(cudaMalloc(&p->scratch, need));
+            p->scratch_bytes = need;
+        }
+        scr = p->scratch;
+    } else if (ws_bytes < need) {
+        return pcx_fail(PCX_ERR_INVALID, "workspace smaller than pcx_plan_workspace_size");
+    }
+
+    const size_t es = f64 ? sizeof(double) : sizeof(float);
+    for (size_t r0 = 0; r0 < batch; r0 += chunk) {
+        const long long rows = (long long)std::min(chunk, batch - r0);
+        const char*     s    = static_cast<const char*>(src) + r0 * sstride * es;
+        char*           d    = static_cast<char*>(dst) + r0 * dstride * es;
+
+        pass_args a{};
+        a.log_n1 = p->log_n1;
+        a.log_n2 = p->log_n2;
+        a.log_lo = p->log_n2;
+        a.tw_hi  = p->tw_hi;
+        a.tw_lo  = p->tw_lo;
+
+        pass_args b = a;
+        if (!(inv && p->order != 0)) {
+            // pass 1: columns src -> scratch (with twiddle); pass 2: rows scratch -> dst
+            a.io            = io;
+            a.io.src        = s;
+            a.io.dst        = scr;
+            a.io.dst_stride = (long long)(2 * n);
+            a.io.lp_dst     = 0;
+            a.io.conj_out   = 0;
+            a.io.scale      = 1.0;
+            a.io.order_out  = 0;
+            a.twiddle       = 1;
+            b.io            = io;
+            b.io.src        = scr;
+            b.io.src_stride = (long long)(2 * n);
+            b.io.src_len    = (int)n;
+            b.io.lp_src     = 0;
+            b.io.conj_in    = 0;
+            b.io.order_in   = 0;
+            b.io.dst        = d;
+            b.twiddle       = 0;
+            b.transposed_out = io.order_out == 0;
+            b.row_map        = io.order_out != 0;
+            PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, a, rows, p->twN1, st, false)
+                             : dispatch_col<float>(p->log_n1, a, rows, p->twN1, st, false));
+            PCX_CUDA_TRY(f64 ? dispatch_row<double>(p->log_n2, b, rows, p->twN2, st, false)
+                             : dispatch_row<float>(p->log_n2, b, rows, p->twN2, st, false));
+        } else {
+            // inverse from a permuted order: rows first (input rows), then columns
+            a.io             = io;
+            a.io.src         = s;
+            a.io.dst         = scr;
+            a.io.dst_stride  = (long long)(2 * n);
+            a.io.lp_dst      = 0;
+            a.io.conj_out    = 0;
+            a.io.scale       = 1.0;
+            a.io.order_out   = 0;
+            a.twiddle        = 1;
+            a.row_map        = 1;
+            a.transposed_out = 0;
+            b.io             = io;
+            b.io.src         = scr;
+            b.io.src_stride  = (long long)(2 * n);
+            b.io.src_len     = (int)n;
+            b.io.lp_src      = 0;
+            b.io.conj_in     = 0;
+            b.io.order_in    = 0;
+            b.io.dst         = d;
+            b.twiddle        = 0;
+            PCX_CUDA_TRY(f64 ? dispatch_row<double>(p->log_n2, a, rows, p->twN2, st, false)
+                             : dispatch_row<float>(p->log_n2, a, rows, p->twN2, st, false));
+            PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, b, rows, p->twN1, st, false)
+                             : dispatch_col<float>(p->log_n1, b, rows, p->twN1, st, false));
+        }
+    }
+    return PCX_OK;
+}
+
+extern "C" int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst,
+                               int pack_src, int direction, int normalize, size_t batch, size_t dst_stride,
+                               size_t src_stride, void* workspace, size_t workspace_bytes, void* stream) {
+    return pcx_guard([&]() -> int {
+        return pcx_fft_run(plan, dst, src, src_len, pack_dst, pack_src, direction, normalize, batch, dst_stride,
+                           src_stride, workspace, workspace_bytes, static_cast<cudaStream_t>(stream), 1.0);
+    });
+}
+
+extern "C" int pcx_fft_exec(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
+                            int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,
+                            void* stream) {
+    return pcx_fft_exec_ws(plan, dst, src, src_len, pack_dst, pack_src, direction, normalize, batch, dst_stride,
+                           src_stride, nullptr, 0, stream);
+}
+
+// Adjoint: y = F x  =>  x_bar = F^H y_bar, the unnormalised inverse read in
+// the plan's order.  y = s * F^H x  =>  x_bar = s * F y_bar.
+extern "C" int pcx_fft_vjp(pcx_plan plan, void* g_in, const void* g_out, int pack, int direction, int normalize,
+                           size_t batch, size_t stride, void* stream) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (direction == PCX_FORWARD) {
+            return pcx_fft_run(plan, g_in, g_out, 0, pack, pack, PCX_INVERSE, 0, batch, stride, stride, nullptr, 0,
+                               st, 1.0);
+        }
+        const double s = normalize ? 1.0 / (double)plan->n : 1.0;
+        return pcx_fft_run(plan, g_in, g_out, 0, pack, pack, PCX_FORWARD, 0, batch, stride, stride, nullptr, 0, st,
+                           s);
+    });
+}

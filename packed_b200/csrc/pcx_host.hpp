@@ -1,0 +1,63 @@
+// Host-side state and error plumbing shared by the C ABI translation units.
+#pragma once
+
+#include "../../include/pcx_cuda.h"
+
+#include <cuda_runtime.h>
+#include <exception>
+#include <string>
+
+// Record `msg` as this thread's last error and return `code`.
+int pcx_fail(int code, const std::string& msg);
+
+// Run `f`, turning C++ exceptions into PCX_ERR_INVALID (no exception crosses the C ABI).
+template<class F>
+int pcx_guard(F&& f) {
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        return pcx_fail(PCX_ERR_INVALID, e.what());
+    } catch (...) {
+        return pcx_fail(PCX_ERR_INVALID, "unknown exception");
+    }
+}
+
+#define PCX_CUDA_TRY(expr)                                                                       \
+    do {                                                                                         \
+        cudaError_t pcx_e_ = (expr);                                                             \
+        if (pcx_e_ != cudaSuccess) {                                                             \
+            return pcx_fail(PCX_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(pcx_e_)); \
+        }                                                                                        \
+    } while (0)
+
+struct pcx_plan_s {
+    size_t n        = 0;
+    int    dtype    = PCX_F32;
+    int    order    = PCX_ORDER_NORMAL;
+    size_t sub_size = 2048;
+    int    log_n    = 0;
+    int    two_pass = 0;
+    int    log_n1   = 0;
+    int    log_n2   = 0;
+    int    device   = 0;
+
+    void*  tw       = nullptr;    // one allocation holding every table below
+    size_t tw_bytes = 0;
+    void*  twL      = nullptr;    // W_N^i, single-pass
+    void*  twN1     = nullptr;    // W_N1^i
+    void*  twN2     = nullptr;    // W_N2^i
+    void*  tw_lo    = nullptr;    // W_N^i, i < N2
+    void*  tw_hi    = nullptr;    // W_N^(i*N2), i < N1
+
+    void*  scratch       = nullptr;    // four-step intermediate (plan-owned)
+    size_t scratch_bytes = 0;
+
+    size_t elem_bytes() const { return dtype == PCX_F64 ? 16 : 8; }
+    size_t chunk_rows(size_t batch) const;
+    void   release();
+};
+
+// Core of pcx_fft_exec (no exception guard); extra_scale multiplies the output.
+int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
+                size_t batch, size_t dstride, size_t sstride, void* ws, size_t ws_bytes, cudaStream_t st,
+                double extra_scale);

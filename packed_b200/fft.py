@@ -1,0 +1,304 @@
+"""Host-side mirror of the reference's FFT API over the CUDA library.
+
+Mirrors ``pcxo::fft_unit`` (reference fft.hpp:565-2166), ``pcxo::vector``
+(vector.hpp:26-382) and ``pcxo::fxcorr_unit`` (fxcorr.hpp:44-147): the same
+constructor arguments, method names, argument meanings and error behaviour
+(``ValueError`` where the reference throws ``std::invalid_argument``, with the
+same messages).  Data live in device memory as torch tensors holding the
+packed split-complex reals; every transform runs in libpcx_cuda.so.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+import torch
+
+from . import _lib
+
+__all__ = ["fft_order", "default_pack_size", "vector", "fft_unit", "fxcorr_unit", "real_size"]
+
+
+class fft_order(enum.IntEnum):
+    """reference fft.hpp:540-544"""
+    normal = 0
+    bit_reversed = 1
+    unordered = 2
+
+
+def default_pack_size(dtype: torch.dtype) -> int:
+    """32 bytes of reals per pack (reference types.hpp:70-72)."""
+    return 32 // torch.empty((), dtype=dtype).element_size()
+
+
+def real_size(n: int, pack: int) -> int:
+    """reals needed for n elements at pack width `pack` (vector.hpp:373-381)."""
+    return (n + pack - 1) // pack * 2 * pack
+
+
+def _dtype_code(dtype: torch.dtype) -> int:
+    if dtype == torch.float32:
+        return _lib.PCX_F32
+    if dtype == torch.float64:
+        return _lib.PCX_F64
+    raise TypeError(f"unsupported real type {dtype}")
+
+
+def _stream_ptr(stream) -> ctypes.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class vector:
+    """Packed split-complex vector in device memory (pcxo::vector<T, P>).
+
+    ``data`` is a 1-D torch tensor of ``real_size(size, pack)`` reals; element i
+    has its real part at ``i + (i // P) * P`` and imaginary part ``P`` further.
+    """
+
+    def __init__(self, size: int, dtype: torch.dtype = torch.float32, pack: int | None = None,
+                 device: str | torch.device = "cuda", data: torch.Tensor | None = None):
+        self.pack_size = pack or default_pack_size(dtype)
+        if self.pack_size <= 0 or self.pack_size & (self.pack_size - 1):
+            raise ValueError("pack size must be a power of two")
+        self._size = int(size)
+        if data is None:
+            data = torch.zeros(real_size(self._size, self.pack_size), dtype=dtype, device=device)
+        self.data = data
+
+    @classmethod
+    def from_complex(cls, z, dtype: torch.dtype = torch.float32, pack: int | None = None, device="cuda"):
+        z = np.asarray(z)
+        p = pack or default_pack_size(dtype)
+        n = z.shape[-1]
+        npk = (n + p - 1) // p
+        zz = np.zeros(npk * p, dtype=np.complex128)
+        zz[:n] = z
+        zz = zz.reshape(npk, p)
+        host = np.stack([zz.real, zz.imag], axis=1).reshape(-1)
+        t = torch.as_tensor(host, dtype=dtype).to(device)
+        return cls(n, dtype, p, device, t)
+
+    def to_complex(self) -> np.ndarray:
+        p = self.pack_size
+        a = self.data.detach().cpu().numpy().astype(np.float64).reshape(-1, 2, p)
+        return (a[:, 0, :] + 1j * a[:, 1, :]).reshape(-1)[: self._size]
+
+    def size(self) -> int:
+        return self._size
+
+    def __len__(self) -> int:
+        return self._size
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.data.dtype
+
+    def __getitem__(self, i: int) -> complex:
+        if not 0 <= i < self._size:
+            raise IndexError("pcxo::vector index out of range")
+        p = self.pack_size
+        o = i + (i // p) * p
+        return complex(float(self.data[o]), float(self.data[o + p]))
+
+
+def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
+    if not t.is_cuda:
+        raise ValueError("data must reside in CUDA device memory")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class fft_unit:
+    """Plan of a power-of-two complex FFT (reference fft.hpp:565-2166).
+
+    ``fft_unit(fft_size, sub_size=2048, dtype=torch.float32, order=fft_order.normal)``
+    """
+
+    def __init__(self, fft_size: int, sub_size: int = 2048, dtype: torch.dtype = torch.float32,
+                 order: fft_order = fft_order.normal):
+        self._dtype = dtype
+        self._order = fft_order(order)
+        self._plan = ctypes.c_void_p()
+        L = _lib.lib()
+        _lib.check(L.pcx_plan_create(ctypes.byref(self._plan), int(fft_size), _dtype_code(dtype), int(self._order),
+                                     int(sub_size)))
+        self._n = int(fft_size)
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                _lib.lib().pcx_plan_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    def __copy__(self):
+        raise TypeError("fft_unit is not assignable (reference fft.hpp:611-612)")
+
+    # ---------------------------------------------------------------- info
+    def size(self) -> int:
+        return self._n
+
+    @property
+    def order(self) -> fft_order:
+        return self._order
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self._dtype
+
+    def workspace_size(self, batch: int = 1) -> int:
+        return int(_lib.lib().pcx_plan_workspace_size(self._plan, batch))
+
+    # ---------------------------------------------------------- raw calls
+    def exec(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
+             batch: int = 1, pack_dst: int | None = None, pack_src: int | None = None, src_len: int = 0,
+             dst_stride: int | None = None, src_stride: int | None = None, stream=None,
+             workspace: torch.Tensor | None = None) -> None:
+        """Batched transform of `batch` rows of packed reals (pcx_fft_exec)."""
+        pd = pack_dst or default_pack_size(self._dtype)
+        ps = pack_src or pd
+        if dst.dtype != self._dtype or src.dtype != self._dtype:
+            raise TypeError("data type does not match the fft_unit")
+        ds = dst_stride if dst_stride is not None else real_size(self._n, pd)
+        ss = src_stride if src_stride is not None else real_size(self._n, ps)
+        L = _lib.lib()
+        if workspace is None:
+            rc = L.pcx_fft_exec(self._plan, _ptr(dst), _ptr(src), src_len, pd, ps, direction, int(normalize), batch,
+                                ds, ss, _stream_ptr(stream))
+        else:
+            rc = L.pcx_fft_exec_ws(self._plan, _ptr(dst), _ptr(src), src_len, pd, ps, direction, int(normalize),
+                                   batch, ds, ss, _ptr(workspace), workspace.numel() * workspace.element_size(),
+                                   _stream_ptr(stream))
+        _lib.check(rc)
+
+    def fft_raw(self, dest: torch.Tensor, source: torch.Tensor | None = None, source_size: int | None = None,
+                pack_dest: int = 1, pack_src: int = 1) -> None:
+        """fft_raw<PD,PS>(dest[, source[, source_size]]) (fft.hpp:624-681)."""
+        src = dest if source is None else source
+        self.exec(dest, src, direction=0, pack_dst=pack_dest, pack_src=pack_src, src_len=source_size or 0)
+
+    def ifft_raw(self, dest: torch.Tensor, source: torch.Tensor | None = None, normalized: bool = True,
+                 pack_dest: int = 1, pack_src: int = 1) -> None:
+        """ifft_raw<Normalized,PD,PS>(dest[, source]) (fft.hpp:689-721)."""
+        src = dest if source is None else source
+        self.exec(dest, src, direction=1, normalize=normalized, pack_dst=pack_dest, pack_src=pack_src)
+
+    # ------------------------------------------------------ vector calls
+    def __call__(self, dest: vector, source: vector | None = None) -> None:
+        """operator()(vector) in place, or operator()(dest, source) (fft.hpp:728-820)."""
+        if source is None:
+            if dest.size() != self._n:
+                raise ValueError(f"input size (which is {dest.size()}) is not equal to fft size (which is "
+                                 f"{self._n})")
+            self.exec(dest.data, dest.data, direction=0, pack_dst=dest.pack_size, pack_src=dest.pack_size)
+            return
+        if dest.size() != self._n:
+            raise ValueError(f"destination size (which is {dest.size()}) is not equal to fft size (which is "
+                             f"{self._n})")
+        if source.size() > self._n:
+            raise ValueError(f"source size (which is {source.size()}) is bigger than fft size (which is "
+                             f"{self._n})")
+        self._check_repack(dest, source)
+        self.exec(dest.data, source.data, direction=0, pack_dst=dest.pack_size, pack_src=source.pack_size,
+                  src_len=source.size())
+
+    def ifft(self, dest: vector, source: vector | None = None, normalized: bool = True) -> None:
+        """ifft<Normalized>(vector) / ifft<Normalized>(dest, source) (fft.hpp:828-915)."""
+        if source is None:
+            if dest.size() != self._n:
+                raise ValueError(f"input size (which is {dest.size()} is not equal to fft size (which is "
+                                 f"{self._n})")
+            self.exec(dest.data, dest.data, direction=1, normalize=normalized, pack_dst=dest.pack_size,
+                      pack_src=dest.pack_size)
+            return
+        if dest.size() != self._n:
+            raise ValueError(f"destination size (which is {dest.size()}) is not equal to fft size (which is "
+                             f"{self._n})")
+        if source.size() != self._n:
+            raise ValueError(f"source size (which is {source.size()}) is not equal to fft size (which is "
+                             f"{self._n})")
+        self._check_repack(dest, source)
+        self.exec(dest.data, source.data, direction=1, normalize=normalized, pack_dst=dest.pack_size,
+                  pack_src=source.pack_size)
+
+    def _check_repack(self, dest: vector, source: vector) -> None:
+        # fft.hpp:783-792 — in-place repack with a pack wider than a register is refused
+        reg = 32 // torch.empty((), dtype=self._dtype).element_size()
+        if (dest.pack_size != source.pack_size and max(dest.pack_size, source.pack_size) > reg
+                and dest.data.data_ptr() == source.data.data_ptr()):
+            raise ValueError(f"cannot perform in-place repack from source pack size (which is {source.pack_size}) "
+                             f"to destination pack size (which is {dest.pack_size})")
+
+    # ------------------------------------------------------------- adjoint
+    def vjp(self, g_out: torch.Tensor, *, direction: int = 0, normalize: bool = True, batch: int = 1,
+            pack: int | None = None, stream=None) -> torch.Tensor:
+        """Cotangent of the input given the cotangent of the output (pcx_fft_vjp)."""
+        p = pack or default_pack_size(self._dtype)
+        g_in = torch.empty_like(g_out)
+        _lib.check(_lib.lib().pcx_fft_vjp(self._plan, _ptr(g_in), _ptr(g_out), p, direction, int(normalize), batch,
+                                          real_size(self._n, p), _stream_ptr(stream)))
+        return g_in
+
+
+class fxcorr_unit:
+    """Overlap-save cross-correlator (reference fxcorr.hpp:44-147).
+
+    ``fxcorr_unit(g, fft_size)``: ``g`` is a :class:`vector` (device) or a
+    complex array-like.  ``unit(x)`` correlates in place; ``unit(dest, src)``
+    out of place (the reference leaves that overload empty, fxcorr.hpp:138-140).
+    """
+
+    def __init__(self, g, fft_size: int, dtype: torch.dtype | None = None):
+        if not isinstance(g, vector):
+            g = vector.from_complex(np.asarray(g), dtype=dtype or torch.float32)
+        self._dtype = g.dtype
+        self._k = g.size()
+        self._n = int(fft_size)
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.lib().pcx_fxcorr_create(ctypes.byref(self._h), _ptr(g.data), self._k, g.pack_size, self._n,
+                                                _dtype_code(self._dtype)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().pcx_fxcorr_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def fft_size(self) -> int:
+        return self._n
+
+    def kernel_size(self) -> int:
+        return self._k
+
+    def exec(self, dst: torch.Tensor, src: torch.Tensor, length: int, *, channels: int = 1, pack: int | None = None,
+             dst_stride: int | None = None, src_stride: int | None = None, stream=None) -> None:
+        p = pack or default_pack_size(self._dtype)
+        rs = real_size(length, p)
+        _lib.check(_lib.lib().pcx_fxcorr_exec(self._h, _ptr(dst), _ptr(src), length, p, channels,
+                                              dst_stride if dst_stride is not None else rs,
+                                              src_stride if src_stride is not None else rs, _stream_ptr(stream)))
+
+    def __call__(self, dest: vector, source: vector | None = None) -> None:
+        if source is None:
+            self.exec(dest.data, dest.data, dest.size(), pack=dest.pack_size)
+            return
+        if dest.size() != source.size() or dest.pack_size != source.pack_size:
+            raise ValueError("destination and source must have the same size and pack size")
+        self.exec(dest.data, source.data, dest.size(), pack=dest.pack_size)
+
+    def vjp(self, gy: torch.Tensor, x: torch.Tensor, length: int, *, channels: int = 1, pack: int | None = None,
+            want_kernel_grad: bool = True, stream=None) -> tuple[torch.Tensor, torch.Tensor | None]:
+        p = pack or default_pack_size(self._dtype)
+        gx = torch.empty_like(gy)
+        gg = torch.empty(real_size(self._k, p), dtype=self._dtype, device=gy.device) if want_kernel_grad else None
+        _lib.check(_lib.lib().pcx_fxcorr_vjp(self._h, _ptr(gx), _ptr(gg) if gg is not None else None, _ptr(gy),
+                                             _ptr(x), length, p, channels, real_size(length, p),
+                                             _stream_ptr(stream)))
+        return gx, gg

@@ -1,0 +1,249 @@
+"""GPU parity of the FFT path (libpcx_cuda.so through its C ABI) against the
+CPU oracle and the reference's golden outputs.  Bar: relative L2 2e-6 (FP32),
+1e-13 (FP64)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from packed_b200 import fft_order, fft_unit, real_size, vector
+from tests._util import TOL, golden, normal_cx, rel_l2, uniform_cx
+
+pytestmark = pytest.mark.gpu
+
+F32, F64 = torch.float32, torch.float64
+NPD = {F32: np.float32, F64: np.float64}
+
+
+def to_dev(a, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).cuda()
+
+
+def run(unit, src_packed, batch, **kw):
+    src = to_dev(src_packed, unit.dtype)
+    dst = torch.empty_like(src) if kw.pop("inplace", False) is False else src
+    unit.exec(dst, src, batch=batch, **kw)
+    torch.cuda.synchronize()
+    return dst.cpu().numpy()
+
+
+def rows_for(n):
+    return max(1, min(6, (1 << 16) // n)) if n <= 4096 else (7 if n >= (1 << 19) else 3)
+
+
+@pytest.mark.parametrize("log_n", list(range(1, 21)))
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_forward_inverse_parity_f32(log_n, order):
+    n = 1 << log_n
+    if order == 2 and n < 16:
+        pytest.skip("unordered defined for n >= 16")
+    rng = np.random.default_rng(100 + log_n)
+    b = rows_for(n)
+    p = min(8, n)
+    z = normal_cx(rng, b, n)
+    x = O.pack(z, p)
+    unit = fft_unit(n, dtype=F32, order=order)
+    got = run(unit, x, b, direction=0, pack_dst=p, pack_src=p)
+    want = O.fft_packed(x, n, order=order, pack_src=p, pack_dst=p)
+    assert rel_l2(O.unpack(got, n, p), O.unpack(want, n, p)) < TOL[np.float32]
+    back = run(unit, want.astype(np.float32), b, direction=1, pack_dst=p, pack_src=p)
+    assert rel_l2(O.unpack(back, n, p), z) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("log_n", [4, 6, 10, 12, 13, 16, 20])
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_parity_f64(log_n, order):
+    n = 1 << log_n
+    rng = np.random.default_rng(200 + log_n)
+    b = 2 if n >= 4096 else 4
+    z = normal_cx(rng, b, n)
+    x = O.pack(z, 4, np.float64)
+    unit = fft_unit(n, dtype=F64, order=order)
+    got = run(unit, x, b, direction=0, pack_dst=4, pack_src=4)
+    want = O.fft_packed(x, n, order=order, pack_src=4, pack_dst=4, dtype=np.float64)
+    assert rel_l2(O.unpack(got, n, 4), O.unpack(want, n, 4)) < TOL[np.float64]
+    back = run(unit, want, b, direction=1, pack_dst=4, pack_src=4)
+    assert rel_l2(O.unpack(back, n, 4), z) < TOL[np.float64]
+
+
+def test_fp64_template_check_c2():
+    # FP64 template check of the size sweep: N=2^12, batch 4096, pack 4, N(0,1) seed 1
+    n, b = 4096, 4096
+    rng = np.random.default_rng(1)
+    z = normal_cx(rng, b, n)
+    x = O.pack(z, 4, np.float64)
+    unit = fft_unit(n, dtype=F64)
+    got = O.unpack(run(unit, x, b, direction=0, pack_dst=4, pack_src=4), n, 4)
+    want = np.fft.fft(z, axis=-1)
+    assert rel_l2(got, want) < TOL[np.float64]
+
+
+@pytest.mark.parametrize("n", [64, 256, 1024, 4096])
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_matches_reference_golden(n, order):
+    G = golden()
+    unit = fft_unit(n, order=order)
+    got = run(unit, G[f"x_{n}"], 1, direction=0)
+    assert rel_l2(O.unpack(got, n, 8), O.unpack(G[f"fwd_{n}_o{order}"], n, 8)) < TOL[np.float32]
+    inv = run(unit, G[f"fwd_{n}_o{order}"], 1, direction=1)
+    assert rel_l2(O.unpack(inv, n, 8), O.unpack(G[f"inv_{n}_o{order}"], n, 8)) < TOL[np.float32]
+    if order:
+        raw = run(unit, G[f"fwd_{n}_o{order}"], 1, direction=1, normalize=False)
+        assert rel_l2(O.unpack(raw, n, 8), O.unpack(G[f"invraw_{n}_o{order}"], n, 8)) < TOL[np.float32]
+
+
+def test_c1_config_against_reference_and_fp64():
+    # N=1024, batch 64, U[-1,1) seed 0; forward then inverse (1/N)
+    G = golden()
+    rng = np.random.default_rng(0)
+    z = np.stack([(rng.uniform(-1, 1, 1024) + 1j * rng.uniform(-1, 1, 1024)).astype(np.complex64)
+                  for _ in range(64)])
+    x = O.pack(z, 8)
+    unit = fft_unit(1024)
+    fwd = run(unit, x, 64, direction=0)
+    inv = run(unit, fwd, 64, direction=1)
+    assert rel_l2(O.unpack(fwd[:4], 1024, 8), O.unpack(G["c1_fwd"], 1024, 8)) < TOL[np.float32]
+    assert rel_l2(O.unpack(inv[:4], 1024, 8), O.unpack(G["c1_inv"], 1024, 8)) < TOL[np.float32]
+    assert rel_l2(O.unpack(fwd, 1024, 8), O.dft(z.astype(np.complex128))) < TOL[np.float32]
+    assert rel_l2(O.unpack(inv, 1024, 8), z) < TOL[np.float32]
+
+
+def test_reference_tone_input():
+    G = golden()
+    got = run(fft_unit(1024), G["tone_x_1024"], 1)
+    assert rel_l2(O.unpack(got, 1024, 8), O.unpack(G["tone_fwd_1024"], 1024, 8)) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("n", [1024, 1 << 14])
+def test_zero_extended_source(n):
+    rng = np.random.default_rng(5)
+    for order in (0, 1, 2):
+        for src_len in (1, 700 * n // 1024, n - 3):
+            z = normal_cx(rng, src_len)
+            src = to_dev(O.pack(z, 8), F32)
+            dst = torch.full((2 * n,), float("nan"), device="cuda")
+            fft_unit(n, order=order).exec(dst, src, src_len=src_len)
+            want = O.fft_packed(O.pack(z, 8), n, order=order, src_len=src_len)
+            assert rel_l2(O.unpack(dst.cpu().numpy(), n, 8), O.unpack(want, n, 8)) < TOL[np.float32]
+    G = golden()
+    got = torch.empty(2048, device="cuda")
+    fft_unit(1024, order=1).exec(got, to_dev(G["zx_src_700"], F32), src_len=700)
+    assert rel_l2(O.unpack(got.cpu().numpy(), 1024, 8), O.unpack(G["zx_fwd_1024_o1"], 1024, 8)) < 2e-6
+
+
+@pytest.mark.parametrize("n", [256, 4096, 1 << 15])
+def test_pack_conversion_and_strides(n):
+    rng = np.random.default_rng(9)
+    b = 3
+    z = normal_cx(rng, b, n)
+    unit = fft_unit(n)
+    want = np.fft.fft(z, axis=-1)
+    for ps, pd in ((1, 8), (8, 1), (2, 4), (4, 4), (8, 8)):
+        pad_s, pad_d = 16, 48
+        rs, rd = real_size(n, ps) + pad_s, real_size(n, pd) + pad_d
+        src = np.zeros((b, rs), np.float32)
+        src[:, : real_size(n, ps)] = O.pack(z, ps)
+        s = to_dev(src, F32)
+        d = torch.zeros((b, rd), device="cuda")
+        unit.exec(d, s, batch=b, pack_src=ps, pack_dst=pd, src_stride=rs, dst_stride=rd)
+        out = d.cpu().numpy()
+        assert rel_l2(O.unpack(out[:, : real_size(n, pd)], n, pd), want) < TOL[np.float32]
+        assert np.all(out[:, real_size(n, pd):] == 0), "wrote outside the rows"
+
+
+@pytest.mark.parametrize("n", [64, 4096, 1 << 17])
+def test_in_place(n):
+    rng = np.random.default_rng(11)
+    z = normal_cx(rng, 2, n)
+    x = to_dev(O.pack(z, 8), F32)
+    unit = fft_unit(n, order=fft_order.bit_reversed)
+    unit.exec(x, x, batch=2)
+    want = O.fft_packed(O.pack(z, 8), n, order=1)
+    assert rel_l2(O.unpack(x.cpu().numpy(), n, 8), O.unpack(want, n, 8)) < TOL[np.float32]
+    unit.exec(x, x, batch=2, direction=1)
+    assert rel_l2(O.unpack(x.cpu().numpy(), n, 8), z) < TOL[np.float32]
+
+
+def test_vector_api_and_errors():
+    n = 512
+    rng = np.random.default_rng(2)
+    z = normal_cx(rng, n)
+    v = vector.from_complex(z)
+    unit = fft_unit(n)
+    unit(v)
+    assert rel_l2(v.to_complex(), np.fft.fft(z)) < TOL[np.float32]
+    unit.ifft(v)
+    assert rel_l2(v.to_complex(), z) < TOL[np.float32]
+    # out-of-place with a shorter source (zero extension) and another pack width
+    s = vector.from_complex(z[:300], pack=4)
+    d = vector(n)
+    unit(d, s)
+    zz = np.zeros(n, complex)
+    zz[:300] = z[:300]
+    assert rel_l2(d.to_complex(), np.fft.fft(zz)) < TOL[np.float32]
+    # out-of-place inverse is the correct inverse (the reference's is not)
+    back = vector(n, pack=2)
+    unit.ifft(back, d)
+    assert rel_l2(back.to_complex(), zz) < TOL[np.float32]
+    with pytest.raises(ValueError, match="is not equal to fft size"):
+        unit(vector(n // 2))
+    with pytest.raises(ValueError, match="is bigger than fft size"):
+        unit(vector(n), vector(n * 2))
+    with pytest.raises(ValueError, match="in-place repack"):
+        unit(vector(n, pack=16, data=d.data), vector(n, pack=8, data=d.data))
+
+
+def test_unnormalized_inverse_all_orders():
+    n = 2048
+    rng = np.random.default_rng(4)
+    z = normal_cx(rng, n)
+    for order in (0, 1, 2):
+        unit = fft_unit(n, order=order)
+        y = O.fft_packed(O.pack(z, 8), n, order=order)
+        got = run(unit, y, 1, direction=1, normalize=False)
+        assert rel_l2(O.unpack(got, n, 8), z * n) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("log_n", [6, 12, 14, 20])
+def test_vjp_adjoint_identity(log_n):
+    # <F x, y> == <x, F^H y> for the forward and the normalised inverse
+    n = 1 << log_n
+    rng = np.random.default_rng(log_n)
+    x, y = normal_cx(rng, n), normal_cx(rng, n)
+    for order in (0, 1):
+        unit = fft_unit(n, dtype=F64, order=order)
+        for direction, norm in ((0, True), (1, True), (1, False)):
+            xd = to_dev(O.pack(x, 4, np.float64), F64)
+            fx = torch.empty_like(xd)
+            unit.exec(fx, xd, direction=direction, normalize=norm)
+            gy = to_dev(O.pack(y, 4, np.float64), F64)
+            gx = unit.vjp(gy, direction=direction, normalize=norm)
+            lhs = np.vdot(O.unpack(fx.cpu().numpy(), n, 4), y)
+            rhs = np.vdot(x, O.unpack(gx.cpu().numpy(), n, 4))
+            assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("log_n", [6, 10, 12, 13, 16, 18, 20])
+def test_full_size_roundtrip_and_parseval(log_n):
+    # C2 size: 1 GiB of complex64 per buffer, N(0,1) seed 1 — size-independent
+    # properties: Parseval and forward->inverse round trip
+    n = 1 << log_n
+    b = (1 << 27) // n
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(b * 2 * n, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    unit = fft_unit(n)
+    unit.exec(y, x, batch=b)
+    ex = (x.double() ** 2).view(b, -1).sum(1)
+    ey = (y.double() ** 2).view(b, -1).sum(1) / n
+    assert torch.max(torch.abs(ey / ex - 1)).item() < 1e-5
+    unit.exec(y, y, batch=b, direction=1)
+    err = torch.linalg.norm((y - x).double()) / torch.linalg.norm(x.double())
+    assert err.item() < 2e-6
+    # the first rows against the oracle
+    rows = x[: 2 * n * min(b, 2)].cpu().numpy().reshape(-1, 2 * n)
+    got = torch.empty(rows.size, device="cuda")
+    unit.exec(got, to_dev(rows, F32), batch=rows.shape[0])
+    want = O.fft_packed(rows, n)
+    assert rel_l2(O.unpack(got.cpu().numpy().reshape(rows.shape), n, 8), O.unpack(want, n, 8)) < 2e-6
