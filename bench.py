@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "FP32 FFT/fxcorr GB/s, % of HBM peak; tensor-core vs plain at ≤2e-6 rel err"
 LOG_NS = list(range(6, 21))
-POINTS = 1 << 27    # complex64 points per 1 GiB buffer
+POINTS = 1 << 27    # complex64 points per 1 GiB buffer (overridable by --points for profiling captures)
 BYTES_PER_POINT_DIR = 16
 
 
@@ -227,7 +227,13 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=27, help="log2 complex points per buffer (profiling captures)")
+    ap.add_argument("--sizes", type=str, default=None, help="comma list of log2 N (profiling captures)")
     args = ap.parse_args()
+    global POINTS, LOG_NS
+    POINTS = 1 << args.points
+    if args.sizes:
+        LOG_NS = [int(v) for v in args.sizes.split(",")]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     config = {"workload": "C2 FP32 FFT size sweep: N=2^6..2^20, 1 GiB complex64 per size (batch 2^27/N), "

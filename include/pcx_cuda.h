@@ -14,7 +14,7 @@
  *
  * The reference (Dooez/packed) is a header-only C++ template library with no
  * FFI of its own; each entry point below names the reference interface whose
- * behaviour it carries.  include/pcxo/*.hpp wraps these calls in the
+ * behaviour it carries.  The headers in include/pcxo/ wrap these calls in the
  * reference's own class templates.
  */
 #ifndef PCX_CUDA_H
@@ -122,6 +122,13 @@ int pcx_fxcorr_destroy(pcx_fxcorr h);
  */
 int pcx_fxcorr_exec(pcx_fxcorr h, void* dst, const void* src, size_t len, int pack, size_t channels,
                     size_t dst_stride, size_t src_stride, void* stream);
+
+/*
+ * PCX_ERR_TIMEOUT if an in-place correlation since the last call had a block
+ * give up waiting for its predecessor's read (bounded device wait; the
+ * affected outputs are not written), else PCX_OK.  Synchronises the device.
+ */
+int pcx_fxcorr_status(pcx_fxcorr h);
 
 /*
  * Adjoint of pcx_fxcorr_exec: given gy (cotangent of y), writes gx

@@ -38,6 +38,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_fxcorr_destroy": (_i, [_vp]),
     "pcx_fxcorr_exec": (_i, [_vp, _vp, _vp, _sz, _i, _sz, _sz, _sz, _vp]),
     "pcx_fxcorr_vjp": (_i, [_vp, _vp, _vp, _vp, _vp, _sz, _i, _sz, _sz, _vp]),
+    "pcx_fxcorr_status": (_i, [_vp]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -142,14 +142,16 @@ __device__ __forceinline__ void dft(cpx<T> (&v)[E]) {
 
 // ---- stage plan for an L = 2^LOGL point Stockham FFT ---------------------
 // Radix-16 stages first (stage 0 carries no twiddles), remainder radix last.
-// Each thread owns E values; in every stage thread t holds the elements
-// t + m*TT (m < E) of its transform, TT = L / E threads per transform.
-template<int LOGL>
+// Each thread owns E values (E = EPT, or L when smaller); in every stage
+// thread t holds the elements t + m*TT (m < E) of its transform, TT = L / E
+// threads per transform.  A radix-R stage runs E/R butterflies per thread.
+template<int LOGL_, int EPT = 16>
 struct splan {
-    static constexpr int L   = 1 << LOGL;
-    static constexpr int E   = LOGL >= 4 ? 16 : (1 << LOGL);
-    static constexpr int TT  = L / E;
-    static constexpr int NST = (LOGL + 3) / 4;
+    static constexpr int LOGL = LOGL_;
+    static constexpr int L    = 1 << LOGL;
+    static constexpr int E    = L < EPT ? L : EPT;
+    static constexpr int TT   = L / E;
+    static constexpr int NST  = (LOGL + 3) / 4;
     __host__ __device__ static constexpr int rbits(int s) { return s < LOGL / 4 ? 4 : LOGL % 4; }
     __host__ __device__ static constexpr int nsbits(int s) {
         int b = 0;
@@ -159,9 +161,10 @@ struct splan {
 };
 
 // Butterflies of stage S.  twL: table W_L^i (i < L).
-template<int LOGL, int S, class T, int E>
+template<class P, int S, class T, int E>
 __device__ __forceinline__ void stage_compute(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ twL) {
-    using P              = splan<LOGL>;
+    static_assert(E == P::E, "register count");
+    constexpr int LOGL   = P::LOGL;
     constexpr int RB     = P::rbits(S);
     constexpr int R      = 1 << RB;
     constexpr int NSB    = P::nsbits(S);
@@ -190,10 +193,10 @@ __device__ __forceinline__ void stage_compute(cpx<T> (&v)[E], int t, const cpx<T
     });
 }
 
-// Output index of value v[g + j*G] after stage S (thread t).
-template<int LOGL, int S>
+// Output index of value v[g + j*G] after stage S (thread t).  After the last
+// stage value v[i] holds frequency t + i*TT.
+template<class P, int S>
 __device__ __forceinline__ int stage_out_index(int t, int g, int j) {
-    using P           = splan<LOGL>;
     constexpr int RB  = P::rbits(S);
     constexpr int NSB = P::nsbits(S);
     const int     b   = t + g * P::TT;

@@ -144,6 +144,10 @@ static cudaError_t dispatch_row(int logl, const pass_args& a, long long rows, co
 
 using namespace pcxg;
 
+cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bool f64, cudaStream_t st) {
+    return f64 ? gen_twiddles<double>(out, count, log_n, mult, st) : gen_twiddles<float>(out, count, log_n, mult, st);
+}
+
 // ------------------------------------------------------------------- plans
 static size_t scratch_cap_bytes() {
     static size_t cap = [] {

@@ -100,10 +100,9 @@ struct xch_interleaved {    // element-major, the M transforms side by side
 
 // Run stages 1..NST-1 through the exchange buffer; on entry v holds stage-0
 // outputs, on exit v holds the final outputs of the last stage.
-template<int LOGL, class X, class T, int E>
+template<class P, class X, class T, int E>
 __device__ __forceinline__ void run_stages(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
                                            const cpx<T>* __restrict__ twL) {
-    using P = splan<LOGL>;
     static_for<P::NST - 1>([&](auto sc) {
         constexpr int S = decltype(sc)::value;    // stage whose outputs we write
         constexpr int G = E / (1 << P::rbits(S));
@@ -111,14 +110,14 @@ __device__ __forceinline__ void run_stages(cpx<T> (&v)[E], cpx<T>* xch, int m, i
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             constexpr int g = i % G, j = i / G;
-            xch[X::idx(m, stage_out_index<LOGL, S>(t, g, j))] = v[i];
+            xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
         });
         __syncthreads();
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             v[i]            = xch[X::idx(m, t + i * P::TT)];
         });
-        stage_compute<LOGL, S + 1>(v, t, twL);
+        stage_compute<P, S + 1>(v, t, twL);
     });
 }
 
@@ -168,8 +167,8 @@ __global__ void __launch_bounds__(NT) k_single(io_args a, const cpx<T>* __restri
         const T        re = raw[o], im = raw[o + Pin];
         v[i]              = {re, a.conj_in ? -im : im};
     });
-    stage_compute<LOGL, 0>(v, t, twL);
-    run_stages<LOGL, X>(v, xch, m, t, twL);
+    stage_compute<P, 0>(v, t, twL);
+    run_stages<P, X>(v, xch, m, t, twL);
     __syncthreads();
 
     // Last stage: value v[g + j*G] is frequency k = t + g*TT + j*Ns.
@@ -182,7 +181,7 @@ __global__ void __launch_bounds__(NT) k_single(io_args a, const cpx<T>* __restri
         static_for<E>([&](auto ic) {
             constexpr int  i = decltype(ic)::value;
             constexpr int  g = i % G, j = i / G;
-            const uint32_t k = stage_out_index<LOGL, S>(t, g, j);
+            const uint32_t k = stage_out_index<P, S>(t, g, j);
             const uint32_t o = m * rout + pk_re(order_pos(k, a.order_out, LOGL), a.lp_dst);
             raw[o]           = v[i].re * sc;
             raw[o + Pout]    = v[i].im * sim;
@@ -282,8 +281,8 @@ __global__ void __launch_bounds__(NT) k_colpass(pass_args a, const cpx<T>* __res
         const T        re = raw[o], im = raw[o + Pin];
         v[i]              = {re, io.conj_in ? -im : im};
     });
-    stage_compute<LOGL, 0>(v, t, twL);
-    run_stages<LOGL, X>(v, xch, c, t, twL);
+    stage_compute<P, 0>(v, t, twL);
+    run_stages<P, X>(v, xch, c, t, twL);
     __syncthreads();
 
     {
@@ -297,7 +296,7 @@ __global__ void __launch_bounds__(NT) k_colpass(pass_args a, const cpx<T>* __res
         static_for<E>([&](auto ic) {
             constexpr int  i  = decltype(ic)::value;
             constexpr int  g  = i % G, j = i / G;
-            const uint32_t k1 = stage_out_index<LOGL, S>(t, g, j);
+            const uint32_t k1 = stage_out_index<P, S>(t, g, j);
             cpx<T>         w  = v[i];
             if (a.twiddle) w = cmul(w, tw_big(hi, lo, k1 * (uint32_t)(c0 + c), a.log_lo));
             const uint32_t o = k1 * SEG + pk_re(c, io.lp_dst);
@@ -358,8 +357,8 @@ __global__ void __launch_bounds__(NT) k_rowpass(pass_args a, const cpx<T>* __res
         const T        re = raw[o], im = raw[o + Pin];
         v[i]              = {re, io.conj_in ? -im : im};
     });
-    stage_compute<LOGL, 0>(v, t, twL);
-    run_stages<LOGL, X>(v, xch, m, t, twL);
+    stage_compute<P, 0>(v, t, twL);
+    run_stages<P, X>(v, xch, m, t, twL);
     __syncthreads();
 
     const int  r      = r0 + m;
@@ -376,7 +375,7 @@ __global__ void __launch_bounds__(NT) k_rowpass(pass_args a, const cpx<T>* __res
         static_for<E>([&](auto ic) {
             constexpr int  i = decltype(ic)::value;
             constexpr int  g = i % G, j = i / G;
-            const uint32_t k = stage_out_index<LOGL, S>(t, g, j);
+            const uint32_t k = stage_out_index<P, S>(t, g, j);
             cpx<T>         w = v[i];
             if (a.twiddle) w = cmul(w, tw_big(hi, lo, k * (uint32_t)rowdft, a.log_lo));
             uint32_t o;

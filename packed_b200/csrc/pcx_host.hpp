@@ -61,3 +61,6 @@ struct pcx_plan_s {
 int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
                 size_t batch, size_t dstride, size_t sstride, void* ws, size_t ws_bytes, cudaStream_t st,
                 double extra_scale);
+
+// Table W_N^(i*mult), i < count, N = 2^log_n, generated in FP64 and rounded once.
+cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bool f64, cudaStream_t st);

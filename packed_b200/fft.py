@@ -257,6 +257,7 @@ class fxcorr_unit:
             g = vector.from_complex(np.asarray(g), dtype=dtype or torch.float32)
         self._dtype = g.dtype
         self._k = g.size()
+        self._pack_g = g.pack_size
         self._n = int(fft_size)
         self._h = ctypes.c_void_p()
         _lib.check(_lib.lib().pcx_fxcorr_create(ctypes.byref(self._h), _ptr(g.data), self._k, g.pack_size, self._n,
@@ -273,6 +274,15 @@ class fxcorr_unit:
 
     def fft_size(self) -> int:
         return self._n
+
+    def step(self, pack: int | None = None) -> int:
+        """Outputs per overlap-save block: (N - (K-1)) rounded down to the pack."""
+        p = pack or default_pack_size(self._dtype)
+        return (self._n - (self._k - 1)) // p * p
+
+    def status(self) -> None:
+        """Raise TimeoutError if an in-place block gave up waiting (pcx_fxcorr_status)."""
+        _lib.check(_lib.lib().pcx_fxcorr_status(self._h))
 
     def kernel_size(self) -> int:
         return self._k
@@ -297,7 +307,8 @@ class fxcorr_unit:
             want_kernel_grad: bool = True, stream=None) -> tuple[torch.Tensor, torch.Tensor | None]:
         p = pack or default_pack_size(self._dtype)
         gx = torch.empty_like(gy)
-        gg = torch.empty(real_size(self._k, p), dtype=self._dtype, device=gy.device) if want_kernel_grad else None
+        gg = (torch.empty(real_size(self._k, self._pack_g), dtype=self._dtype, device=gy.device)
+              if want_kernel_grad else None)
         _lib.check(_lib.lib().pcx_fxcorr_vjp(self._h, _ptr(gx), _ptr(gg) if gg is not None else None, _ptr(gy),
                                              _ptr(x), length, p, channels, real_size(length, p),
                                              _stream_ptr(stream)))

@@ -1,0 +1,129 @@
+// C++ drop-in check: the reference's own call patterns (tests/test_fft.cpp,
+// tests/test_fxcorr.cpp of the reference) compiled against include/pcxo/*.hpp
+// and run on the GPU.  Exit status 0 on success.
+#include "pcxo/fft.hpp"
+#include "pcxo/fxcorr.hpp"
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+using cd = std::complex<double>;
+
+static std::vector<cd> dft(const std::vector<cd>& x, int sign) {
+    const std::size_t n = x.size();
+    std::vector<cd>   X(n);
+    for (std::size_t k = 0; k < n; ++k) {
+        cd s = 0;
+        for (std::size_t j = 0; j < n; ++j) s += x[j] * std::polar(1.0, sign * 2 * M_PI * double((j * k) % n) / n);
+        X[k] = s;
+    }
+    return X;
+}
+
+template<typename V>
+static double rel_err(const V& got, const std::vector<cd>& want) {
+    double num = 0, den = 0;
+    for (std::size_t i = 0; i < want.size(); ++i) {
+        cd g = std::complex<double>(got[i]);
+        num += std::norm(g - want[i]);
+        den += std::norm(want[i]);
+    }
+    return std::sqrt(num / den);
+}
+
+static int fails = 0;
+static void expect(bool ok, const char* what, double v = 0) {
+    std::printf("%-44s %s %.3e\n", what, ok ? "ok  " : "FAIL", v);
+    if (!ok) ++fails;
+}
+
+int main() {
+    std::mt19937_64                        rng(0);
+    std::uniform_real_distribution<float> u(-1, 1);
+    constexpr float                        pi = 3.14159265358979323846f;
+    for (std::size_t n: {64u, 1024u, 8192u}) {
+        pcxo::vector<float>           v(n);
+        std::vector<std::complex<float>> sv(n);
+        std::vector<cd>                  x(n);
+        for (std::size_t i = 0; i < n; ++i) {
+            auto val = std::exp(std::complex<float>(0, 2 * pi * i / n * 13.37f));    // reference test input
+            v[i]     = val;
+            sv[i]    = val;
+            x[i]     = cd(val);
+        }
+        const auto X = dft(x, -1);
+        pcxo::fft_unit<float> unit(n);
+        unit(v);
+        expect(rel_err(v, X) < 2e-6, "fft_unit<float>(vector) normal", rel_err(v, X));
+        unit.ifft(v);
+        expect(rel_err(v, x) < 2e-6, "ifft(vector) round trip", rel_err(v, x));
+        unit(sv);    // host std::vector<std::complex<float>>: staged
+        expect(rel_err(sv, X) < 2e-6, "fft_unit(std::vector<complex>)", rel_err(sv, X));
+        pcxo::vector<float> out(n);
+        unit(out, v);
+        expect(rel_err(out, X) < 2e-6, "fft_unit(dest, src)", rel_err(out, X));
+        pcxo::fft_unit<float, pcxo::fft_order::bit_reversed> ubr(n);
+        pcxo::vector<float>                                  w = v;
+        ubr.fft_raw<8>(w.data());
+        ubr.ifft_raw<true, 8>(w.data());
+        expect(rel_err(w, x) < 2e-6, "bit_reversed fft_raw/ifft_raw", rel_err(w, x));
+        // zero-extended source (fft.hpp:759-820)
+        pcxo::vector<float> shortv(n / 2 + 3);
+        std::vector<cd>     xs(n, 0.0);
+        for (std::size_t i = 0; i < shortv.size(); ++i) {
+            shortv[i] = std::complex<float>(u(rng), u(rng));
+            xs[i]     = cd(std::complex<float>(shortv[i]));
+        }
+        unit(out, shortv);
+        expect(rel_err(out, dft(xs, -1)) < 2e-6, "zero-extended out-of-place", rel_err(out, dft(xs, -1)));
+    }
+    {
+        pcxo::vector<double> v(4096);
+        std::vector<cd>      x(4096);
+        for (std::size_t i = 0; i < 4096; ++i) x[i] = cd(u(rng), u(rng)), v[i] = x[i];
+        pcxo::fft_unit<double> unit(4096);
+        unit(v);
+        expect(rel_err(v, dft(x, -1)) < 1e-13, "fft_unit<double>", rel_err(v, dft(x, -1)));
+    }
+    {    // fxcorr (tests/test_fxcorr.cpp: naive correlation ground truth)
+        const std::size_t   k = 300, s = 10000, nf = 1024;
+        pcxo::vector<float> g(k), f(s);
+        std::vector<cd>     gd(k), fd(s), y(s);
+        for (std::size_t i = 0; i < k; ++i) gd[i] = cd(u(rng), u(rng)), g[i] = gd[i];
+        for (std::size_t i = 0; i < s; ++i) fd[i] = cd(u(rng), u(rng)), f[i] = fd[i];
+        for (std::size_t i = 0; i < s; ++i) {
+            cd acc = 0;
+            for (std::size_t j = 0; j < k && i + j < s; ++j) acc += fd[i + j] * std::conj(gd[j]);
+            y[i] = acc;
+        }
+        pcxo::fxcorr_unit<float> xc(g, nf);
+        pcxo::vector<float>      dst(s);
+        xc(dst, f);
+        expect(rel_err(dst, y) < 2e-6, "fxcorr_unit(dest, src)", rel_err(dst, y));
+        xc(f);
+        expect(rel_err(f, y) < 2e-6, "fxcorr_unit(vector) in place", rel_err(f, y));
+    }
+    {    // exceptions keep the reference's types and messages
+        bool thrown = false;
+        try {
+            pcxo::fft_unit<float> bad(1000);
+        } catch (const std::invalid_argument& e) {
+            thrown = std::string(e.what()).find("power of two") != std::string::npos;
+        }
+        expect(thrown, "invalid_argument for non power of two");
+        thrown = false;
+        try {
+            pcxo::fft_unit<float> unit(64);
+            pcxo::vector<float>   v(32);
+            unit(v);
+        } catch (const std::invalid_argument& e) {
+            thrown = std::string(e.what()).find("is not equal to fft size") != std::string::npos;
+        }
+        expect(thrown, "invalid_argument for size mismatch");
+    }
+    std::printf(fails ? "FAILED %d\n" : "ALL OK\n", fails);
+    return fails ? 1 : 0;
+}

@@ -1,0 +1,203 @@
+"""GPU parity of the fused overlap-save correlator and its adjoint against the
+CPU oracle (direct FP64 sums, overlap-save restatement) and the reference's
+golden outputs."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from packed_b200 import fxcorr_unit, real_size, vector
+from packed_b200.autograd import FxcorrFunction
+from tests._util import TOL, golden, normal_cx, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+F32, F64 = torch.float32, torch.float64
+
+
+def dev(a, dtype=F32):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).cuda()
+
+
+def corr(z, g, n_fft, pack=8, inplace=True, dtype=F32, channels=1):
+    npd = np.float32 if dtype == F32 else np.float64
+    s = z.shape[-1]
+    unit = fxcorr_unit(vector.from_complex(g, dtype=dtype), n_fft)
+    x = dev(O.pack(z, pack, npd), dtype)
+    y = x if inplace else torch.full_like(x, float("nan"))
+    unit.exec(y, x, s, channels=channels, pack=pack)
+    torch.cuda.synchronize()
+    if inplace:
+        unit.status()
+    return O.unpack(y.cpu().numpy(), s, pack)
+
+
+def test_reference_single_block_golden():
+    G = golden()
+    for tag, k, n, s in (("xc1", 128, 256, 128), ("xc2", 512, 1024, 512)):
+        z, g = O.unpack(G[f"{tag}_x"], s, 8), O.unpack(G[f"{tag}_g"], k, 8)
+        got = corr(z, g, n)
+        assert rel_l2(got, O.unpack(G[f"{tag}_y"], s, 8)) < 1e-5
+        assert rel_l2(got, O.xcorr_direct(z, g)) < TOL[np.float32]
+
+
+def test_multi_block_against_corrected_reference():
+    G = golden()
+    z, g = O.unpack(G["xc3_x"], 3000, 8), O.unpack(G["xc3_g"], 100, 8)
+    got = corr(z, g, 512)
+    assert rel_l2(got, O.unpack(G["xc3_y"], 3000, 8)) < TOL[np.float32]
+    assert rel_l2(got, O.xcorr_direct(z, g)) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("s,k,n", [(1, 1, 64), (100, 13, 64), (777, 60, 128), (5000, 200, 1024), (4096, 1, 256),
+                                   (20000, 1000, 2048), (33333, 3000, 4096), (70000, 4000, 8192),
+                                   (100000, 4096, 16384), (50000, 12000, 16384)])
+@pytest.mark.parametrize("inplace", [True, False])
+def test_against_direct_sum(s, k, n, inplace):
+    rng = np.random.default_rng(s + k)
+    z, g = normal_cx(rng, s), normal_cx(rng, k, sigma=1 / np.sqrt(k))
+    got = corr(z, g, n, inplace=inplace)
+    want = O.xcorr_ols(z, g, n) if s * k > 5e7 else O.xcorr_direct(z, g)
+    assert rel_l2(got, want) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("pack", [1, 2, 4, 8, 16])
+def test_pack_widths_and_channels(pack):
+    rng = np.random.default_rng(pack)
+    ch, s, k, n = 3, 3001, 77, 512
+    z, g = normal_cx(rng, ch, s), normal_cx(rng, k)
+    unit = fxcorr_unit(vector.from_complex(g), n)
+    x = dev(O.pack(z, pack))
+    unit.exec(x, x, s, channels=ch, pack=pack)
+    got = O.unpack(x.cpu().numpy(), s, pack)
+    for c in range(ch):
+        assert rel_l2(got[c], O.xcorr_direct(z[c], g)) < TOL[np.float32]
+
+
+def test_fp64():
+    rng = np.random.default_rng(64)
+    z, g = normal_cx(rng, 20000), normal_cx(rng, 700)
+    got = corr(z, g, 2048, pack=4, dtype=F64)
+    assert rel_l2(got, O.xcorr_ols(z, g, 2048, 4)) < TOL[np.float64]
+
+
+def test_c3_shape_reduced_channels():
+    # C3 parameters (K=4096, N_fft=16384, step 12288) on 4 channels of 2^18
+    rng = np.random.default_rng(2)
+    ch, s, k, n = 4, 1 << 18, 4096, 16384
+    z = normal_cx(rng, ch, s).astype(np.complex64)
+    g = normal_cx(rng, k, sigma=1 / 64).astype(np.complex64)
+    unit = fxcorr_unit(vector.from_complex(g), n)
+    assert unit.step() == 12288
+    x = dev(O.pack(z, 8))
+    unit.exec(x, x, s, channels=ch)
+    unit.status()
+    got = O.unpack(x.cpu().numpy(), s, 8)
+    for c in range(ch):
+        assert rel_l2(got[c], O.xcorr_ols(z[c], g, n)) < TOL[np.float32]
+
+
+@pytest.mark.slow
+def test_c3_full_size_sampled():
+    # full C3: 256 channels x 2^20, in place; 64 random outputs per 8 channels
+    # checked against direct FP64 sums (size-independent property)
+    ch, s, k, n = 256, 1 << 20, 4096, 16384
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    x = torch.randn(ch * 2 * s, device="cuda", generator=gen)
+    rng = np.random.default_rng(3)
+    g = normal_cx(rng, k, sigma=1 / 64).astype(np.complex64)
+    unit = fxcorr_unit(vector.from_complex(g), n)
+    orig = x.clone()
+    unit.exec(x, x, s, channels=ch)
+    unit.status()
+    xo = orig.view(ch, 2 * s)
+    y = x.view(ch, 2 * s)
+    gd = g.astype(np.complex128)
+    for c in rng.integers(0, ch, 8):
+        zc = O.unpack(xo[c].cpu().numpy(), s, 8)
+        yc = O.unpack(y[c].cpu().numpy(), s, 8)
+        idx = np.concatenate([rng.integers(0, s, 60), [0, 12287, 12288, s - 1]])
+        for i in idx:
+            seg = zc[i:i + k]
+            want = np.sum(seg * np.conj(gd[: len(seg)]))
+            assert abs(yc[i] - want) <= 2e-5 * (np.sqrt(k) / 64 * 1.5 + abs(want))
+
+
+def test_vjp_against_oracle():
+    rng = np.random.default_rng(11)
+    ch, s, k, n = 2, 9000, 300, 1024
+    z, g = normal_cx(rng, ch, s), normal_cx(rng, k)
+    gy = normal_cx(rng, ch, s)
+    unit = fxcorr_unit(vector.from_complex(g), n)
+    gx, gg = unit.vjp(dev(O.pack(gy, 8)), dev(O.pack(z, 8)), s, channels=ch)
+    gx = O.unpack(gx.cpu().numpy(), s, 8)
+    gg = O.unpack(gg.cpu().numpy(), k, 8)
+    gg_want = np.zeros(k, complex)
+    for c in range(ch):
+        gxw, ggw = O.xcorr_vjp_direct(z[c], g, gy[c])
+        assert rel_l2(gx[c], gxw) < TOL[np.float32]
+        gg_want += ggw
+    assert rel_l2(gg, gg_want) < TOL[np.float32]
+
+
+def test_autograd_c3_gradients_vs_fd():
+    # loss = sum w |y|^2, w ~ U[0,1) seed 6; C3 kernel shape (K=4096, N=16384)
+    # on 1 channel of 2^16; gradients at 64 random coordinates vs FP64 central
+    # finite differences (h = 1e-6) of the FP64 direct loss.
+    rng = np.random.default_rng(2)
+    s, k, n = 1 << 16, 4096, 16384
+    z = normal_cx(rng, s)
+    g = normal_cx(rng, k, sigma=1 / 64)
+    w = np.random.default_rng(6).uniform(0, 1, s)
+    x = dev(O.pack(z, 8)).requires_grad_(True)
+    gt = dev(O.pack(g, 8)).requires_grad_(True)
+    y = FxcorrFunction.apply(x, gt, n, s, k, 1)
+    wt = dev(O.pack(w.astype(complex), 8))
+    wr = wt.clone()
+    wr.view(-1, 2, 8)[:, 1, :] = wt.view(-1, 2, 8)[:, 0, :]    # weight both re and im
+    loss = (wr * y * y).sum()
+    loss.backward()
+    gx = O.unpack(x.grad.cpu().numpy(), s, 8)
+    gg = O.unpack(gt.grad.cpu().numpy(), k, 8)
+    yd = O.xcorr_ols(z, g, n)
+
+    def local_loss_x(zz, i):
+        lo, hi = max(0, i - k + 1), i + 1
+        seg = zz[lo: min(s, hi + k - 1)]
+        yy = np.array([np.sum(seg[m - lo: m - lo + k] * np.conj(g[: len(seg[m - lo: m - lo + k])]))
+                       for m in range(lo, hi)])
+        return float(np.sum(w[lo:hi] * np.abs(yy) ** 2))
+
+    h = 1e-6
+    for i in rng.integers(0, s, 32):
+        for unit_dir, part in ((1.0, "re"), (1j, "im")):
+            zp, zm = z.copy(), z.copy()
+            zp[i] += h * unit_dir
+            zm[i] -= h * unit_dir
+            fd = (local_loss_x(zp, i) - local_loss_x(zm, i)) / (2 * h)
+            an = gx[i].real if part == "re" else gx[i].imag
+            assert abs(fd - an) <= 1e-6 * max(1.0, abs(fd)) + 2e-5 * abs(fd)
+    # kernel coordinates: FD of the full FP64 loss (overlap-save in FP64)
+    for j in rng.integers(0, k, 32):
+        for unit_dir, part in ((1.0, "re"), (1j, "im")):
+            gp, gm = g.copy(), g.copy()
+            gp[j] += h * unit_dir
+            gm[j] -= h * unit_dir
+            lp = float(np.sum(w * np.abs(O.xcorr_ols(z, gp, n)) ** 2))
+            lm = float(np.sum(w * np.abs(O.xcorr_ols(z, gm, n)) ** 2))
+            fd = (lp - lm) / (2 * h)
+            an = gg[j].real if part == "re" else gg[j].imag
+            assert abs(fd - an) <= 1e-6 * max(1.0, abs(fd)) + 2e-5 * abs(fd)
+    assert np.isfinite(yd).all()
+
+
+def test_errors():
+    g = vector.from_complex(np.ones(100))
+    with pytest.raises(ValueError, match="power of two"):
+        fxcorr_unit(g, 1000)
+    with pytest.raises(ValueError):
+        fxcorr_unit(g, 64)
+    unit = fxcorr_unit(g, 128)
+    x = torch.zeros(real_size(100, 8), device="cuda")
+    with pytest.raises(ValueError):
+        unit.exec(x, x, 100, pack=3)
