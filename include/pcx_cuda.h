@@ -95,6 +95,31 @@ int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, i
                     void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Size of the device scratch array that pcx_fft_exec_noalloc uses (8 MiB,
+ * held by every GPU that loads the library until the process exits).
+ */
+#define PCX_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/*
+ * No counterpart in the reference (which has no GPU and no scratch).
+ * As pcx_fft_exec, but allocates nothing, for callers that cannot allocate
+ * device memory while running (a fixed memory budget set at start-up, device
+ * memory handed out only by the caller's own pool, rules that forbid device
+ * allocation after initialisation).  The four-step path (n > 4096) uses a
+ * file-scope device array of PCX_NOALLOC_SCRATCH_BYTES instead of allocated
+ * scratch, processing the batch in chunks that fit it; sizes whose single
+ * transform does not fit (n * element bytes > 8 MiB: only fp64 at n = 2^20)
+ * are rejected with
+ * PCX_ERR_UNSUPPORTED.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls whose GPU work overlaps race.
+ * The plan itself must already exist (pcx_plan_create allocates).
+ */
+int pcx_fft_exec_noalloc(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
+                         int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,
+                         void* stream);
+
+/*
  * Adjoint (vector-Jacobian product) of pcx_fft_exec with the same arguments:
  * given the cotangent g_out of the transform's output, writes the cotangent
  * of its input.  The forward DFT's adjoint is the unnormalised inverse read

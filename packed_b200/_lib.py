@@ -34,6 +34,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_fft_exec": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),
     "pcx_fft_exec_ws": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp]),
     "pcx_fft_vjp": (_i, [_vp, _vp, _vp, _i, _i, _i, _sz, _sz, _vp]),
+    "pcx_fft_exec_noalloc": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),
     "pcx_fxcorr_create": (_i, [ctypes.POINTER(_vp), _vp, _sz, _i, _sz, _i]),
     "pcx_fxcorr_destroy": (_i, [_vp]),
     "pcx_fxcorr_exec": (_i, [_vp, _vp, _vp, _sz, _i, _sz, _sz, _sz, _vp]),

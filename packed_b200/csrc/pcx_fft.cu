@@ -286,7 +286,7 @@ int check_pack(int pack, const char* what) {
 
 int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
                 size_t batch, size_t dstride, size_t sstride, void* ws, size_t ws_bytes, cudaStream_t st,
-                double extra_scale) {
+                double extra_scale, size_t chunk_cap) {
     if (!p) return pcx_fail(PCX_ERR_INVALID, "plan is null");
     if (int rc = check_pack(pd, "destination")) return rc;
     if (int rc = check_pack(ps, "source")) return rc;
@@ -349,7 +349,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     }
 
     // four-step through L2-sized chunks of scratch
-    const size_t chunk = p->chunk_rows(batch);
+    const size_t chunk = chunk_cap ? std::min(chunk_cap, p->chunk_rows(batch)) : p->chunk_rows(batch);
     const size_t need  = chunk * n * eb;
     void*        scr   = ws;
     if (!scr) {

@@ -58,9 +58,11 @@ struct pcx_plan_s {
 };
 
 // Core of pcx_fft_exec (no exception guard); extra_scale multiplies the output.
+// chunk_cap (rows per four-step chunk, 0 = no cap) lets a caller with a
+// fixed workspace bound the chunk to it.
 int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
                 size_t batch, size_t dstride, size_t sstride, void* ws, size_t ws_bytes, cudaStream_t st,
-                double extra_scale);
+                double extra_scale, size_t chunk_cap = 0);
 
 // Table W_N^(i*mult), i < count, N = 2^log_n, generated in FP64 and rounded once.
 cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bool f64, cudaStream_t st);
