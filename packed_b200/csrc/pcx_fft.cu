@@ -2,6 +2,7 @@
 // FP64), the launch schedule for the single-pass and four-step paths, and the
 // FFT entry points of the C ABI (include/pcx_cuda.h).
 #include "pcx_fft_kernels.cuh"
+#include "pcx_fft_v2.cuh"
 #include "pcx_host.hpp"
 
 #include <algorithm>
@@ -153,7 +154,7 @@ static size_t scratch_cap_bytes() {
     static size_t cap = [] {
         const char* e = std::getenv("PCX_SCRATCH_MB");
         long        v = e ? std::atol(e) : 0;
-        return (size_t)(v > 0 ? v : 40) << 20;
+        return (size_t)(v > 0 ? v : 24) << 20;
     }();
     return cap;
 }
@@ -202,6 +203,42 @@ static int plan_init_tables(pcx_plan_s* p) {
                              : dispatch_row<float>(lg, z, 0, nullptr, 0, true));
         }
     }
+    // hot-path tables: stage twiddles per sub-transform, W_{16*N2}^m
+    {
+        int e1 = 0, e2 = 0;
+        if (!p->two_pass) {
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(log_n, nullptr, f64, 0, &e1));
+            PCX_CUDA_TRY(cudaMalloc(&p->stw, (size_t)std::max(e1, 2) * eb));
+            p->stwL = p->stw;
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(log_n, p->stwL, f64, 0, &e1));
+            v2_args z{};
+            cudaError_t e = pcx_v2_single(f64, log_n, z, 0, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+        } else {
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(p->log_n1, nullptr, f64, 0, &e1));
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(p->log_n2, nullptr, f64, 0, &e2));
+            const size_t nb = (size_t)16 << p->log_n2;
+            PCX_CUDA_TRY(cudaMalloc(&p->stw, ((size_t)e1 + e2 + nb) * eb));
+            char* base = static_cast<char*>(p->stw);
+            p->stw1    = base;
+            p->stw2    = base + (size_t)e1 * eb;
+            p->tw_b    = base + ((size_t)e1 + e2) * eb;
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(p->log_n1, p->stw1, f64, 0, &e1));
+            PCX_CUDA_TRY(pcx_v2_stage_twiddles(p->log_n2, p->stw2, f64, 0, &e2));
+            PCX_CUDA_TRY(gen(p->tw_b, (int)nb, p->log_n2 + 4, 1));
+            v2_args     z{};
+            cudaError_t e = pcx_v2_col(f64, p->log_n1, p->log_n2, z, 0, p->sms, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+            e = pcx_v2_row(f64, p->log_n1, p->log_n2, z, 0, p->sms, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+            PCX_CUDA_TRY(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+            for (int i = 0; i < 2; ++i) {
+                PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_col[i], cudaEventDisableTiming));
+                PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_row[i], cudaEventDisableTiming));
+            }
+            PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+        }
+    }
     PCX_CUDA_TRY(cudaDeviceSynchronize());
     return PCX_OK;
 }
@@ -239,6 +276,10 @@ extern "C" int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, s
         p->log_n1   = (p->log_n + 1) / 2;
         p->log_n2   = p->log_n / 2;
         cudaGetDevice(&p->device);
+        if (cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess) {
+            (void)cudaGetLastError();
+            p->sms = 148;
+        }
         int rc = plan_init_tables(p);
         if (rc != PCX_OK) {
             p->release();
@@ -252,9 +293,18 @@ extern "C" int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, s
 
 void pcx_plan_s::release() {
     if (tw) cudaFree(tw);
+    if (stw) cudaFree(stw);
     if (scratch) cudaFree(scratch);
+    if (side) cudaStreamDestroy(side);
+    for (int i = 0; i < 2; ++i) {
+        if (ev_col[i]) cudaEventDestroy(ev_col[i]);
+        if (ev_row[i]) cudaEventDestroy(ev_row[i]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     tw      = nullptr;
+    stw     = nullptr;
     scratch = nullptr;
+    side    = nullptr;
 }
 
 extern "C" int pcx_plan_destroy(pcx_plan plan) {
@@ -270,7 +320,7 @@ extern "C" size_t pcx_plan_size(pcx_plan plan) { return plan ? plan->n : 0; }
 
 extern "C" size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch) {
     if (!plan || !plan->two_pass) return 0;
-    return plan->chunk_rows(batch) * plan->n * plan->elem_bytes();
+    return 2 * plan->chunk_rows(batch) * plan->n * plan->elem_bytes();
 }
 
 // ------------------------------------------------------------------ exec
@@ -338,8 +388,30 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     io.scale      = scale;
     const bool f64 = p->dtype == PCX_F64;
     const size_t eb = p->elem_bytes();
+    const int    lp_def = f64 ? 2 : 3;    // default pack: 32 bytes of reals
+
+    // hot-path argument block for the pcx_fft_v2.cuh kernels
+    v2_args h{};
+    h.conj_in  = io.conj_in;
+    h.conj_out = io.conj_out;
+    h.scale    = io.scale;
 
     if (!p->two_pass) {
+        const bool hot = io.order_in == 0 && io.order_out == 0 && src_len == n && io.lp_src == lp_def &&
+                         io.lp_dst == lp_def && p->log_n >= 7;
+        if (hot) {
+            h.src        = src;
+            h.dst        = dst;
+            h.src_stride = (long long)sstride;
+            h.dst_stride = (long long)dstride;
+            h.batch      = (long long)batch;
+            h.stw        = p->stwL;
+            cudaError_t e = pcx_v2_single(f64, p->log_n, h, st, false);
+            if (e != cudaErrorNotSupported) {
+                PCX_CUDA_TRY(e);
+                return PCX_OK;
+            }
+        }
         io.src   = src;
         io.dst   = dst;
         io.batch = (long long)batch;
@@ -348,11 +420,15 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         return PCX_OK;
     }
 
-    // four-step through L2-sized chunks of scratch
-    const size_t chunk = chunk_cap ? std::min(chunk_cap, p->chunk_rows(batch)) : p->chunk_rows(batch);
-    const size_t need  = chunk * n * eb;
+    // Four-step through L2-sized chunks of scratch.  With two scratch buffers
+    // the passes are pipelined over two streams: the column pass of chunk c+1
+    // (caller's stream) runs beside the row pass of chunk c (side stream).
+    size_t       chunk = chunk_cap ? std::min(chunk_cap, p->chunk_rows(batch)) : p->chunk_rows(batch);
+    const size_t per   = n * eb;
     void*        scr   = ws;
+    int          nbuf  = 2;
     if (!scr) {
+        const size_t need = 2 * chunk * per;
         if (p->scratch_bytes < need) {
             if (p->scratch) cudaFree(p->scratch);
             p->scratch       = nullptr;
@@ -361,15 +437,44 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
             p->scratch_bytes = need;
         }
         scr = p->scratch;
-    } else if (ws_bytes < need) {
-        return pcx_fail(PCX_ERR_INVALID, "workspace smaller than pcx_plan_workspace_size");
+    } else {
+        if (ws_bytes < chunk * per) {
+            if (chunk_cap == 0) return pcx_fail(PCX_ERR_INVALID, "workspace smaller than pcx_plan_workspace_size");
+            chunk = std::max<size_t>(1, ws_bytes / per);
+        }
+        if (ws_bytes >= 2 * chunk * per) {
+            nbuf = 2;
+        } else if (ws_bytes >= 2 * per) {
+            chunk = ws_bytes / (2 * per);
+            nbuf  = 2;
+        } else {
+            nbuf = 1;
+        }
     }
+    const int nchunks = (int)((batch + chunk - 1) / chunk);
+    if (nchunks <= 1) nbuf = 1;
 
-    const size_t es = f64 ? sizeof(double) : sizeof(float);
-    for (size_t r0 = 0; r0 < batch; r0 += chunk) {
+    const size_t es     = f64 ? sizeof(double) : sizeof(float);
+    const bool   direct = !(inv && p->order != 0);
+    // hot-path eligibility of each pass
+    const bool col_hot = direct && src_len == n && io.lp_src == lp_def;
+    const bool row_hot = direct && io.order_out == 0 && io.lp_dst == lp_def;
+
+    std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
+    if (nbuf == 2) {
+        lock.lock();
+        PCX_CUDA_TRY(cudaEventRecord(p->ev_fork, st));
+        PCX_CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    }
+    for (int ci = 0; ci < nchunks; ++ci) {
+        const size_t    r0   = (size_t)ci * chunk;
         const long long rows = (long long)std::min(chunk, batch - r0);
         const char*     s    = static_cast<const char*>(src) + r0 * sstride * es;
         char*           d    = static_cast<char*>(dst) + r0 * dstride * es;
+        const int       b    = nbuf == 2 ? (ci & 1) : 0;
+        void*           buf  = static_cast<char*>(scr) + (size_t)b * chunk * per;
+        cudaStream_t    st2  = nbuf == 2 ? p->side : st;
+        if (nbuf == 2 && ci >= 2) PCX_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_row[b], 0));
 
         pass_args a{};
         a.log_n1 = p->log_n1;
@@ -377,39 +482,82 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         a.log_lo = p->log_n2;
         a.tw_hi  = p->tw_hi;
         a.tw_lo  = p->tw_lo;
-
-        pass_args b = a;
-        if (!(inv && p->order != 0)) {
+        pass_args bb = a;
+        if (direct) {
             // pass 1: columns src -> scratch (with twiddle); pass 2: rows scratch -> dst
-            a.io            = io;
-            a.io.src        = s;
-            a.io.dst        = scr;
-            a.io.dst_stride = (long long)(2 * n);
-            a.io.lp_dst     = 0;
-            a.io.conj_out   = 0;
-            a.io.scale      = 1.0;
-            a.io.order_out  = 0;
-            a.twiddle       = 1;
-            b.io            = io;
-            b.io.src        = scr;
-            b.io.src_stride = (long long)(2 * n);
-            b.io.src_len    = (int)n;
-            b.io.lp_src     = 0;
-            b.io.conj_in    = 0;
-            b.io.order_in   = 0;
-            b.io.dst        = d;
-            b.twiddle       = 0;
-            b.transposed_out = io.order_out == 0;
-            b.row_map        = io.order_out != 0;
-            PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, a, rows, p->twN1, st, false)
-                             : dispatch_col<float>(p->log_n1, a, rows, p->twN1, st, false));
-            PCX_CUDA_TRY(f64 ? dispatch_row<double>(p->log_n2, b, rows, p->twN2, st, false)
-                             : dispatch_row<float>(p->log_n2, b, rows, p->twN2, st, false));
+            bool done = false;
+            if (col_hot) {
+                v2_args c = h;
+                c.src        = s;
+                c.dst        = buf;
+                c.src_stride = (long long)sstride;
+                c.dst_stride = (long long)(2 * n);
+                c.batch      = rows;
+                c.conj_out   = 0;
+                c.scale      = 1.0;
+                c.stw        = p->stw1;
+                c.tw_hi      = p->tw_hi;
+                c.tw_lo      = p->tw_lo;
+                c.tw_b       = p->tw_b;
+                cudaError_t e = pcx_v2_col(f64, p->log_n1, p->log_n2, c, st, p->sms, false);
+                if (e != cudaErrorNotSupported) {
+                    PCX_CUDA_TRY(e);
+                    done = true;
+                }
+            }
+            if (!done) {
+                a.io            = io;
+                a.io.src        = s;
+                a.io.dst        = buf;
+                a.io.dst_stride = (long long)(2 * n);
+                a.io.lp_dst     = 0;
+                a.io.conj_out   = 0;
+                a.io.scale      = 1.0;
+                a.io.order_out  = 0;
+                a.twiddle       = 1;
+                PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, a, rows, p->twN1, st, false)
+                                 : dispatch_col<float>(p->log_n1, a, rows, p->twN1, st, false));
+            }
+            if (nbuf == 2) {
+                PCX_CUDA_TRY(cudaEventRecord(p->ev_col[b], st));
+                PCX_CUDA_TRY(cudaStreamWaitEvent(st2, p->ev_col[b], 0));
+            }
+            done = false;
+            if (row_hot) {
+                v2_args r = h;
+                r.src        = buf;
+                r.dst        = d;
+                r.src_stride = (long long)(2 * n);
+                r.dst_stride = (long long)dstride;
+                r.batch      = rows;
+                r.conj_in    = 0;
+                r.stw        = p->stw2;
+                cudaError_t e = pcx_v2_row(f64, p->log_n1, p->log_n2, r, st2, p->sms, false);
+                if (e != cudaErrorNotSupported) {
+                    PCX_CUDA_TRY(e);
+                    done = true;
+                }
+            }
+            if (!done) {
+                bb.io             = io;
+                bb.io.src         = buf;
+                bb.io.src_stride  = (long long)(2 * n);
+                bb.io.src_len     = (int)n;
+                bb.io.lp_src      = 0;
+                bb.io.conj_in     = 0;
+                bb.io.order_in    = 0;
+                bb.io.dst         = d;
+                bb.twiddle        = 0;
+                bb.transposed_out = io.order_out == 0;
+                bb.row_map        = io.order_out != 0;
+                PCX_CUDA_TRY(f64 ? dispatch_row<double>(p->log_n2, bb, rows, p->twN2, st2, false)
+                                 : dispatch_row<float>(p->log_n2, bb, rows, p->twN2, st2, false));
+            }
         } else {
             // inverse from a permuted order: rows first (input rows), then columns
             a.io             = io;
             a.io.src         = s;
-            a.io.dst         = scr;
+            a.io.dst         = buf;
             a.io.dst_stride  = (long long)(2 * n);
             a.io.lp_dst      = 0;
             a.io.conj_out    = 0;
@@ -418,20 +566,30 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
             a.twiddle        = 1;
             a.row_map        = 1;
             a.transposed_out = 0;
-            b.io             = io;
-            b.io.src         = scr;
-            b.io.src_stride  = (long long)(2 * n);
-            b.io.src_len     = (int)n;
-            b.io.lp_src      = 0;
-            b.io.conj_in     = 0;
-            b.io.order_in    = 0;
-            b.io.dst         = d;
-            b.twiddle        = 0;
+            bb.io            = io;
+            bb.io.src        = buf;
+            bb.io.src_stride = (long long)(2 * n);
+            bb.io.src_len    = (int)n;
+            bb.io.lp_src     = 0;
+            bb.io.conj_in    = 0;
+            bb.io.order_in   = 0;
+            bb.io.dst        = d;
+            bb.twiddle       = 0;
             PCX_CUDA_TRY(f64 ? dispatch_row<double>(p->log_n2, a, rows, p->twN2, st, false)
                              : dispatch_row<float>(p->log_n2, a, rows, p->twN2, st, false));
-            PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, b, rows, p->twN1, st, false)
-                             : dispatch_col<float>(p->log_n1, b, rows, p->twN1, st, false));
+            if (nbuf == 2) {
+                PCX_CUDA_TRY(cudaEventRecord(p->ev_col[b], st));
+                PCX_CUDA_TRY(cudaStreamWaitEvent(st2, p->ev_col[b], 0));
+            }
+            PCX_CUDA_TRY(f64 ? dispatch_col<double>(p->log_n1, bb, rows, p->twN1, st2, false)
+                             : dispatch_col<float>(p->log_n1, bb, rows, p->twN1, st2, false));
         }
+        if (nbuf == 2) PCX_CUDA_TRY(cudaEventRecord(p->ev_row[b], st2));
+    }
+    if (nbuf == 2) {
+        // join: the caller's stream waits for the last row passes
+        PCX_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_row[(nchunks - 1) & 1], 0));
+        if (nchunks >= 2) PCX_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_row[(nchunks - 2) & 1], 0));
     }
     return PCX_OK;
 }

@@ -1,0 +1,298 @@
+// Hot-path FFT kernels: natural order, pack width known at compile time.
+//
+// Differences from the general kernels in pcx_fft_kernels.cuh:
+//  * data go straight between global memory and registers — stage 0 reads
+//    element t + i*TT of its row, and the Stockham last stage leaves
+//    frequency t + i*TT in v[i], so both ends are coalesced without a
+//    shared-memory staging copy; shared memory only carries the exchanges
+//    between stages;
+//  * every address is a per-thread base plus compile-time offsets (sizes and
+//    pack width are template parameters);
+//  * stage twiddles come from per-stage tables laid out [k][j] so that one
+//    butterfly's R twiddles are R contiguous entries (vector loads);
+//  * the four-step twiddle W_N^(k1*n2), k1 = t + i*TT, is W_N^(t*n2) (one
+//    two-level lookup per thread) times W_{16*N2}^(i*n2) (one table entry).
+#pragma once
+
+#include "pcx_fft_kernels.cuh"
+
+namespace pcxg {
+
+// ---- per-stage twiddle tables ------------------------------------------------
+// Stage S >= 1 of splan P has Ns = 2^nsbits(S) butterfly positions k and
+// radix R; its table holds W_{Ns*R}^(j*k) at [k*R + j] (j = 0 unused).
+template<class P>
+__host__ __device__ constexpr int stage_tw_offset(int S) {
+    int off = 0;
+    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) * (1 << P::rbits(s));
+    return off;
+}
+template<class P>
+__host__ __device__ constexpr int stage_tw_size() {
+    return stage_tw_offset<P>(P::NST);
+}
+
+template<class T>
+__global__ void k_stage_twiddles(cpx<T>* out, int ns, int r, int log_nsr) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns * r) return;
+    const int       k = q / r, j = q - k * r;
+    const long long e = (long long)j * k;
+    double          s, c;
+    sincospi(2.0 * (double)e / (double)(1LL << log_nsr), &s, &c);
+    out[q] = {T(c), T(-s)};
+}
+
+template<class T>
+__device__ __forceinline__ void ldg2(const cpx<T>* p, cpx<T>& a, cpx<T>& b);
+template<>
+__device__ __forceinline__ void ldg2(const cpx<float>* p, cpx<float>& a, cpx<float>& b) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    a              = {v.x, v.y};
+    b              = {v.z, v.w};
+}
+template<>
+__device__ __forceinline__ void ldg2(const cpx<double>* p, cpx<double>& a, cpx<double>& b) {
+    a = ldg_cpx(p);
+    b = ldg_cpx(p + 1);
+}
+
+template<class P, int S, class T, int E>
+__device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ stw) {
+    constexpr int RB  = P::rbits(S);
+    constexpr int R   = 1 << RB;
+    constexpr int NSB = P::nsbits(S);
+    constexpr int G   = E / R;
+    static_for<G>([&](auto gc) {
+        constexpr int g = decltype(gc)::value;
+        cpx<T>        a[R];
+        static_for<R>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            a[j]            = v[g + j * G];
+        });
+        if constexpr (NSB > 0) {
+            const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
+            const cpx<T>* tw = stw + stage_tw_offset<P>(S) + k * R;
+            cpx<T>        w[R];
+            static_for<R / 2>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                ldg2(tw + 2 * j, w[2 * j], w[2 * j + 1]);
+            });
+            static_for<R - 1>([&](auto jc) {
+                constexpr int j = decltype(jc)::value + 1;
+                a[j]            = cmul(a[j], w[j]);
+            });
+        }
+        dft<R, 1, 0>(a);
+        static_for<R>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            v[g + j * G]    = a[j];
+        });
+    });
+}
+
+// Exchange-buffer index with the padding (one slot per 16) split into a
+// per-thread base and compile-time offsets.  Valid when the low four bits of
+// base plus those of the offset do not carry (true for every Stockham access
+// pattern here: offsets are multiples of 16, or the base is).
+__device__ __forceinline__ int pad16(int l) { return l + (l >> 4); }
+
+template<class P, class X, class T, int E>
+__device__ __forceinline__ void run_stages_tab(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
+                                               const cpx<T>* __restrict__ stw) {
+    static_for<P::NST - 1>([&](auto sc) {
+        constexpr int S = decltype(sc)::value;
+        constexpr int G = E / (1 << P::rbits(S));
+        __syncthreads();
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int g = i % G, j = i / G;
+            xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
+        });
+        __syncthreads();
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = xch[X::idx(m, t + i * P::TT)];
+        });
+        stage_compute_tab<P, S + 1>(v, t, stw);
+    });
+}
+
+// Exchange layout for groups of G8 transforms side by side (element-major
+// inside a group), groups one after another.
+template<int L, int M, int G8>
+struct xch_grouped {
+    static constexpr int LP   = L + (L >= 16 ? L / 16 : 0);
+    static constexpr int size = M * LP;
+    __device__ static __forceinline__ int idx(int m, int l) {
+        const int pl = l + (L >= 16 ? (l >> 4) : 0);
+        return ((m / G8) * LP + pl) * G8 + (m % G8);
+    }
+};
+
+template<int LP>
+__device__ __forceinline__ int pk(int i) {
+    return ((i >> LP) << (LP + 1)) | (i & ((1 << LP) - 1));
+}
+
+struct v2_args {
+    const void* src;
+    void*       dst;
+    long long   src_stride;    // reals between rows (transforms)
+    long long   dst_stride;
+    long long   batch;         // rows (transforms) in this launch
+    int         conj_in;
+    int         conj_out;
+    double      scale;
+    const void* stw;           // stage twiddles of the sub-transform
+    const void* tw_hi;         // four-step twiddle, two-level W_N^e
+    const void* tw_lo;
+    const void* tw_b;          // W_{16*N2}^m, m < 16*N2
+};
+
+// ---------------------------------------------------------------------------
+// Single-pass, natural order, N = 2^LOGL (128 <= N <= 4096), pack 2^LP.
+template<class T, int LOGL, int LP, int NT>
+__global__ void __launch_bounds__(NT) k_single2(v2_args a) {
+    using P          = splan<LOGL>;
+    constexpr int L  = P::L;
+    constexpr int E  = P::E;
+    constexpr int TT = P::TT;
+    constexpr int M  = NT / TT;
+    constexpr int PK = 1 << LP;
+    static_assert(TT % PK == 0, "pack must divide threads per row");
+    using X = xch_blocked<L, M>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    cpx<T>*       xch = reinterpret_cast<cpx<T>*>(smem);
+    const auto*   stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const int     tid = threadIdx.x;
+    const int     m   = tid / TT;
+    const int     t   = tid - m * TT;
+    const long long row = (long long)blockIdx.x * M + m;
+    const bool    live  = row < a.batch;
+    const T*      src = reinterpret_cast<const T*>(a.src) + (live ? row : 0) * a.src_stride + pk<LP>(t);
+    T*            dst = reinterpret_cast<T*>(a.dst) + row * a.dst_stride + pk<LP>(t);
+
+    cpx<T> v[E];
+    static_for<E>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const T       re = src[2 * i * TT], im = src[2 * i * TT + PK];
+        v[i]           = {re, a.conj_in ? -im : im};
+    });
+    stage_compute_tab<P, 0>(v, t, stw);
+    run_stages_tab<P, X>(v, xch, m, t, stw);
+    if (live) {
+        const T sc  = T(a.scale);
+        const T sim = a.conj_out ? -sc : sc;
+        static_for<E>([&](auto ic) {
+            constexpr int i   = decltype(ic)::value;
+            dst[2 * i * TT]      = v[i].re * sc;
+            dst[2 * i * TT + PK] = v[i].im * sim;
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four-step column pass: C columns n2 = c0..c0+C-1 of N1 = 2^LOGN1 rows,
+// packed natural input (pack 2^LP) -> interleaved scratch rows [k1][n2],
+// with the twiddle W_N^(k1*n2).  Persistent over the launch's tiles.
+template<class T, int LOGN1, int LOGN2, int LP, int C, int NT>
+__global__ void __launch_bounds__(NT, 2) k_col2(v2_args a) {
+    using P           = splan<LOGN1>;
+    constexpr int N1  = P::L;
+    constexpr int N2  = 1 << LOGN2;
+    constexpr int E   = P::E;
+    constexpr int TT  = P::TT;
+    constexpr int PK  = 1 << LP;
+    constexpr int TPR = N2 / C;    // tiles per transform
+    static_assert(NT == C * TT, "threads");
+    static_assert(C % PK == 0, "pack must divide the column group");
+    using X = xch_interleaved<N1, C>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    cpx<T>*     xch = reinterpret_cast<cpx<T>*>(smem);
+    const auto* stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const auto* thi = reinterpret_cast<const cpx<T>*>(a.tw_hi);
+    const auto* tlo = reinterpret_cast<const cpx<T>*>(a.tw_lo);
+    const auto* tb  = reinterpret_cast<const cpx<T>*>(a.tw_b);
+    const int   tid = threadIdx.x;
+    const int   c   = tid % C;
+    const int   t   = tid / C;
+    const long long tiles = a.batch * TPR;
+
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long row = tile / TPR;
+        const int       c0  = (int)(tile - row * TPR) * C;
+        const int       n2  = c0 + c;
+        const T* src = reinterpret_cast<const T*>(a.src) + row * a.src_stride + pk<LP>(t * N2 + n2);
+        cpx<T>   v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i  = decltype(ic)::value;
+            const T       re = src[2 * i * TT * N2], im = src[2 * i * TT * N2 + PK];
+            v[i]            = {re, a.conj_in ? -im : im};
+        });
+        stage_compute_tab<P, 0>(v, t, stw);
+        run_stages_tab<P, X>(v, xch, c, t, stw);
+        // v[i] = column spectrum at k1 = t + i*TT; twiddle W_N^(k1*n2)
+        const uint32_t e0   = (uint32_t)t * (uint32_t)n2;
+        const cpx<T>   base = cmul(ldg_cpx(thi + (e0 >> LOGN2)), ldg_cpx(tlo + (e0 & (N2 - 1))));
+        cpx<T>*        dst  = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            cpx<T>        w = base;
+            if constexpr (i > 0) w = cmul(base, ldg_cpx(tb + ((i * n2) & (16 * N2 - 1))));
+            dst[(long long)i * TT * N2] = cmul(v[i], w);
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four-step row pass: CR rows k1 = r0..r0+CR-1 of N2 = 2^LOGN2 interleaved
+// scratch elements -> natural packed output X[k2*N1 + k1] (pack 2^LP).
+// Threads: G8 rows fastest (one 64-byte output segment per k2), then t.
+template<class T, int LOGN1, int LOGN2, int LP, int CR, int G8, int NT>
+__global__ void __launch_bounds__(NT, 2) k_row2(v2_args a) {
+    using P           = splan<LOGN2>;
+    constexpr int N1  = 1 << LOGN1;
+    constexpr int N2  = P::L;
+    constexpr int E   = P::E;
+    constexpr int TT  = P::TT;
+    constexpr int PK  = 1 << LP;
+    constexpr int TPR = N1 / CR;
+    static_assert(NT == CR * TT, "threads");
+    static_assert(CR % G8 == 0 && G8 % PK == 0, "row grouping");
+    using X = xch_grouped<N2, CR, G8>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    cpx<T>*     xch = reinterpret_cast<cpx<T>*>(smem);
+    const auto* stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const int   tid = threadIdx.x;
+    const int   mlo = tid % G8;
+    const int   t   = (tid / G8) % TT;
+    const int   mhi = tid / (G8 * TT);
+    const int   m   = mhi * G8 + mlo;
+    const long long tiles = a.batch * TPR;
+
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long row = tile / TPR;
+        const int       r0  = (int)(tile - row * TPR) * CR;
+        const int       k1  = r0 + m;
+        const cpx<T>*   src = reinterpret_cast<const cpx<T>*>(a.src) + row * (a.src_stride / 2) + (long long)k1 * N2 + t;
+        cpx<T>          v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = src[i * TT];
+        });
+        stage_compute_tab<P, 0>(v, t, stw);
+        run_stages_tab<P, X>(v, xch, m, t, stw);
+        // v[i] = X[k2*N1 + k1], k2 = t + i*TT
+        T*      dst = reinterpret_cast<T*>(a.dst) + row * a.dst_stride + pk<LP>(t * N1 + k1);
+        const T sc  = T(a.scale);
+        const T sim = a.conj_out ? -sc : sc;
+        static_for<E>([&](auto ic) {
+            constexpr int i              = decltype(ic)::value;
+            dst[2 * i * TT * N1]         = v[i].re * sc;
+            dst[2 * i * TT * N1 + PK]    = v[i].im * sim;
+        });
+    }
+}
+
+}    // namespace pcxg

@@ -5,7 +5,12 @@
 
 #include <cuda_runtime.h>
 #include <exception>
+#include <mutex>
 #include <string>
+
+namespace pcxg {
+struct v2_args;
+}
 
 // Record `msg` as this thread's last error and return `code`.
 int pcx_fail(int code, const std::string& msg);
@@ -52,6 +57,22 @@ struct pcx_plan_s {
     void*  scratch       = nullptr;    // four-step intermediate (plan-owned)
     size_t scratch_bytes = 0;
 
+    // hot-path tables (pcx_fft_v2.cuh)
+    void*  stw      = nullptr;    // one allocation: stage twiddles (N | N1, N2) and W_{16*N2}^m
+    void*  stwL     = nullptr;    // stage twiddles of the single pass
+    void*  stw1     = nullptr;    // stage twiddles of the column pass (N1)
+    void*  stw2     = nullptr;    // stage twiddles of the row pass (N2)
+    void*  tw_b     = nullptr;    // W_{16*N2}^m, m < 16*N2
+    int    sms      = 148;
+
+    // four-step chunk pipeline: column passes on the caller's stream, row
+    // passes on `side`, two scratch buffers
+    cudaStream_t side = nullptr;
+    cudaEvent_t  ev_col[2]{};
+    cudaEvent_t  ev_row[2]{};
+    cudaEvent_t  ev_fork = nullptr;
+    std::mutex   mu;
+
     size_t elem_bytes() const { return dtype == PCX_F64 ? 16 : 8; }
     size_t chunk_rows(size_t batch) const;
     void   release();
@@ -66,3 +87,13 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
 
 // Table W_N^(i*mult), i < count, N = 2^log_n, generated in FP64 and rounded once.
 cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bool f64, cudaStream_t st);
+
+// Hot-path launches (pcx_v2_*.cu); cudaErrorNotSupported when no variant exists.
+cudaError_t pcx_v2_single(bool f64, int log_n, const pcxg::v2_args& a, cudaStream_t st, bool attr_only);
+cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
+                       bool attr_only);
+cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
+                       bool attr_only);
+// Stage-twiddle table of an L = 2^log_l point transform: *entries complex
+// values; generated into `out` unless it is null.
+cudaError_t pcx_v2_stage_twiddles(int log_l, void* out, bool f64, cudaStream_t st, int* entries);
