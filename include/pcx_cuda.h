@@ -67,6 +67,12 @@ int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, size_t sub_s
 int pcx_plan_destroy(pcx_plan plan);
 /* fft_unit::size() (fft.hpp:615-617). */
 size_t pcx_plan_size(pcx_plan plan);
+/*
+ * PCX_ERR_TIMEOUT if a kernel of this plan gave up a bounded wait for its
+ * input copy since the last call (its rows are then not written), else
+ * PCX_OK.  Synchronises with the device.
+ */
+int pcx_plan_status(pcx_plan plan);
 /* Bytes of scratch an exec of this plan uses for `batch` rows (0 for n <= 4096). */
 size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
 

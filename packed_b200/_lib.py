@@ -30,6 +30,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_plan_create": (_i, [ctypes.POINTER(_vp), _sz, _i, _i, _sz]),
     "pcx_plan_destroy": (_i, [_vp]),
     "pcx_plan_size": (_sz, [_vp]),
+    "pcx_plan_status": (_i, [_vp]),
     "pcx_plan_workspace_size": (_sz, [_vp, _sz]),
     "pcx_fft_exec": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),
     "pcx_fft_exec_ws": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp]),

@@ -203,6 +203,8 @@ static int plan_init_tables(pcx_plan_s* p) {
                              : dispatch_row<float>(lg, z, 0, nullptr, 0, true));
         }
     }
+    PCX_CUDA_TRY(cudaMalloc(&p->err, sizeof(int)));
+    PCX_CUDA_TRY(cudaMemset(p->err, 0, sizeof(int)));
     // hot-path tables: stage twiddles per sub-transform, W_{16*N2}^m
     {
         int e1 = 0, e2 = 0;
@@ -213,6 +215,9 @@ static int plan_init_tables(pcx_plan_s* p) {
             PCX_CUDA_TRY(pcx_v2_stage_twiddles(log_n, p->stwL, f64, 0, &e1));
             v2_args z{};
             cudaError_t e = pcx_v2_single(f64, log_n, z, 0, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+            v3_args z3{};
+            e = pcx_v3_single(f64, log_n, z3, 0, p->sms, true);
             if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
         } else {
             PCX_CUDA_TRY(pcx_v2_stage_twiddles(p->log_n1, nullptr, f64, 0, &e1));
@@ -301,6 +306,8 @@ void pcx_plan_s::release() {
         if (ev_row[i]) cudaEventDestroy(ev_row[i]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (err) cudaFree(err);
+    err = nullptr;
     tw      = nullptr;
     stw     = nullptr;
     scratch = nullptr;
@@ -317,6 +324,19 @@ extern "C" int pcx_plan_destroy(pcx_plan plan) {
 }
 
 extern "C" size_t pcx_plan_size(pcx_plan plan) { return plan ? plan->n : 0; }
+
+extern "C" int pcx_plan_status(pcx_plan plan) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        int err = 0;
+        PCX_CUDA_TRY(cudaMemcpy(&err, plan->err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+            PCX_CUDA_TRY(cudaMemset(plan->err, 0, sizeof(int)));
+            return pcx_fail(PCX_ERR_TIMEOUT, "a transform of this plan gave up waiting for its input copy");
+        }
+        return PCX_OK;
+    });
+}
 
 extern "C" size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch) {
     if (!plan || !plan->two_pass) return 0;
@@ -397,6 +417,30 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     h.scale    = io.scale;
 
     if (!p->two_pass) {
+        // TMA-fed kernel: any order, default pack, full-length rows on 16-byte strides
+        const size_t vr = 16 / (f64 ? sizeof(double) : sizeof(float));
+        const bool   tma = src_len == n && io.lp_src == lp_def && io.lp_dst == lp_def && p->log_n >= 5 &&
+                         (batch == 1 || (sstride % vr == 0 && dstride % vr == 0));
+        if (tma) {
+            v3_args t3{};
+            t3.src        = src;
+            t3.dst        = dst;
+            t3.src_stride = (long long)sstride;
+            t3.dst_stride = (long long)dstride;
+            t3.batch      = (long long)batch;
+            t3.conj_in    = io.conj_in;
+            t3.conj_out   = io.conj_out;
+            t3.order_in   = io.order_in;
+            t3.order_out  = io.order_out;
+            t3.scale      = io.scale;
+            t3.stw        = p->stwL;
+            t3.error      = p->err;
+            cudaError_t e = pcx_v3_single(f64, p->log_n, t3, st, p->sms, false);
+            if (e != cudaErrorNotSupported) {
+                PCX_CUDA_TRY(e);
+                return PCX_OK;
+            }
+        }
         const bool hot = io.order_in == 0 && io.order_out == 0 && src_len == n && io.lp_src == lp_def &&
                          io.lp_dst == lp_def && p->log_n >= 7;
         if (hot) {

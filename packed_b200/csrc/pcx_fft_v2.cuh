@@ -15,6 +15,7 @@
 #pragma once
 
 #include "pcx_fft_kernels.cuh"
+#include "pcx_tma.cuh"
 
 namespace pcxg {
 
@@ -292,6 +293,158 @@ __global__ void __launch_bounds__(NT, 2) k_row2(v2_args a) {
             dst[2 * i * TT * N1]         = v[i].re * sc;
             dst[2 * i * TT * N1 + PK]    = v[i].im * sim;
         });
+    }
+}
+
+}    // namespace pcxg
+
+// ===========================================================================
+// TMA-fed single pass.  Persistent CTAs; each tile (M rows) is brought into
+// shared memory by one-dimensional bulk copies through a two-stage ring, so
+// the next tiles are in flight while this one is transformed.  Stage 0 reads
+// the packed rows from shared memory (any input order), the last stage
+// writes packed rows into a staging area (any output order) that the threads
+// copy out with 16-byte stores.  Rows are padded in shared memory so that
+// the rows of one warp fall into different banks.
+namespace pcxg {
+
+struct v3_args {
+    const void* src;
+    void*       dst;
+    long long   src_stride;
+    long long   dst_stride;
+    long long   batch;
+    int         conj_in;
+    int         conj_out;
+    int         order_in;
+    int         order_out;
+    double      scale;
+    const void* stw;
+    int*        error;    // set when a bounded wait gives up
+};
+
+template<int TT>
+__host__ __device__ constexpr int single3_pad() {
+    return TT >= 32 ? 0 : (TT >= 8 ? 8 : 4);
+}
+template<class T, int LOGL, int NT>
+__host__ __device__ constexpr int single3_smem() {
+    using P          = splan<LOGL>;
+    constexpr int M  = NT / P::TT;
+    constexpr int RS = 2 * P::L + single3_pad<P::TT>();
+    return 2 * M * RS * (int)sizeof(T) + xch_blocked<P::L, M>::size * (int)sizeof(cpx<T>);
+}
+
+template<class T, int LOGL, int LP, int NT>
+__global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
+    using P             = splan<LOGL>;
+    constexpr int L     = P::L;
+    constexpr int E     = P::E;
+    constexpr int TT    = P::TT;
+    constexpr int M     = NT / TT;
+    constexpr int PK    = 1 << LP;
+    constexpr int PADR  = single3_pad<TT>();
+    constexpr int RS    = 2 * L + PADR;    // shared-memory row stride (reals)
+    constexpr int TILE  = M * RS;
+    constexpr int ROWB  = 2 * L * (int)sizeof(T);
+    constexpr int V     = 16 / (int)sizeof(T);
+    using X             = xch_blocked<L, M>;
+    static_assert(X::size * 2 >= TILE, "staging fits the exchange buffer");
+    static_assert((RS * (int)sizeof(T)) % 16 == 0, "rows stay 16-byte aligned");
+    extern __shared__ __align__(128) unsigned char smem[];
+    T*               in0 = reinterpret_cast<T*>(smem);
+    cpx<T>*          xch = reinterpret_cast<cpx<T>*>(in0 + 2 * TILE);
+    T*               stg = reinterpret_cast<T*>(xch);
+    __shared__ uint64_t full[2];
+    const auto*      stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const T*         src = reinterpret_cast<const T*>(a.src);
+    T*               dst = reinterpret_cast<T*>(a.dst);
+    const int        tid = threadIdx.x;
+    const int        m   = tid / TT;
+    const int        t   = tid - m * TT;
+    const long long  ntile = (a.batch + M - 1) / M;
+    const bool       contig_in  = PADR == 0 && a.src_stride == 2 * L;
+    const bool       contig_out = PADR == 0 && a.dst_stride == 2 * L;
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](long long tile, int s) {    // thread 0 only
+        const int  rows = (int)min((long long)M, a.batch - tile * M);
+        T*         buf  = in0 + s * TILE;
+        const T*   g    = src + tile * M * a.src_stride;
+        mbar_arrive_expect_tx(&full[s], (uint32_t)rows * ROWB);
+        if (contig_in) {
+            bulk_g2s(buf, g, (uint32_t)rows * ROWB, &full[s]);
+        } else {
+            for (int r = 0; r < rows; ++r) bulk_g2s(buf + r * RS, g + r * a.src_stride, ROWB, &full[s]);
+        }
+    };
+    if (tid == 0) {
+        if ((long long)blockIdx.x < ntile) issue(blockIdx.x, 0);
+        if ((long long)blockIdx.x + gridDim.x < ntile) issue(blockIdx.x + gridDim.x, 1);
+    }
+
+    long long k = 0;
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x, ++k) {
+        const int      s   = (int)(k & 1);
+        const uint32_t par = (uint32_t)((k >> 1) & 1);
+        const bool     ok  = mbar_wait_bounded(&full[s], par);
+        if (__syncthreads_or(!ok)) {
+            // give up: record it, let the other stage's copy land, leave together
+            if (tid == 0) {
+                atomicExch(a.error, 1);
+                mbar_wait_bounded(&full[s], par, 100000000ull);
+                mbar_wait_bounded(&full[s ^ 1], par ^ (s ? 1u : 0u), 100000000ull);
+            }
+            __syncthreads();
+            return;
+        }
+        const T* in = in0 + s * TILE;
+        cpx<T>   v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int  i  = decltype(ic)::value;
+            const uint32_t p  = order_pos(t + i * TT, a.order_in, LOGL);
+            const int      o  = m * RS + pk<LP>((int)p);
+            const T        re = in[o], im = in[o + PK];
+            v[i]              = {re, a.conj_in ? -im : im};
+        });
+        __syncthreads();    // stage s consumed: refill it with the tile after next
+        if (tid == 0 && tile + 2 * (long long)gridDim.x < ntile) issue(tile + 2 * (long long)gridDim.x, s);
+        stage_compute_tab<P, 0>(v, t, stw);
+        run_stages_tab<P, X>(v, xch, m, t, stw);
+        __syncthreads();    // exchange reads done: reuse the buffer as staging
+        {
+            constexpr int S   = P::NST - 1;
+            constexpr int G   = E / (1 << P::rbits(S));
+            const T       sc  = T(a.scale);
+            const T       sim = a.conj_out ? -sc : sc;
+            static_for<E>([&](auto ic) {
+                constexpr int  i = decltype(ic)::value;
+                constexpr int  g = i % G, j = i / G;
+                const uint32_t kf = stage_out_index<P, S>(t, g, j);
+                const int      o  = m * RS + pk<LP>((int)order_pos(kf, a.order_out, LOGL));
+                stg[o]            = v[i].re * sc;
+                stg[o + PK]       = v[i].im * sim;
+            });
+        }
+        __syncthreads();
+        const int rows = (int)min((long long)M, a.batch - tile * M);
+        T*        d    = dst + tile * M * a.dst_stride;
+        if (contig_out) {
+            for (int q = tid; q < rows * (2 * L / V); q += NT) {
+                *reinterpret_cast<float4*>(d + q * V) = *reinterpret_cast<const float4*>(stg + q * V);
+            }
+        } else {
+            for (int q = tid; q < rows * (2 * L / V); q += NT) {
+                const int r = q / (2 * L / V), c = (q - r * (2 * L / V)) * V;
+                *reinterpret_cast<float4*>(d + r * a.dst_stride + c) = *reinterpret_cast<const float4*>(stg + r * RS + c);
+            }
+        }
     }
 }
 

@@ -10,6 +10,7 @@
 
 namespace pcxg {
 struct v2_args;
+struct v3_args;
 }
 
 // Record `msg` as this thread's last error and return `code`.
@@ -64,6 +65,7 @@ struct pcx_plan_s {
     void*  stw2     = nullptr;    // stage twiddles of the row pass (N2)
     void*  tw_b     = nullptr;    // W_{16*N2}^m, m < 16*N2
     int    sms      = 148;
+    int*   err      = nullptr;    // device flag: a bounded wait in a kernel gave up
 
     // four-step chunk pipeline: column passes on the caller's stream, row
     // passes on `side`, two scratch buffers
@@ -90,6 +92,7 @@ cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bo
 
 // Hot-path launches (pcx_v2_*.cu); cudaErrorNotSupported when no variant exists.
 cudaError_t pcx_v2_single(bool f64, int log_n, const pcxg::v2_args& a, cudaStream_t st, bool attr_only);
+cudaError_t pcx_v3_single(bool f64, int log_n, const pcxg::v3_args& a, cudaStream_t st, int sms, bool attr_only);
 cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only);
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,

@@ -150,6 +150,10 @@ class fft_unit:
     def dtype(self) -> torch.dtype:
         return self._dtype
 
+    def status(self) -> None:
+        """Raise TimeoutError if a kernel gave up a bounded wait (pcx_plan_status)."""
+        _lib.check(_lib.lib().pcx_plan_status(self._plan))
+
     def workspace_size(self, batch: int = 1) -> int:
         return int(_lib.lib().pcx_plan_workspace_size(self._plan, batch))
 
