@@ -236,6 +236,10 @@ static int plan_init_tables(pcx_plan_s* p) {
             if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
             e = pcx_v2_row(f64, p->log_n1, p->log_n2, z, 0, p->sms, true);
             if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+            e = pcx_v3_col(f64, p->log_n1, p->log_n2, z, 0, 0, nullptr, 0, p->sms, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
+            e = pcx_v3_row(f64, p->log_n1, p->log_n2, z, nullptr, 0, p->sms, true);
+            if (e != cudaErrorNotSupported) PCX_CUDA_TRY(e);
             PCX_CUDA_TRY(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
             for (int i = 0; i < 2; ++i) {
                 PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_col[i], cudaEventDisableTiming));
@@ -502,6 +506,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     const bool   direct = !(inv && p->order != 0);
     // hot-path eligibility of each pass
     const bool col_hot = direct && src_len == n && io.lp_src == lp_def;
+    const bool use_tma = std::getenv("PCX_NO_TMA") == nullptr;
     const bool row_hot = direct && io.order_out == 0 && io.lp_dst == lp_def;
 
     std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
@@ -531,6 +536,28 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
             // pass 1: columns src -> scratch (with twiddle); pass 2: rows scratch -> dst
             bool done = false;
             if (col_hot) {
+                v2_args c = h;
+                c.src        = src;
+                c.dst        = buf;
+                c.src_stride = (long long)sstride;
+                c.dst_stride = (long long)(2 * n);
+                c.batch      = rows;
+                c.conj_out   = 0;
+                c.scale      = 1.0;
+                c.stw        = p->stw1;
+                c.tw_hi      = p->tw_hi;
+                c.tw_lo      = p->tw_lo;
+                c.tw_b       = p->tw_b;
+                cudaError_t e = use_tma ? pcx_v3_col(f64, p->log_n1, p->log_n2, c, (long long)batch, (long long)r0,
+                                                     p->err, st, p->sms, false)
+                                        : cudaErrorNotSupported;
+                if (e != cudaErrorNotSupported) {
+                    PCX_CUDA_TRY(e);
+                    done = true;
+                }
+                c.src = s;
+            }
+            if (!done && col_hot) {
                 v2_args c = h;
                 c.src        = s;
                 c.dst        = buf;
@@ -567,7 +594,22 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
                 PCX_CUDA_TRY(cudaStreamWaitEvent(st2, p->ev_col[b], 0));
             }
             done = false;
-            if (row_hot) {
+            if (row_hot && use_tma) {
+                v2_args r = h;
+                r.src        = buf;
+                r.dst        = d;
+                r.src_stride = (long long)(2 * n);
+                r.dst_stride = (long long)dstride;
+                r.batch      = rows;
+                r.conj_in    = 0;
+                r.stw        = p->stw2;
+                cudaError_t e = pcx_v3_row(f64, p->log_n1, p->log_n2, r, p->err, st2, p->sms, false);
+                if (e != cudaErrorNotSupported) {
+                    PCX_CUDA_TRY(e);
+                    done = true;
+                }
+            }
+            if (!done && row_hot) {
                 v2_args r = h;
                 r.src        = buf;
                 r.dst        = d;

@@ -413,6 +413,7 @@ __global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
             const T        re = in[o], im = in[o + PK];
             v[i]              = {re, a.conj_in ? -im : im};
         });
+        fence_proxy_async_smem();
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < ntile) issue(tile + 2 * (long long)gridDim.x, s);
         stage_compute_tab<P, 0>(v, t, stw);
@@ -446,6 +447,231 @@ __global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
             }
         }
     }
+}
+
+}    // namespace pcxg
+
+namespace pcxg {
+
+// ===========================================================================
+// TMA-fed four-step passes.  Same arithmetic as k_col2 / k_row2; the input
+// tiles arrive in shared memory through a two-stage bulk-copy ring
+// (column pass: 3-D tensor copies of N1 x 64-byte row segments; row pass:
+// one bulk copy per scratch row into padded rows), outputs are written from
+// registers as in the direct kernels.
+
+// Read (re, im) stored `pk_off` reals apart at `o`; lanes with bit SW set
+// fetch the imaginary part first, so the two halves of each shared-memory
+// wavefront hit disjoint banks.
+template<class T, int SW>
+__device__ __forceinline__ cpx<T> lds_swapped(const T* base, int o, int pk_off) {
+    const bool sw = (threadIdx.x & SW) != 0;
+    const T    x0 = base[o + (sw ? pk_off : 0)];
+    const T    x1 = base[o + (sw ? 0 : pk_off)];
+    return {sw ? x1 : x0, sw ? x0 : x1};
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct v3_pass_args {
+    v2_args   base;
+    long long row0;    // first batch row of this launch in the tensor map (column pass)
+    int*      error;
+};
+
+template<class T, int LOGN1>
+__host__ __device__ constexpr int col3_boxy() {
+    return (1 << LOGN1) < 256 ? (1 << LOGN1) : 256;
+}
+
+template<class T, int LOGN1, int LOGN2, int LP, int C, int NT>
+__global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensorMap tmap, v3_pass_args pa) {
+    using P            = splan<LOGN1>;
+    constexpr int N1   = P::L;
+    constexpr int N2   = 1 << LOGN2;
+    constexpr int E    = P::E;
+    constexpr int TT   = P::TT;
+    constexpr int PK   = 1 << LP;
+    constexpr int TPR  = N2 / C;
+    constexpr int SEG  = 2 * C;                // reals per row segment
+    constexpr int TILE = N1 * SEG;             // reals per stage
+    constexpr int BOXY = col3_boxy<T, LOGN1>();
+    constexpr int SW   = sizeof(T) == 8 ? 8 : 16;
+    static_assert(NT == C * TT, "threads");
+    using X = xch_interleaved<N1, C>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    T*                  in0 = reinterpret_cast<T*>(smem);
+    cpx<T>*             xch = reinterpret_cast<cpx<T>*>(in0 + 2 * TILE);
+    __shared__ uint64_t full[2];
+    const v2_args&      a   = pa.base;
+    const auto*         stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const auto*         thi = reinterpret_cast<const cpx<T>*>(a.tw_hi);
+    const auto*         tlo = reinterpret_cast<const cpx<T>*>(a.tw_lo);
+    const auto*         tb  = reinterpret_cast<const cpx<T>*>(a.tw_b);
+    const int           tid = threadIdx.x;
+    const int           c   = tid % C;
+    const int           t   = tid / C;
+    const long long     tiles = a.batch * TPR;
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long tile, int s) {
+        const long long row = tile / TPR;
+        const int       c0  = (int)(tile - row * TPR) * C;
+        T*              buf = in0 + s * TILE;
+        mbar_arrive_expect_tx(&full[s], TILE * (int)sizeof(T));
+#pragma unroll
+        for (int y = 0; y < N1; y += BOXY) tma_load_3d(buf + y * SEG, &tmap, 2 * c0, y, (int)(pa.row0 + row), &full[s]);
+    };
+    if (tid == 0) {
+        if ((long long)blockIdx.x < tiles) issue(blockIdx.x, 0);
+        if ((long long)blockIdx.x + gridDim.x < tiles) issue(blockIdx.x + gridDim.x, 1);
+    }
+    long long k = 0;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+        const int      s   = (int)(k & 1);
+        const uint32_t par = (uint32_t)((k >> 1) & 1);
+        const bool     ok  = mbar_wait_bounded(&full[s], par);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(pa.error, 1);
+                mbar_wait_bounded(&full[s], par, 100000000ull);
+                mbar_wait_bounded(&full[s ^ 1], par ^ (s ? 1u : 0u), 100000000ull);
+            }
+            __syncthreads();
+            return;
+        }
+        const long long row = tile / TPR;
+        const int       c0  = (int)(tile - row * TPR) * C;
+        const int       n2  = c0 + c;
+        const T*        in  = in0 + s * TILE;
+        cpx<T>          v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            cpx<T>        x = lds_swapped<T, SW>(in, (t + i * TT) * SEG + pk<LP>(c), PK);
+            v[i]            = {x.re, a.conj_in ? -x.im : x.im};
+        });
+        fence_proxy_async_smem();
+        __syncthreads();    // stage s consumed: refill it with the tile after next
+        if (tid == 0 && tile + 2 * (long long)gridDim.x < tiles) issue(tile + 2 * (long long)gridDim.x, s);
+        stage_compute_tab<P, 0>(v, t, stw);
+        run_stages_tab<P, X>(v, xch, c, t, stw);
+        const uint32_t e0   = (uint32_t)t * (uint32_t)n2;
+        const cpx<T>   base = cmul(ldg_cpx(thi + (e0 >> LOGN2)), ldg_cpx(tlo + (e0 & (N2 - 1))));
+        cpx<T>*        dst  = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            cpx<T>        w = base;
+            if constexpr (i > 0) w = cmul(base, ldg_cpx(tb + ((i * n2) & (16 * N2 - 1))));
+            dst[(long long)i * TT * N2] = cmul(v[i], w);
+        });
+    }
+}
+
+template<class T, int LOGN1, int C>
+__host__ __device__ constexpr int col3_smem() {
+    return 2 * (1 << LOGN1) * 2 * C * (int)sizeof(T) + xch_interleaved<(1 << LOGN1), C>::size * (int)sizeof(cpx<T>);
+}
+
+template<class T, int LOGN1, int LOGN2, int LP, int CR, int G8, int NT>
+__global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
+    using P            = splan<LOGN2>;
+    constexpr int N1   = 1 << LOGN1;
+    constexpr int N2   = P::L;
+    constexpr int E    = P::E;
+    constexpr int TT   = P::TT;
+    constexpr int PK   = 1 << LP;
+    constexpr int TPR  = N1 / CR;
+    constexpr int RSI  = N2 + 2;               // padded shared row (complex)
+    constexpr int TILE = CR * RSI;             // complex per stage
+    constexpr int ROWB = N2 * (int)sizeof(cpx<T>);
+    static_assert(NT == CR * TT, "threads");
+    using X = xch_grouped<N2, CR, G8>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    cpx<T>*             in0 = reinterpret_cast<cpx<T>*>(smem);
+    cpx<T>*             xch = in0 + 2 * TILE;
+    __shared__ uint64_t full[2];
+    const v2_args&      a   = pa.base;
+    const auto*         stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    const int           tid = threadIdx.x;
+    const int           mlo = tid % G8;
+    const int           t   = (tid / G8) % TT;
+    const int           mhi = tid / (G8 * TT);
+    const int           m   = mhi * G8 + mlo;
+    const long long     tiles = a.batch * TPR;
+    const cpx<T>*       src = reinterpret_cast<const cpx<T>*>(a.src);
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long tile, int s) {
+        const long long row = tile / TPR;
+        const int       r0  = (int)(tile - row * TPR) * CR;
+        cpx<T>*         buf = in0 + s * TILE;
+        const cpx<T>*   g   = src + row * (a.src_stride / 2) + (long long)r0 * N2;
+        mbar_arrive_expect_tx(&full[s], CR * ROWB);
+        for (int r = 0; r < CR; ++r) bulk_g2s(buf + r * RSI, g + (long long)r * N2, ROWB, &full[s]);
+    };
+    if (tid == 0) {
+        if ((long long)blockIdx.x < tiles) issue(blockIdx.x, 0);
+        if ((long long)blockIdx.x + gridDim.x < tiles) issue(blockIdx.x + gridDim.x, 1);
+    }
+    long long k = 0;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+        const int      s   = (int)(k & 1);
+        const uint32_t par = (uint32_t)((k >> 1) & 1);
+        const bool     ok  = mbar_wait_bounded(&full[s], par);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(pa.error, 1);
+                mbar_wait_bounded(&full[s], par, 100000000ull);
+                mbar_wait_bounded(&full[s ^ 1], par ^ (s ? 1u : 0u), 100000000ull);
+            }
+            __syncthreads();
+            return;
+        }
+        const long long row = tile / TPR;
+        const int       r0  = (int)(tile - row * TPR) * CR;
+        const int       k1  = r0 + m;
+        const cpx<T>*   in  = in0 + s * TILE + m * RSI + t;
+        cpx<T>          v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = in[i * TT];
+        });
+        fence_proxy_async_smem();
+        __syncthreads();    // stage s consumed: refill it with the tile after next
+        if (tid == 0 && tile + 2 * (long long)gridDim.x < tiles) issue(tile + 2 * (long long)gridDim.x, s);
+        stage_compute_tab<P, 0>(v, t, stw);
+        run_stages_tab<P, X>(v, xch, m, t, stw);
+        T*      dst = reinterpret_cast<T*>(a.dst) + row * a.dst_stride + pk<LP>(t * N1 + k1);
+        const T sc  = T(a.scale);
+        const T sim = a.conj_out ? -sc : sc;
+        static_for<E>([&](auto ic) {
+            constexpr int i           = decltype(ic)::value;
+            dst[2 * i * TT * N1]      = v[i].re * sc;
+            dst[2 * i * TT * N1 + PK] = v[i].im * sim;
+        });
+    }
+}
+
+template<class T, int LOGN2, int CR, int G8>
+__host__ __device__ constexpr int row3_smem() {
+    return 2 * CR * ((1 << LOGN2) + 2) * (int)sizeof(cpx<T>) +
+           xch_grouped<(1 << LOGN2), CR, G8>::size * (int)sizeof(cpx<T>);
 }
 
 }    // namespace pcxg

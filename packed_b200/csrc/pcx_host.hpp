@@ -97,6 +97,10 @@ cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a,
                        bool attr_only);
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only);
+cudaError_t pcx_v3_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, long long total_rows, long long row0,
+                       int* err, cudaStream_t st, int sms, bool attr_only);
+cudaError_t pcx_v3_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, int* err, cudaStream_t st, int sms,
+                       bool attr_only);
 // Stage-twiddle table of an L = 2^log_l point transform: *entries complex
 // values; generated into `out` unless it is null.
 cudaError_t pcx_v2_stage_twiddles(int log_l, void* out, bool f64, cudaStream_t st, int* entries);

@@ -3,6 +3,7 @@
 // own shared memory and one global address.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -50,6 +51,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (timer_ns() - t0 > limit_ns) return false;
     }
     return true;
+}
+
+// Order this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy (TMA) accesses to the same memory.  Every thread that
+// read a stage runs it before the barrier that precedes the refill.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // 1-D bulk copy global -> shared (16-byte aligned addresses, size multiple

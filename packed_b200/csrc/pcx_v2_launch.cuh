@@ -32,4 +32,24 @@ inline cudaError_t persistent_grid(K kern, int nt, int bytes, long long tiles, i
     return cudaSuccess;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+inline cudaError_t encode_tensor_map(CUtensorMap* map, bool f64, int rank, void* base, const cuuint64_t* dims,
+                                     const cuuint64_t* strides, const cuuint32_t* box, const cuuint32_t* estr) {
+    using fn_t     = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static fn_t fn = nullptr;
+    if (!fn) {
+        void*                           p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || !p) return e != cudaSuccess ? e : cudaErrorNotSupported;
+        fn = reinterpret_cast<fn_t>(p);
+    }
+    const CUresult r = fn(map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base, dims,
+                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 }    // namespace pcxg

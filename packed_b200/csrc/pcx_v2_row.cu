@@ -35,7 +35,46 @@ static cudaError_t dispatch(int l1, int l2, const v2_args& a, cudaStream_t st, i
     }
 }
 
+template<class T, int LOGN1, int LOGN2>
+static cudaError_t launch3(const v2_args& a, int* err, cudaStream_t st, int sms, bool attr_only) {
+    constexpr int G8    = v2cfg<T>::G8;
+    constexpr int CR    = std::max(G8, v2cfg<T>::TILE >> LOGN2);
+    constexpr int NT    = CR * splan<LOGN2>::TT;
+    constexpr int bytes = row3_smem<T, LOGN2, CR, G8>();
+    auto          kern  = k_row3<T, LOGN1, LOGN2, v2cfg<T>::LP, CR, G8, NT>;
+    if (attr_only) return set_smem(kern, bytes);
+    const long long tiles = a.batch * ((1 << LOGN1) / CR);
+    if (tiles == 0) return cudaSuccess;
+    unsigned    grid = 0;
+    cudaError_t e    = persistent_grid(kern, NT, bytes, tiles, sms, &grid);
+    if (e != cudaSuccess) return e;
+    v3_pass_args pa{a, 0, err};
+    kern<<<grid, NT, bytes, st>>>(pa);
+    return cudaGetLastError();
+}
+
+template<class T>
+static cudaError_t dispatch3(int l1, int l2, const v2_args& a, int* err, cudaStream_t st, int sms, bool attr_only) {
+    switch (l1 * 32 + l2) {
+    case 7 * 32 + 6: return launch3<T, 7, 6>(a, err, st, sms, attr_only);
+    case 7 * 32 + 7: return launch3<T, 7, 7>(a, err, st, sms, attr_only);
+    case 8 * 32 + 7: return launch3<T, 8, 7>(a, err, st, sms, attr_only);
+    case 8 * 32 + 8: return launch3<T, 8, 8>(a, err, st, sms, attr_only);
+    case 9 * 32 + 8: return launch3<T, 9, 8>(a, err, st, sms, attr_only);
+    case 9 * 32 + 9: return launch3<T, 9, 9>(a, err, st, sms, attr_only);
+    case 10 * 32 + 9: return launch3<T, 10, 9>(a, err, st, sms, attr_only);
+    case 10 * 32 + 10: return launch3<T, 10, 10>(a, err, st, sms, attr_only);
+    default: return cudaErrorNotSupported;
+    }
+}
+
 }    // namespace pcxg
+
+cudaError_t pcx_v3_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, int* err, cudaStream_t st, int sms,
+                       bool attr_only) {
+    return f64 ? pcxg::dispatch3<double>(log_n1, log_n2, a, err, st, sms, attr_only)
+               : pcxg::dispatch3<float>(log_n1, log_n2, a, err, st, sms, attr_only);
+}
 
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only) {
