@@ -1,17 +1,26 @@
-"""Benchmark of the batched FP32 FFT size sweep (packed split-complex, pack 8).
-
-Workload (one step): for every N = 2^6 .. 2^20, a forward and an inverse
-(1/N) transform over a 1 GiB buffer of complex64 (batch = 2^27 / N rows),
-N(0,1) synthetic data, out of place between two resident 1 GiB buffers (each
-larger than the 126 MB L2, so no L2 flush is needed between iterations).
-
-metric: algorithmic GB/s = 16 B per complex point per direction / time.
+"""Benchmarks of the packed FFT / correlation hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c3|c5]
 
-Multi-GPU (torchrun, one rank per GPU): every rank runs the same sweep on its
-own buffers (independent transforms, no collective on the data path: weak
-scaling); the step time is the max over ranks.
+Workloads (synthetic data, N(0,1) unless stated; all buffers stay resident in
+HBM and are larger than the 126 MB L2, so no flush is needed between steps):
+
+  c2 (default)  FP32 FFT size sweep: for every N = 2^6..2^20 a forward and an
+                inverse (1/N) transform over a 1 GiB complex64 buffer (batch
+                2^27/N), pack 8 split-complex, natural order, out of place.
+  c1            N=1024, batch 64, forward then inverse (U[-1,1), seed 0).
+  c3            fxcorr: 256 channels x 2^20 complex64 samples correlated in place
+                with a 4096-tap kernel (sigma 1/64) by overlap-save, N_fft 16384.
+  c5            ragged batch: 10,000 FFTs, N log-uniform 2^8..2^18, plus 500
+                correlations (S 2^12..2^20, K 64..8192), one persistent launch
+                replayed from a CUDA graph, against per-size plain launches.
+
+metric: algorithmic GB/s = 16 B per complex point per direction (c2, c1, c5)
+or 16 B per signal sample (c3), divided by the device time of the step.
+Multi-GPU (torchrun, one rank per GPU): every rank runs the same workload on
+its own buffers (independent transforms, no collective: weak scaling); the
+step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -31,9 +40,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "FP32 FFT/fxcorr GB/s, % of HBM peak; tensor-core vs plain at ≤2e-6 rel err"
-LOG_NS = list(range(6, 21))
-POINTS = 1 << 27    # complex64 points per 1 GiB buffer (overridable by --points for profiling captures)
-BYTES_PER_POINT_DIR = 16
+B_PT = 16    # algorithmic bytes per complex point per direction (read + write complex64)
 
 
 def peaks() -> dict:
@@ -53,103 +60,257 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.samples: list[list[str]] = []
-        self._stop = threading.Event()
-        self._t = threading.Thread(target=self._run, daemon=True)
+        self._proc = None
+        self._t = None
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            for line in self._proc.stdout:
+                self.samples.append([s.strip() for s in line.strip().split(",")])
+        except Exception:
+            pass
 
     def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        time.sleep(0.15)
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=5)
 
     def summary(self) -> dict:
-        if not self.samples:
+        rows = [s for s in self.samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in rows]
+        mx = [float(s[1]) for s in rows if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        reasons = sorted({names[i] for s in rows for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
 
 
-# --------------------------------------------------------------- CPU leg
-def cpu_reference(budget_s: float = 12.0) -> dict:
-    """The reference fft_unit<float> (compiled from its headers) on the host
-    cores: a bounded sample of every size of the sweep, forward + inverse."""
-    import oracle as O
-    if not O.ref_available():
-        return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/libpcx_ref.so not built"}
-    import ctypes
-    threads = O.host_threads()
-    fp = ctypes.POINTER(ctypes.c_float)
-    per_size = budget_s / len(LOG_NS)
-    tot_bytes, tot_t, rows_used = 0.0, 0.0, {}
-    rng = np.random.default_rng(1)
-    for lg in LOG_NS:
-        n = 1 << lg
-        rows = max(threads, min((POINTS // n), (1 << 22) // n))
-        data = rng.standard_normal(rows * 2 * n).astype(np.float32)
-        ptr = data.ctypes.data_as(fp)
-        # one calibration pass, then as many passes as fit the per-size budget
-        t0 = time.perf_counter()
-        O.ref().ref_fft_batch_f32(0, n, rows, ptr, 0, threads)
-        O.ref().ref_fft_batch_f32(0, n, rows, ptr, 1, threads)
-        dt = time.perf_counter() - t0
-        reps = max(1, int(per_size / max(dt, 1e-6)) - 1)
-        t0 = time.perf_counter()
-        for _ in range(reps):
+# --------------------------------------------------------------- workloads
+class C2Sweep:
+    name = "c2"
+    log_ns = list(range(6, 21))
+    points = 1 << 27
+
+    def config(self, world):
+        return {"workload": "C2 FP32 FFT size sweep: N=2^6..2^20, 1 GiB complex64 per size (batch 2^27/N), "
+                            "fwd+inv(1/N), pack 8 split-complex, natural order, out of place",
+                "sizes": [1 << lg for lg in self.log_ns], "global_batch_points": self.points * world,
+                "l2": "inputs 1 GiB > L2 (no flush needed)", "parallelism": f"independent shards x{world}"}
+
+    def setup(self, dev, rank):
+        import torch
+        from packed_b200 import fft_unit
+        g = torch.Generator(device=dev).manual_seed(1 + rank)
+        self.x = torch.randn(2 * self.points, device=dev, generator=g)
+        self.y = torch.empty_like(self.x)
+        self.units = {lg: fft_unit(1 << lg) for lg in self.log_ns}
+
+    def bytes_per_step(self):
+        return len(self.log_ns) * self.points * B_PT * 2
+
+    def parts(self):
+        return [str(1 << lg) for lg in self.log_ns]
+
+    def run_part(self, key):
+        lg = int(key).bit_length() - 1
+        b = self.points >> lg
+        self.units[lg].exec(self.y, self.x, batch=b, direction=0)
+        self.units[lg].exec(self.x, self.y, batch=b, direction=1)
+
+    def part_bytes(self, key):
+        return self.points * B_PT * 2
+
+    def e2e(self, torch, stream):
+        host_in = torch.empty(2 * self.points, dtype=torch.float32).pin_memory()
+        host_in.copy_(self.x.cpu())
+        host_out = torch.empty_like(host_in).pin_memory()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for lg in self.log_ns:
+            self.x.copy_(host_in, non_blocking=True)
+            self.run_part(str(1 << lg))
+            host_out.copy_(self.x, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        nb = 2 * self.points * 4 * len(self.log_ns)
+        return {"value": self.bytes_per_step() / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nb,
+                "d2h_bytes_per_step": nb, "ms_per_step": ms}
+
+    def launches(self):
+        total = 0
+        for lg, u in self.units.items():
+            b = self.points >> lg
+            if lg <= 12:
+                total += 2
+            else:
+                ws = u.workspace_size(b)
+                chunk = max(1, ws // (2 * (1 << lg) * 8))
+                total += 2 * 2 * ((b + chunk - 1) // chunk)
+        return total
+
+    def cpu_reference(self, budget_s=12.0):
+        import ctypes
+        import oracle as O
+        if not O.ref_available():
+            return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref/libpcx_ref.so not built"}
+        threads = O.host_threads()
+        fp = ctypes.POINTER(ctypes.c_float)
+        per = budget_s / len(self.log_ns)
+        tot_b, tot_t = 0.0, 0.0
+        rng = np.random.default_rng(1)
+        for lg in self.log_ns:
+            n = 1 << lg
+            rows = max(threads, min(self.points >> lg, (1 << 22) >> lg))
+            data = rng.standard_normal(rows * 2 * n).astype(np.float32)
+            ptr = data.ctypes.data_as(fp)
+            t0 = time.perf_counter()
             O.ref().ref_fft_batch_f32(0, n, rows, ptr, 0, threads)
             O.ref().ref_fft_batch_f32(0, n, rows, ptr, 1, threads)
+            reps = max(1, int(per / max(time.perf_counter() - t0, 1e-6)) - 1)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                O.ref().ref_fft_batch_f32(0, n, rows, ptr, 0, threads)
+                O.ref().ref_fft_batch_f32(0, n, rows, ptr, 1, threads)
+            tot_t += time.perf_counter() - t0
+            tot_b += reps * rows * n * B_PT * 2
+        return {"value": tot_b / tot_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
+                "sample": f"reference fft_unit<float> (oracle/_ref) normal order fwd+inv on {threads} threads, "
+                          f"per N in 2^6..2^20 a batch of max({threads}, 2^22/N) rows repeated for ~{per:.1f} s"}
+
+
+class C1(C2Sweep):
+    name = "c1"
+    log_ns = [10]
+    points = 1024 * 64
+
+    def config(self, world):
+        return {"workload": "C1: N=1024, batch 64, forward then inverse (1/N), pack 8, U[-1,1) seed 0",
+                "global_batch_points": self.points * world, "l2": "1 MiB working set (L2 resident: latency-bound)",
+                "parallelism": f"independent shards x{world}"}
+
+    def setup(self, dev, rank):
+        import torch
+        from packed_b200 import fft_unit
+        rng = np.random.default_rng(0)
+        z = rng.uniform(-1, 1, (64, 1024)) + 1j * rng.uniform(-1, 1, (64, 1024))
+        a = np.zeros((64, 128, 2, 8), np.float32)
+        a[:, :, 0, :] = z.real.reshape(64, 128, 8)
+        a[:, :, 1, :] = z.imag.reshape(64, 128, 8)
+        self.x = torch.as_tensor(a.reshape(-1)).to(dev)
+        self.y = torch.empty_like(self.x)
+        self.units = {10: fft_unit(1024)}
+
+
+class C3Fxcorr:
+    name = "c3"
+    channels, length, k, n_fft = 256, 1 << 20, 4096, 16384
+
+    def config(self, world):
+        return {"workload": "C3 fxcorr: 256 channels x 2^20 complex64 (N(0,1) seed 2), 4096-tap kernel "
+                            "(N(0,1/4096) seed 3), overlap-save N_fft 16384 (step 12288), in place, pack 8",
+                "global_batch_points": self.channels * self.length * world,
+                "l2": "2 GiB signal > L2 (no flush needed)", "parallelism": f"independent shards x{world}"}
+
+    def setup(self, dev, rank):
+        import torch
+        from packed_b200 import fxcorr_unit, vector
+        g = torch.Generator(device=dev).manual_seed(2 + rank)
+        self.x = torch.randn(self.channels * 2 * self.length, device=dev, generator=g)
+        rng = np.random.default_rng(3)
+        taps = (rng.standard_normal(self.k) + 1j * rng.standard_normal(self.k)) / 64
+        self.unit = fxcorr_unit(vector.from_complex(taps, device=dev), self.n_fft)
+
+    def bytes_per_step(self):
+        return self.channels * self.length * B_PT
+
+    def parts(self):
+        return ["fxcorr"]
+
+    def run_part(self, key):
+        self.unit.exec(self.x, self.x, self.length, channels=self.channels)
+
+    def part_bytes(self, key):
+        return self.bytes_per_step()
+
+    def e2e(self, torch, stream):
+        host = torch.empty_like(self.x, device="cpu").pin_memory()
+        host.copy_(self.x.cpu())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        self.x.copy_(host, non_blocking=True)
+        self.run_part("fxcorr")
+        host.copy_(self.x, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        nb = self.x.numel() * 4
+        return {"value": self.bytes_per_step() / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nb,
+                "d2h_bytes_per_step": nb, "ms_per_step": ms}
+
+    def launches(self):
+        return 1
+
+    def cpu_reference(self, budget_s=12.0):
+        import ctypes
+        import oracle as O
+        if not O.ref_available():
+            return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref/libpcx_ref.so not built"}
+        threads = O.host_threads()
+        fp = ctypes.POINTER(ctypes.c_float)
+        rng = np.random.default_rng(3)
+        taps = ((rng.standard_normal(self.k) + 1j * rng.standard_normal(self.k)) / 64).astype(np.complex64)
+        g = O.pack(taps, 8)
+        ch = max(threads, 8)
+        sig = np.random.default_rng(2).standard_normal(ch * 2 * self.length).astype(np.float32)
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            O.ref().ref_fxcorr_fixed_batch_f32(g.ctypes.data_as(fp), self.k, self.n_fft, sig.ctypes.data_as(fp),
+                                               self.length, ch, threads)
+            reps += 1
+            if time.perf_counter() - t0 > budget_s / 2:
+                break
         dt = time.perf_counter() - t0
-        tot_t += dt
-        tot_bytes += reps * rows * n * BYTES_PER_POINT_DIR * 2
-        rows_used[n] = rows * reps
-    return {"value": tot_bytes / tot_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-            "sample": f"fft_unit<float> normal order fwd+inv, per N in 2^6..2^20 a batch of "
-                      f"max({threads}, 2^22/N) rows repeated for ~{per_size:.1f} s "
-                      f"({sum(rows_used.values())} transforms pairs total)"}
+        return {"value": reps * ch * self.length * B_PT / dt / 1e9, "unit": "GB/s", "cores": threads,
+                "kind": "reference",
+                "sample": f"reference fft_unit<float, unordered> overlap-save (offsets corrected) on {threads} "
+                          f"threads, {ch} channels x 2^20 x {reps} repetitions"}
 
 
-# --------------------------------------------------------------- GPU leg
-def run_gpu(args, rank: int, world: int) -> dict | None:
+WORKLOADS = {"c2": C2Sweep, "c1": C1, "c3": C3Fxcorr}
+
+
+# ----------------------------------------------------------------- driver
+def run(args, wl, rank, world):
     import torch
     import torch.distributed as dist
-    from packed_b200 import fft_unit
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    g = torch.Generator(device=dev).manual_seed(1 + rank)
-    reals = 2 * POINTS
-    x = torch.randn(reals, device=dev, generator=g)
-    y = torch.empty_like(x)
-    units = {lg: fft_unit(1 << lg) for lg in LOG_NS}
+    wl.setup(dev, rank)
     stream = torch.cuda.current_stream()
-
-    def step(events=None):
-        for lg in LOG_NS:
-            n = 1 << lg
-            b = POINTS // n
-            if events is not None:
-                events[lg][0].record(stream)
-            units[lg].exec(y, x, batch=b, direction=0)
-            units[lg].exec(x, y, batch=b, direction=1)
-            if events is not None:
-                events[lg][1].record(stream)
 
     def barrier():
         if world > 1:
@@ -157,67 +318,34 @@ def run_gpu(args, rank: int, world: int) -> dict | None:
         torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        step()
+        for p in wl.parts():
+            wl.run_part(p)
     barrier()
-    per = {lg: [] for lg in LOG_NS}
+    per = {p: [] for p in wl.parts()}
     with ClockSampler(dev.index) as clk:
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        ev = [{p: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for p in wl.parts()}
+              for _ in range(args.steps)]
         barrier()
-        t_start.record(stream)
-        for _ in range(args.steps):
-            ev = {lg: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for lg in LOG_NS}
-            step(ev)
-            torch.cuda.synchronize()
-            for lg in LOG_NS:
-                per[lg].append(ev[lg][0].elapsed_time(ev[lg][1]))
-        t_end.record(stream)
+        t0.record(stream)
+        for s in range(args.steps):
+            for p in wl.parts():
+                ev[s][p][0].record(stream)
+                wl.run_part(p)
+                ev[s][p][1].record(stream)
+        t1.record(stream)
         barrier()
-    ms = t_start.elapsed_time(t_end)
+    ms = t0.elapsed_time(t1)
+    for s in range(args.steps):
+        for p in wl.parts():
+            per[p].append(ev[s][p][0].elapsed_time(ev[s][p][1]))
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = t.item()
-    clocks = clk.summary()
-
-    # e2e through the public API with host buffers: per size one batch of the
-    # same 1 GiB, pinned host -> device, forward + inverse, device -> host
-    e2e = None
-    if rank == 0:
-        host_in = torch.empty(reals, dtype=torch.float32).pin_memory()
-        host_in.copy_(x.cpu())
-        host_out = torch.empty_like(host_in).pin_memory()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for lg in LOG_NS:
-            n = 1 << lg
-            x.copy_(host_in, non_blocking=True)
-            units[lg].exec(y, x, batch=POINTS // n, direction=0)
-            units[lg].exec(x, y, batch=POINTS // n, direction=1)
-            host_out.copy_(x, non_blocking=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1)
-        e2e_bytes = len(LOG_NS) * POINTS * BYTES_PER_POINT_DIR * 2
-        e2e = {"value": e2e_bytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
-               "h2d_bytes_per_step": reals * 4 * len(LOG_NS), "d2h_bytes_per_step": reals * 4 * len(LOG_NS),
-               "ms_per_step": e2e_ms}
-    bytes_step = len(LOG_NS) * POINTS * BYTES_PER_POINT_DIR * 2 * world
-    return {"ms": ms, "per": per, "bytes_step": bytes_step, "clocks": clocks, "e2e": e2e, "units": units}
-
-
-def launches_per_step(units) -> int:
-    total = 0
-    for lg, u in units.items():
-        n = 1 << lg
-        b = POINTS // n
-        if lg <= 12:
-            total += 2
-        else:
-            chunk = max(1, u.workspace_size(b) // (n * 8))
-            total += 2 * 2 * ((b + chunk - 1) // chunk)
-    return total
+    e2e = wl.e2e(torch, stream) if rank == 0 else None
+    return {"ms": ms, "per": per, "clocks": clk.summary(), "e2e": e2e}
 
 
 def main() -> None:
@@ -226,34 +354,32 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--points", type=int, default=27, help="log2 complex points per buffer (profiling captures)")
+    ap.add_argument("--points", type=int, default=None, help="log2 complex points per buffer (profiling captures)")
     ap.add_argument("--sizes", type=str, default=None, help="comma list of log2 N (profiling captures)")
     args = ap.parse_args()
-    global POINTS, LOG_NS
-    POINTS = 1 << args.points
-    if args.sizes:
-        LOG_NS = [int(v) for v in args.sizes.split(",")]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    config = {"workload": "C2 FP32 FFT size sweep: N=2^6..2^20, 1 GiB complex64 per size (batch 2^27/N), "
-                          "fwd+inv(1/N), pack 8 split-complex, natural order, out of place",
-              "global_batch_points": POINTS * world, "sizes": [1 << lg for lg in LOG_NS],
-              "l2": "inputs 1 GiB > L2 (no flush needed)", "parallelism": f"independent shards x{world}"}
+    wl = WORKLOADS[args.workload]()
+    if args.points is not None and hasattr(wl, "points"):
+        wl.points = 1 << args.points
+    if args.sizes and hasattr(wl, "log_ns"):
+        wl.log_ns = [int(v) for v in args.sizes.split(",")]
+    config = wl.config(world)
 
     if args.impl == "reference":
         if rank != 0:
             return
-        times = []
-        cb = None
+        vals, cb = [], None
         for i in range(args.warmup + args.steps):
-            cb = cpu_reference(budget_s=max(3.0, 12.0 / max(1, args.steps)))
+            cb = wl.cpu_reference(budget_s=max(3.0, 60.0 / max(1, args.warmup + args.steps)))
             if i >= args.warmup:
-                times.append(cb["value"])
-        v = statistics.median(times) if times and times[0] else None
+                vals.append(cb["value"])
+        v = statistics.median(vals) if vals and vals[0] is not None else None
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1)", "config": config,
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "cpu_baseline": {**cb, "value": v},
                 "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -265,7 +391,7 @@ def main() -> None:
         from datetime import timedelta
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = run_gpu(args, rank, world)
+    res = run(args, wl, rank, world)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -273,31 +399,28 @@ def main() -> None:
         return
     pk = peaks()
     ms_step = res["ms"] / args.steps
-    value = res["bytes_step"] / (ms_step / 1e3) / 1e9
-    # dominant kernel family: the size with the largest share of the step
-    mean = {lg: statistics.mean(v) for lg, v in res["per"].items()}
+    value = wl.bytes_per_step() * world / (ms_step / 1e3) / 1e9
+    mean = {p: statistics.mean(v) for p, v in res["per"].items()}
     top = max(mean, key=mean.get)
-    alg = POINTS * BYTES_PER_POINT_DIR * 2
-    ach = alg / (mean[top] / 1e3) / 1e9
-    per_size = {str(1 << lg): round(alg / (mean[lg] / 1e3) / 1e9, 1) for lg in LOG_NS}
+    ach = wl.part_bytes(top) / (mean[top] / 1e3) / 1e9
+    per_part = {p: round(wl.part_bytes(p) / (mean[p] / 1e3) / 1e9, 1) for p in wl.parts()}
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
-        traffic = json.loads(tp.read_text()).get(str(1 << top))
+        traffic = json.loads(tp.read_text()).get(f"{wl.name}:{top}")
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1), seed 1+rank", "config": config,
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
         "pct_hbm": 100.0 * value / world / pk["hbm_gbs"],
-        "per_size_gbs": per_size,
+        "per_part_gbs": per_part,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": traffic, "peak_src": pk["src"],
-                     "kernel": f"N={1 << top} fwd+inv ({'single-pass' if top <= 12 else 'four-step'})",
-                     "algorithmic_bytes_per_launch": alg // 2},
-        "clocks": res["clocks"], "e2e": res["e2e"], "gpu_launches": launches_per_step(res["units"]) * args.steps,
+                     "kernel": f"{wl.name}:{top}", "algorithmic_bytes": wl.part_bytes(top)},
+        "clocks": res["clocks"], "e2e": res["e2e"], "gpu_launches": wl.launches() * args.steps,
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference()
+        line["cpu_baseline"] = wl.cpu_reference()
     print(json.dumps(line))
 
 

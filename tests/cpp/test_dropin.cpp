@@ -3,6 +3,7 @@
 // and run on the GPU.  Exit status 0 on success.
 #include "pcxo/fft.hpp"
 #include "pcxo/fxcorr.hpp"
+#include "pcxo/mdstorage.hpp"
 
 #include <cmath>
 #include <complex>
@@ -105,6 +106,51 @@ int main() {
         expect(rel_err(dst, y) < 2e-6, "fxcorr_unit(dest, src)", rel_err(dst, y));
         xc(f);
         expect(rel_err(f, y) < 2e-6, "fxcorr_unit(vector) in place", rel_err(f, y));
+    }
+    {    // md::dynamic_storage (mdstorage.hpp): rows as vectors and batched row transforms
+        enum class ax { x, y, z };
+        using enum ax;
+        constexpr auto basis = pcxo::md::left_basis<x, y, z>{};
+        const unsigned nx = 1000, ny = 3, nz = 5;    // inner axis x, padded to whole packs
+        auto           st = pcxo::md::dynamic_storage<float, basis>(nx, ny, nz);
+        expect(st.extent<x>() == nx && st.extent<z>() == nz && st.row_stride() == 2000, "md storage extents / padding");
+        std::vector<std::vector<cd>> rows;
+        for (unsigned k = 0; k < nz; ++k) {
+            for (unsigned j = 0; j < ny; ++j) {
+                auto row = st.slice<z>(k).slice<y>(j);
+                std::vector<cd> r(nx);
+                for (unsigned i = 0; i < nx; ++i) {
+                    r[i]   = cd(u(rng), u(rng));
+                    row[i] = r[i];
+                }
+                rows.push_back(r);
+            }
+        }
+        // nx = 1000 is not a power of two: use the first 512 points of every row via a 512-point storage
+        auto st2 = pcxo::md::dynamic_storage<float, basis>(512u, ny, nz);
+        std::vector<std::vector<cd>> want;
+        for (unsigned k = 0, q = 0; k < nz; ++k) {
+            for (unsigned j = 0; j < ny; ++j, ++q) {
+                auto row = st2.slice<z>(k).slice<y>(j);
+                std::vector<cd> r(rows[q].begin(), rows[q].begin() + 512);
+                for (unsigned i = 0; i < 512; ++i) row[i] = r[i];
+                want.push_back(dft(r, -1));
+            }
+        }
+        pcxo::fft_unit<float> unit(512);
+        pcxo::md::fft_rows(unit, st2);
+        double worst = 0;
+        for (unsigned k = 0, q = 0; k < nz; ++k) {
+            for (unsigned j = 0; j < ny; ++j, ++q) {
+                auto row = st2.slice<z>(k).slice<y>(j);
+                worst    = std::max(worst, rel_err(row, want[q]));
+            }
+        }
+        expect(worst < 2e-6, "md::fft_rows over 15 rows", worst);
+        auto one = st2.slice<z>(2).slice<y>(1);
+        unit.ifft(one);    // a single row through the vector interface
+        std::vector<cd> back(rows[2 * ny + 1].begin(), rows[2 * ny + 1].begin() + 512);
+        expect(rel_err(one, back) < 2e-6, "fft_unit on an md row slice", rel_err(one, back));
     }
     {    // exceptions keep the reference's types and messages
         bool thrown = false;
