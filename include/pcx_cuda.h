@@ -171,6 +171,29 @@ int pcx_fxcorr_status(pcx_fxcorr h);
 int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, const void* x, size_t len, int pack,
                    size_t channels, size_t stride, void* stream);
 
+/*
+ * Ragged persistent batch.  No counterpart in the reference (which runs one
+ * transform per call): n_fft complex64 FFTs of power-of-two sizes 2^5..2^18
+ * (one transform each, device pointers, pack 8, natural order; all forward,
+ * or all inverse of one size when normalised) and n_xc out-of-place
+ * correlations (signal xc_len[j] samples, kernel of xc_k[j] taps at xc_g[j],
+ * FFT size xc_nfft[j] in 2^7..2^14), executed by ONE persistent launch that
+ * takes work items from a device queue (four-step transforms as column and
+ * row tiles with device-side dependencies), captured once as a CUDA graph.
+ * Pointers are fixed at creation; each exec replays the graph.
+ */
+typedef struct pcx_ragged_s* pcx_ragged;
+int pcx_ragged_create(pcx_ragged* h, int dtype, size_t n_fft, const size_t* sizes, void* const* dst,
+                      const void* const* src, int direction, int normalize, size_t n_xc, const size_t* xc_len,
+                      const size_t* xc_k, const void* const* xc_g, const size_t* xc_nfft, void* const* xc_dst,
+                      const void* const* xc_src);
+int pcx_ragged_exec(pcx_ragged h, void* stream);
+/* PCX_ERR_TIMEOUT if a work item gave up waiting for a dependency (synchronises). */
+int pcx_ragged_status(pcx_ragged h);
+/* Work items in the queue. */
+size_t pcx_ragged_items(pcx_ragged h);
+int    pcx_ragged_destroy(pcx_ragged h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,12 +98,56 @@ __device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const c
 // pattern here: offsets are multiples of 16, or the base is).
 __device__ __forceinline__ int pad16(int l) { return l + (l >> 4); }
 
+// Stage-S twiddles of thread t (radix R, G butterflies): w[g*R + j].
+template<class P, int S, class T>
+__device__ __forceinline__ void load_stage_tw(cpx<T>* w, int t, const cpx<T>* __restrict__ stw) {
+    constexpr int RB  = P::rbits(S);
+    constexpr int R   = 1 << RB;
+    constexpr int NSB = P::nsbits(S);
+    constexpr int G   = P::E / R;
+    static_for<G>([&](auto gc) {
+        constexpr int g  = decltype(gc)::value;
+        const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
+        const cpx<T>* tw = stw + stage_tw_offset<P>(S) + k * R;
+        static_for<R / 2>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            ldg2(tw + 2 * j, w[g * R + 2 * j], w[g * R + 2 * j + 1]);
+        });
+    });
+}
+
+// Butterflies of stage S >= 1 with preloaded twiddles.
+template<class P, int S, class T, int E>
+__device__ __forceinline__ void stage_apply_tw(cpx<T> (&v)[E], const cpx<T>* w) {
+    constexpr int RB = P::rbits(S);
+    constexpr int R  = 1 << RB;
+    constexpr int G  = E / R;
+    static_for<G>([&](auto gc) {
+        constexpr int g = decltype(gc)::value;
+        cpx<T>        a[R];
+        a[0] = v[g];
+        static_for<R - 1>([&](auto jc) {
+            constexpr int j = decltype(jc)::value + 1;
+            a[j]            = cmul(v[g + j * G], w[g * R + j]);
+        });
+        dft<R, 1, 0>(a);
+        static_for<R>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            v[g + j * G]    = a[j];
+        });
+    });
+}
+
+// Stages 1..NST-1 through the exchange buffer; each stage's twiddles are
+// requested before the exchange barriers so their latency overlaps them.
 template<class P, class X, class T, int E>
 __device__ __forceinline__ void run_stages_tab(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
                                                const cpx<T>* __restrict__ stw) {
     static_for<P::NST - 1>([&](auto sc) {
         constexpr int S = decltype(sc)::value;
         constexpr int G = E / (1 << P::rbits(S));
+        cpx<T>        w[E];
+        load_stage_tw<P, S + 1>(w, t, stw);
         __syncthreads();
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
@@ -115,7 +159,25 @@ __device__ __forceinline__ void run_stages_tab(cpx<T> (&v)[E], cpx<T>* xch, int 
             constexpr int i = decltype(ic)::value;
             v[i]            = xch[X::idx(m, t + i * P::TT)];
         });
-        stage_compute_tab<P, S + 1>(v, t, stw);
+        stage_apply_tw<P, S + 1>(v, w);
+    });
+}
+
+// b^i for i = 0..15 by repeated squaring (at most five products deep).
+template<class T>
+__device__ __forceinline__ void powers16(cpx<T> b, cpx<T> (&p)[16]) {
+    p[0] = {T(1), T(0)};
+    p[1] = b;
+    p[2] = cmul(b, b);
+    p[3] = cmul(p[2], b);
+    p[4] = cmul(p[2], p[2]);
+    p[5] = cmul(p[4], b);
+    p[6] = cmul(p[4], p[2]);
+    p[7] = cmul(p[4], p[3]);
+    p[8] = cmul(p[4], p[4]);
+    static_for<7>([&](auto ic) {
+        constexpr int i = decltype(ic)::value + 1;
+        p[8 + i]        = cmul(p[8], p[i]);
     });
 }
 
@@ -236,11 +298,13 @@ __global__ void __launch_bounds__(NT, 2) k_col2(v2_args a) {
         // v[i] = column spectrum at k1 = t + i*TT; twiddle W_N^(k1*n2)
         const uint32_t e0   = (uint32_t)t * (uint32_t)n2;
         const cpx<T>   base = cmul(ldg_cpx(thi + (e0 >> LOGN2)), ldg_cpx(tlo + (e0 & (N2 - 1))));
+        cpx<T>         bp[16];
+        powers16(ldg_cpx(tb + n2), bp);
         cpx<T>*        dst  = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             cpx<T>        w = base;
-            if constexpr (i > 0) w = cmul(base, ldg_cpx(tb + ((i * n2) & (16 * N2 - 1))));
+            if constexpr (i > 0) w = cmul(base, bp[i]);
             dst[(long long)i * TT * N2] = cmul(v[i], w);
         });
     }
@@ -568,11 +632,13 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
         run_stages_tab<P, X>(v, xch, c, t, stw);
         const uint32_t e0   = (uint32_t)t * (uint32_t)n2;
         const cpx<T>   base = cmul(ldg_cpx(thi + (e0 >> LOGN2)), ldg_cpx(tlo + (e0 & (N2 - 1))));
+        cpx<T>         bp[16];
+        powers16(ldg_cpx(tb + n2), bp);
         cpx<T>*        dst  = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             cpx<T>        w = base;
-            if constexpr (i > 0) w = cmul(base, ldg_cpx(tb + ((i * n2) & (16 * N2 - 1))));
+            if constexpr (i > 0) w = cmul(base, bp[i]);
             dst[(long long)i * TT * N2] = cmul(v[i], w);
         });
     }

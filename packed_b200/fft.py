@@ -317,3 +317,50 @@ class fxcorr_unit:
                                              _ptr(x), length, p, channels, real_size(length, p),
                                              _stream_ptr(stream)))
         return gx, gg
+
+
+class ragged_batch:
+    """Many FFTs of uneven power-of-two sizes and correlations in ONE
+    persistent launch fed by a device work queue, replayed from a CUDA graph
+    (pcx_ragged_*).  No counterpart in the reference.
+
+    ``ffts``: list of ``(dst, src, n)`` — one complex64 transform each, pack 8
+    (``n`` in 2^5..2^18).  ``xcorrs``: list of ``(dst, src, length, g, n_fft)``
+    with ``g`` a :class:`vector` of kernel taps (out of place).  Pointers are
+    fixed at construction; calling the object replays the graph.
+    """
+
+    def __init__(self, ffts, xcorrs=(), direction: int = 0, normalize: bool = True):
+        n = len(ffts)
+        m = len(xcorrs)
+        sz = (ctypes.c_size_t * max(n, 1))(*[int(f[2]) for f in ffts])
+        dsts = (ctypes.c_void_p * max(n, 1))(*[f[0].data_ptr() for f in ffts])
+        srcs = (ctypes.c_void_p * max(n, 1))(*[f[1].data_ptr() for f in ffts])
+        xl = (ctypes.c_size_t * max(m, 1))(*[int(x[2]) for x in xcorrs])
+        xk = (ctypes.c_size_t * max(m, 1))(*[int(x[3].size()) for x in xcorrs])
+        xg = (ctypes.c_void_p * max(m, 1))(*[x[3].data.data_ptr() for x in xcorrs])
+        xn = (ctypes.c_size_t * max(m, 1))(*[int(x[4]) for x in xcorrs])
+        xd = (ctypes.c_void_p * max(m, 1))(*[x[0].data_ptr() for x in xcorrs])
+        xs = (ctypes.c_void_p * max(m, 1))(*[x[1].data_ptr() for x in xcorrs])
+        self._keep = (ffts, xcorrs)
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.lib().pcx_ragged_create(ctypes.byref(self._h), _lib.PCX_F32, n, sz, dsts, srcs, direction,
+                                                int(normalize), m, xl, xk, xg, xn, xd, xs))
+
+    def __call__(self, stream=None) -> None:
+        _lib.check(_lib.lib().pcx_ragged_exec(self._h, _stream_ptr(stream)))
+
+    def status(self) -> None:
+        _lib.check(_lib.lib().pcx_ragged_status(self._h))
+
+    def items(self) -> int:
+        return int(_lib.lib().pcx_ragged_items(self._h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().pcx_ragged_destroy(h)
+            except Exception:
+                pass
+            self._h = None
