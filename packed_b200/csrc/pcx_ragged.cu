@@ -41,6 +41,7 @@ struct fft_req {
     float*       dst;
     int          slot;        // four-step scratch slot
     int          prev;        // transform that used the slot before (-1 none)
+    int          prev_rows;   // row tiles of that transform (its completion count)
 };
 struct xc_req {
     const float*      src;
@@ -136,7 +137,7 @@ __device__ bool col_item(const args& A, const item& it, cpx<float>* xch, int* s_
     const fft_req&  r   = A.req[it.a];
     if (tid == 0) {
         // the slot is free once the previous user finished all its row tiles
-        *s_flag = r.prev < 0 || wait_count(A.row_done + r.prev, A.row_tiles[L1 + L2]);
+        *s_flag = r.prev < 0 || wait_count(A.row_done + r.prev, r.prev_rows);
     }
     __syncthreads();
     if (!*s_flag) return false;
@@ -390,7 +391,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (lg < 5 || lg > 18 || (sizes[i] & (sizes[i] - 1))) {
                 return fail(pcx_fail(PCX_ERR_UNSUPPORTED, "ragged FFT sizes must be powers of two in 2^5..2^18"));
             }
-            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1};
+            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1, 0};
             by_lg[lg].push_back((int)i);
         }
         int sms = 148, dev = 0;
@@ -498,14 +499,15 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
         size_t    slot_elems = 0;
         for (auto& [lg, idx]: by_lg)
             if (lg > 12) slot_elems = std::max<size_t>(slot_elems, size_t(1) << lg);
-        for (size_t q = 0; q < four.size(); ++q) {
-            req[four[q]].slot = (int)(q % NSLOT);
-            req[four[q]].prev = q >= (size_t)NSLOT ? four[q - NSLOT] : -1;
-        }
         // four-step transforms in queue order with their sizes
         std::vector<int> four_lg;
         for (auto& [lg, idx]: by_lg)
             if (lg > 12) four_lg.insert(four_lg.end(), idx.size(), lg);
+        for (size_t q = 0; q < four.size(); ++q) {
+            req[four[q]].slot = (int)(q % NSLOT);
+            req[four[q]].prev = q >= (size_t)NSLOT ? four[q - NSLOT] : -1;
+            req[four[q]].prev_rows = q >= (size_t)NSLOT ? h->A.row_tiles[four_lg[q - NSLOT]] : 0;
+        }
         const size_t nfill = fill.size(), nfour = four.size();
         size_t       fi    = 0;
         auto         push_fill = [&](size_t upto) {
