@@ -172,6 +172,19 @@ int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, const void*
                    size_t channels, size_t stride, void* stream);
 
 /*
+ * Tensor-core form of the batched FFT (no reference counterpart): radix-16
+ * stages as dense 32x32 real DFT-matrix products on the tensor cores
+ * (tcgen05.mma, FP32 accumulation in tensor memory) with split operands,
+ * precision 0: bfloat16 hi + lo, three products (kind::f16);
+ * precision 1: tf32 hi + lo, three products (kind::tf32).
+ * `batch` contiguous rows of a complex64 plan in natural order, pack 8,
+ * 2^8 <= n <= 2^12.  Errors against an FP64 oracle are reported per size by
+ * the test suite and the benchmark.
+ */
+int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int direction, int normalize, size_t batch,
+                    int precision, void* stream);
+
+/*
  * Ragged persistent batch.  No counterpart in the reference (which runs one
  * transform per call): n_fft complex64 FFTs of power-of-two sizes 2^5..2^18
  * (one transform each, device pointers, pack 8, natural order; all forward,

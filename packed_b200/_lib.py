@@ -41,6 +41,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_fxcorr_exec": (_i, [_vp, _vp, _vp, _sz, _i, _sz, _sz, _sz, _vp]),
     "pcx_fxcorr_vjp": (_i, [_vp, _vp, _vp, _vp, _vp, _sz, _i, _sz, _sz, _vp]),
     "pcx_fxcorr_status": (_i, [_vp]),
+    "pcx_tc_fft_exec": (_i, [_vp, _vp, _vp, _i, _i, _sz, _i, _vp]),
     "pcx_ragged_create": (_i, [ctypes.POINTER(_vp), _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_vp),
                                ctypes.POINTER(_vp), _i, _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                ctypes.POINTER(_vp), ctypes.POINTER(_sz), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),

@@ -101,23 +101,27 @@ __device__ void single_items(const args& A, const item& it, cpx<float>* xch) {
     const int  t    = tid - m * TT;
     const bool live = m < it.b;
     const fft_req& r = A.req[it.a + (live ? m : 0)];
-    const float*   s = r.src + pk<LPK>(t);
-    float*         d = r.dst + pk<LPK>(t);
+    const float*   s = r.src;
+    float*         d = r.dst;
     const auto*    stw = A.tb.stw[LOGL];
     cpx<float>     v[E];
+    // element t + i*TT; its packed offset splits into base + constant only
+    // when TT is a multiple of the pack width
     static_for<E>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        const float   re = s[2 * i * TT], im = s[2 * i * TT + 8];
-        v[i]           = {re, A.conj ? -im : im};
+        constexpr int i  = decltype(ic)::value;
+        const int     o  = pk<LPK>(t + i * TT);
+        const float   re = s[o], im = s[o + 8];
+        v[i]             = {re, A.conj ? -im : im};
     });
     stage_compute_tab<P, 0>(v, t, stw);
     run_stages_tab<P, X>(v, xch, m, t, stw);
     if (live) {
         const float sc = A.scale, sim = A.conj ? -A.scale : A.scale;
         static_for<E>([&](auto ic) {
-            constexpr int i     = decltype(ic)::value;
-            d[2 * i * TT]       = v[i].re * sc;
-            d[2 * i * TT + 8]   = v[i].im * sim;
+            constexpr int i = decltype(ic)::value;
+            const int     o = pk<LPK>(t + i * TT);
+            d[o]            = v[i].re * sc;
+            d[o + 8]        = v[i].im * sim;
         });
     }
 }

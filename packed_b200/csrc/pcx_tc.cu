@@ -1,0 +1,395 @@
+// Tensor-core FFT: radix-16 stages as dense DFT-matrix products on the
+// fifth-generation tensor cores (tcgen05.mma, FP32 accumulation in TMEM).
+//
+// A radix-16 stage over 128 butterflies is D = X * A^T with X the 128 x 32
+// real matrix of twiddled inputs (16 complex per row: reals then
+// imaginaries) and A the 32 x 32 real form of the 16-point DFT,
+//   [[C, S], [-S, C]],  C = cos(2 pi jk/16), S = sin(2 pi jk/16).
+// Operands are split so that the products recover FP32-level accuracy:
+//   PREC_BF16: x = hi + lo in bfloat16, D = Xh Ah + Xh Al + Xl Ah (three
+//              products, kind::f16);
+//   PREC_TF32: the same split in tf32 (kind::tf32).
+// The dropped lo*lo term and the representation error of hi + lo set the
+// accuracy (about 2^-16 per stage for bfloat16, 2^-21 for tf32).
+//
+// One CTA of 128 threads transforms T rows; thread i owns TMEM lane i (one
+// butterfly per 128-row block).  Twiddles, the remainder radix-2/4/8 stage and
+// the data movement stay on the CUDA cores; one elected thread issues the
+// MMAs and commits them to an mbarrier.  Every mbarrier wait is bounded.
+#include "pcx_fft_v2.cuh"
+#include "pcx_host.hpp"
+
+#include <cuda_bf16.h>
+
+namespace pcxg {
+namespace tc {
+
+constexpr int NT = 128;
+enum : int { PREC_BF16 = 0, PREC_TF32 = 1 };
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template<int PREC>
+__device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    if constexpr (PREC == PREC_BF16) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+            : "memory");
+    }
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of
+// 8 rows x 16 bytes; lbo = byte step between K-adjacent core matrices,
+// sbo = byte step between 8-row groups.
+__device__ __forceinline__ uint64_t sdesc(const void* p, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((smem_u32(p) >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;    // descriptor version of this architecture
+    return d;                  // base offset 0, no swizzle
+}
+
+// Operand element type and its per-MMA K.
+template<int PREC>
+struct op_traits;
+template<>
+struct op_traits<PREC_BF16> {
+    using elem                      = uint16_t;
+    static constexpr int K_PER_MMA  = 16;
+    static constexpr int PER_CHUNK  = 8;    // elements per 16-byte core-matrix row
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+    __device__ static void split(float x, elem& hi, elem& lo) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+        hi                    = __bfloat16_as_ushort(h);
+        lo                    = __bfloat16_as_ushort(l);
+    }
+};
+template<>
+struct op_traits<PREC_TF32> {
+    using elem                      = uint32_t;
+    static constexpr int K_PER_MMA  = 8;
+    static constexpr int PER_CHUNK  = 4;
+    static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+    __device__ static uint32_t to_tf32(float x) {
+        uint32_t r;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+        return r;
+    }
+    __device__ static void split(float x, elem& hi, elem& lo) {
+        hi = to_tf32(x);
+        lo = to_tf32(x - __uint_as_float(hi));
+    }
+};
+
+// Byte offset of element (row, k) of a rows x 32 K-major operand stored as
+// [k chunk][8-row group][row in group][element in chunk].
+template<int PREC, int ROWS>
+__device__ __forceinline__ uint32_t op_off(int row, int k) {
+    using O                 = op_traits<PREC>;
+    constexpr uint32_t ROWB = 16;
+    constexpr uint32_t CM   = 8 * ROWB;           // core matrix bytes
+    constexpr uint32_t LBO  = (ROWS / 8) * CM;    // next K chunk
+    return (uint32_t)(k / O::PER_CHUNK) * LBO + (uint32_t)(row / 8) * CM + (uint32_t)(row % 8) * ROWB +
+           (uint32_t)(k % O::PER_CHUNK) * (uint32_t)sizeof(typename O::elem);
+}
+
+struct tc_args {
+    const float* src;
+    float*       dst;
+    long long    batch;
+    int          conj;
+    float        scale;
+    const void*  twN;    // W_N^i
+    int*         error;
+};
+
+// Smem plan: work[2][T*N] complex | A_hi | A_lo (128 x 32) | B_hi | B_lo (32 x 32)
+template<int LOGN, int PREC>
+struct tc_cfg {
+    static constexpr int N     = 1 << LOGN;
+    static constexpr int T     = N >= 2048 ? 1 : 2048 / N;    // rows per CTA: >= 128 butterflies per stage
+    static constexpr int R0B   = LOGN % 4;                    // remainder stage (CUDA cores) first
+    static constexpr int NTC   = LOGN / 4;                    // radix-16 tensor-core stages
+    static constexpr int OPB   = (int)sizeof(typename op_traits<PREC>::elem);
+    static constexpr int ABYTE = 128 * 32 * OPB;
+    static constexpr int BBYTE = 32 * 32 * OPB;
+    static constexpr int SMEM  = 2 * T * N * 8 + 2 * ABYTE + 2 * BBYTE;
+};
+
+template<int LOGN, int PREC>
+__global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
+    using C  = tc_cfg<LOGN, PREC>;
+    using O  = op_traits<PREC>;
+    using E  = typename O::elem;
+    constexpr int N   = C::N;
+    constexpr int T   = C::T;
+    constexpr int NB  = T * N / 16;    // radix-16 butterflies per stage in this CTA
+    extern __shared__ __align__(128) unsigned char smem[];
+    cpx<float>* work0 = reinterpret_cast<cpx<float>*>(smem);
+    cpx<float>* work1 = work0 + T * N;
+    unsigned char* opA_hi = reinterpret_cast<unsigned char*>(work1 + T * N);
+    unsigned char* opA_lo = opA_hi + C::ABYTE;
+    unsigned char* opB_hi = opA_lo + C::ABYTE;
+    unsigned char* opB_lo = opB_hi + C::BBYTE;
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tslot;
+    bool                aborted = false;
+    const int  tid  = threadIdx.x;
+    const int  warp = tid / 32;
+    const auto* twN = reinterpret_cast<const cpx<float>*>(a.twN);
+    const long long row0 = (long long)blockIdx.x * T;
+    const int       rows = (int)min((long long)T, a.batch - row0);
+
+    if (warp == 0) {
+        tmem_alloc(&tslot, 32);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        fence_barrier_init();
+    }
+    // constant operand: the 32 x 32 real DFT matrix, split
+    for (int q = tid; q < 32 * 32; q += NT) {
+        const int n = q / 32, k = q % 32;
+        const int nn = n % 16, kk = k % 16;
+        double    s, c;
+        sincospi(2.0 * (double)((nn * kk) % 16) / 16.0, &s, &c);
+        double v;
+        if (n < 16) v = k < 16 ? c : s;
+        else v = k < 16 ? -s : c;
+        E hi, lo;
+        O::split((float)v, hi, lo);
+        // exact lo from the double value
+        if constexpr (PREC == PREC_BF16) {
+            const __nv_bfloat16 h = __ushort_as_bfloat16(hi);
+            lo = __bfloat16_as_ushort(__double2bfloat16(v - (double)__bfloat162float(h)));
+        } else {
+            lo = O::to_tf32((float)(v - (double)__uint_as_float(hi)));
+        }
+        *reinterpret_cast<E*>(opB_hi + op_off<PREC, 32>(n, k)) = hi;
+        *reinterpret_cast<E*>(opB_lo + op_off<PREC, 32>(n, k)) = lo;
+    }
+    // rows in natural order (conjugated for the inverse); missing rows are zero
+    for (int q = tid; q < T * N; q += NT) {
+        const int r = q / N, e = q % N;
+        cpx<float> v = {0.f, 0.f};
+        if (r < rows) {
+            const float* s = a.src + (row0 + r) * (2 * N) + ((e >> 3) << 4) + (e & 7);
+            v              = {s[0], a.conj ? -s[8] : s[8]};
+        }
+        work0[q] = v;
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = tslot;
+    cpx<float>*    in    = work0;
+    cpx<float>*    out   = work1;
+    int            ns    = 1;    // size of the sub-transforms done so far
+
+    // remainder stage (radix 2, 4 or 8) on the CUDA cores, no twiddles
+    if constexpr (C::R0B > 0) {
+        constexpr int R  = 1 << C::R0B;
+        constexpr int NR = T * N / R;
+        for (int b = tid; b < NR; b += NT) {
+            const int  tr = b / (N / R), bl = b % (N / R);
+            cpx<float> x[R];
+            static_for<R>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                x[j]            = in[tr * N + bl + j * (N / R)];
+            });
+            dft<R, 1, 0>(x);
+            static_for<R>([&](auto jc) {
+                constexpr int j              = decltype(jc)::value;
+                out[tr * N + bl * R + j]     = x[j];
+            });
+        }
+        ns = R;
+        cpx<float>* t = in;
+        in            = out;
+        out           = t;
+        __syncthreads();
+    }
+
+    uint32_t phase = 0;
+    for (int st = 0; st < C::NTC; ++st) {
+        for (int mb = 0; mb < NB; mb += 128) {
+            const int  b  = mb + tid;
+            const int  tr = b / (N / 16), bl = b % (N / 16);
+            const int  k  = bl % ns;
+            cpx<float> x[16];
+            static_for<16>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                cpx<float>    v = in[tr * N + bl + j * (N / 16)];
+                if (j > 0 && ns > 1) v = cmul(v, ldg_cpx(twN + ((j * k) * (N / (16 * ns)))));
+                x[j] = v;
+            });
+            // operand rows: reals 0..15 then imaginaries 16..31
+            static_for<16>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                E             h, l;
+                O::split(x[j].re, h, l);
+                *reinterpret_cast<E*>(opA_hi + op_off<PREC, 128>(tid, j))      = h;
+                *reinterpret_cast<E*>(opA_lo + op_off<PREC, 128>(tid, j))      = l;
+                O::split(x[j].im, h, l);
+                *reinterpret_cast<E*>(opA_hi + op_off<PREC, 128>(tid, j + 16)) = h;
+                *reinterpret_cast<E*>(opA_lo + op_off<PREC, 128>(tid, j + 16)) = l;
+            });
+            fence_proxy_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+                constexpr uint32_t LBO_A = (128 / 8) * 128, LBO_B = (32 / 8) * 128, SBO = 128;
+                constexpr int      KS    = 32 / O::K_PER_MMA;               // MMAs per product
+                constexpr int      CH    = O::K_PER_MMA / O::PER_CHUNK;     // chunks per MMA (2)
+                uint32_t           acc   = 0;
+                const unsigned char* A[3] = {opA_lo, opA_hi, opA_hi};
+                const unsigned char* B[3] = {opB_hi, opB_lo, opB_hi};
+                for (int p = 0; p < 3; ++p) {
+                    for (int ks = 0; ks < KS; ++ks) {
+                        umma<PREC>(taddr, sdesc(A[p] + ks * CH * LBO_A, LBO_A, SBO), sdesc(B[p] + ks * CH * LBO_B, LBO_B, SBO),
+                                   O::IDESC, acc);
+                        acc = 1;
+                    }
+                }
+                umma_commit(&mbar);
+            }
+            const bool ok = mbar_wait_bounded(&mbar, phase);
+            if (__syncthreads_or(!ok)) {
+                // give up: record it and let the MMAs in flight finish before TMEM is freed
+                if (tid == 0) {
+                    atomicExch(a.error, 1);
+                    mbar_wait_bounded(&mbar, phase, 100000000ull);
+                }
+                aborted = true;
+                break;
+            }
+            phase ^= 1;
+            tc_fence_after();
+            uint32_t r[32];
+            tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), r);
+            // outputs of this butterfly, Stockham placement
+            const int base = tr * N + (bl / ns) * ns * 16 + k;
+            static_for<16>([&](auto jc) {
+                constexpr int j        = decltype(jc)::value;
+                out[base + j * ns]     = {__uint_as_float(r[j]), __uint_as_float(r[j + 16])};
+            });
+            tc_fence_before();
+            __syncthreads();    // operands and accumulator free for the next block
+        }
+        if (aborted) break;
+        ns *= 16;
+        cpx<float>* t = in;
+        in            = out;
+        out           = t;
+        __syncthreads();
+    }
+    if (!aborted) {
+        const float sc = a.scale, sim = a.conj ? -a.scale : a.scale;
+        for (int q = tid; q < rows * N; q += NT) {
+            const int r = q / N, e = q % N;
+            float*    d = a.dst + (row0 + r) * (2 * N) + ((e >> 3) << 4) + (e & 7);
+            d[0]        = in[q].re * sc;
+            d[8]        = in[q].im * sim;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, 32);
+}
+
+}    // namespace tc
+}    // namespace pcxg
+
+using namespace pcxg;
+
+namespace {
+template<int LOGN, int PREC>
+cudaError_t launch_tc(const tc::tc_args& a, cudaStream_t st) {
+    using C   = tc::tc_cfg<LOGN, PREC>;
+    auto kern = tc::k_tcfft<LOGN, PREC>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    const long long grid = (a.batch + C::T - 1) / C::T;
+    if (grid == 0) return cudaSuccess;
+    kern<<<(unsigned)grid, tc::NT, C::SMEM, st>>>(a);
+    return cudaGetLastError();
+}
+template<int PREC>
+cudaError_t dispatch_tc(int log_n, const tc::tc_args& a, cudaStream_t st) {
+    switch (log_n) {
+    case 8: return launch_tc<8, PREC>(a, st);
+    case 9: return launch_tc<9, PREC>(a, st);
+    case 10: return launch_tc<10, PREC>(a, st);
+    case 11: return launch_tc<11, PREC>(a, st);
+    case 12: return launch_tc<12, PREC>(a, st);
+    default: return cudaErrorNotSupported;
+    }
+}
+}    // namespace
+
+// Tensor-core transform of `batch` contiguous rows (pack 8, natural order).
+extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int direction, int normalize,
+                               size_t batch, int precision, void* stream) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        if (plan->dtype != PCX_F32 || plan->order != PCX_ORDER_NORMAL) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form: complex64, natural order");
+        }
+        if (plan->log_n < 8 || plan->log_n > 12) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form built for 2^8 <= N <= 2^12");
+        }
+        if (precision != 0 && precision != 1) return pcx_fail(PCX_ERR_INVALID, "precision: 0 bf16x3, 1 tf32x3");
+        // full W_N table (the plan's single-pass table)
+        tc::tc_args a{};
+        a.src   = static_cast<const float*>(src);
+        a.dst   = static_cast<float*>(dst);
+        a.batch = (long long)batch;
+        a.conj  = direction == PCX_INVERSE;
+        a.scale = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
+        a.twN   = plan->twL;
+        a.error = plan->err;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cudaError_t  e  = precision == 0 ? dispatch_tc<tc::PREC_BF16>(plan->log_n, a, st)
+                                         : dispatch_tc<tc::PREC_TF32>(plan->log_n, a, st);
+        PCX_CUDA_TRY(e);
+        return PCX_OK;
+    });
+}

@@ -237,6 +237,13 @@ class fft_unit:
             raise ValueError(f"cannot perform in-place repack from source pack size (which is {source.pack_size}) "
                              f"to destination pack size (which is {dest.pack_size})")
 
+    def exec_tensor_core(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
+                         batch: int = 1, precision: str = "bf16", stream=None) -> None:
+        """Tensor-core form (pcx_tc_fft_exec): split-bf16 or split-tf32 DFT-matrix stages."""
+        prec = {"bf16": 0, "tf32": 1}[precision]
+        _lib.check(_lib.lib().pcx_tc_fft_exec(self._plan, _ptr(dst), _ptr(src), direction, int(normalize), batch,
+                                              prec, _stream_ptr(stream)))
+
     # ------------------------------------------------------------- adjoint
     def vjp(self, g_out: torch.Tensor, *, direction: int = 0, normalize: bool = True, batch: int = 1,
             pack: int | None = None, stream=None) -> torch.Tensor:

@@ -1,0 +1,50 @@
+"""Tensor-core form (tcgen05 split-precision DFT-matrix stages): accuracy
+against the FP64 oracle per size, and agreement with the plain FP32 path.
+The split-bf16 form is held to its own measured bound (the bf16 hi + lo
+split leaves about 2^-16 per stage); the split-tf32 form to the FP32 bar."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from packed_b200 import fft_unit
+from tests._util import TOL, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BF16_BOUND = 1e-4
+
+
+def c4_input(rng, b, n):
+    # N(0,1) plus a 1e-3 tone at a seeded bin
+    z = rng.standard_normal((b, n)) + 1j * rng.standard_normal((b, n))
+    k = rng.integers(0, n, b)
+    z += 1e-3 * np.exp(2j * np.pi * k[:, None] * np.arange(n)[None, :] / n)
+    return z, k
+
+
+@pytest.mark.parametrize("log_n", [8, 9, 10, 11, 12])
+@pytest.mark.parametrize("precision", ["bf16", "tf32"])
+def test_tc_fft_accuracy(log_n, precision):
+    n = 1 << log_n
+    b = 33
+    rng = np.random.default_rng(4)
+    z, k = c4_input(rng, b, n)
+    x = torch.as_tensor(O.pack(z, 8)).cuda()
+    y = torch.full_like(x, float("nan"))
+    unit = fft_unit(n)
+    unit.exec_tensor_core(y, x, batch=b, precision=precision)
+    torch.cuda.synchronize()
+    unit.status()
+    got = O.unpack(y.cpu().numpy(), n, 8)
+    want = np.fft.fft(z, axis=-1)
+    err = rel_l2(got, want)
+    bound = TOL[np.float32] if precision == "tf32" else BF16_BOUND
+    assert err < bound, f"{precision} N={n}: rel L2 {err:.3e}"
+    # the tone bin keeps its value
+    tone = np.abs(got[np.arange(b), k] - want[np.arange(b), k]).max()
+    assert tone < 1e-2
+    # inverse round trip
+    back = torch.empty_like(y)
+    unit.exec_tensor_core(back, y, batch=b, direction=1, precision=precision)
+    assert rel_l2(O.unpack(back.cpu().numpy(), n, 8), z) < 2 * bound
