@@ -1,7 +1,7 @@
 """Benchmarks of the packed FFT / correlation hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c3|c5]
+                    [--workload c2|c1|c3|c4|c5]
 
 Workloads (synthetic data, N(0,1) unless stated; all buffers stay resident in
 HBM and are larger than the 126 MB L2, so no flush is needed between steps):
@@ -12,6 +12,9 @@ HBM and are larger than the 126 MB L2, so no flush is needed between steps):
   c1            N=1024, batch 64, forward then inverse (U[-1,1), seed 0).
   c3            fxcorr: 256 channels x 2^20 complex64 samples correlated in place
                 with a 4096-tap kernel (sigma 1/64) by overlap-save, N_fft 16384.
+  c4            tensor-core form: N in {256, 1024, 4096}, batch 4096, split-bf16
+                and split-tf32 DFT-matrix stages vs the plain FP32 path, with
+                rel L2 / max-abs / tone-bin error vs FP64 per N.
   c5            ragged batch: 10,000 FFTs, N log-uniform 2^8..2^18, plus 500
                 correlations (S 2^12..2^20, K 64..8192), one persistent launch
                 replayed from a CUDA graph, against per-size plain launches.
@@ -299,7 +302,163 @@ class C3Fxcorr:
                           f"threads, {ch} channels x 2^20 x {reps} repetitions"}
 
 
-WORKLOADS = {"c2": C2Sweep, "c1": C1, "c3": C3Fxcorr}
+class C4TensorCore:
+    """Tensor-core split-precision FFT against the plain FP32 path, batch 4096."""
+    name = "c4"
+    log_ns = [8, 10, 12]
+    batch = 4096
+
+    def config(self, world):
+        return {"workload": "C4: N in {256, 1024, 4096}, batch 4096, complex64 N(0,1) + 1e-3 tone at a seeded bin "
+                            "(seed 4); tensor-core split-bf16 and split-tf32 forward vs plain FP32 forward",
+                "global_batch_points": sum(self.batch << lg for lg in self.log_ns) * world,
+                "l2": "inputs 8-128 MiB per size; timed steps back to back",
+                "parallelism": f"independent shards x{world}"}
+
+    def setup(self, dev, rank):
+        import torch
+        from packed_b200 import fft_unit
+        self.units, self.x, self.y, self.z = {}, {}, {}, {}
+        rng = np.random.default_rng(4)
+        for lg in self.log_ns:
+            n = 1 << lg
+            z = rng.standard_normal((self.batch, n)) + 1j * rng.standard_normal((self.batch, n))
+            k = rng.integers(0, n, self.batch)
+            z += 1e-3 * np.exp(2j * np.pi * k[:, None] * np.arange(n)[None, :] / n)
+            a = np.zeros((self.batch, n // 8, 2, 8), np.float32)
+            a[:, :, 0, :] = z.real.reshape(self.batch, -1, 8)
+            a[:, :, 1, :] = z.imag.reshape(self.batch, -1, 8)
+            self.z[lg] = (z[:16], k[:16])
+            self.x[lg] = torch.as_tensor(a.reshape(-1)).to(dev)
+            self.y[lg] = torch.empty_like(self.x[lg])
+            self.units[lg] = fft_unit(n)
+
+    def parts(self):
+        return [f"{m}:{1 << lg}" for lg in self.log_ns for m in ("plain", "tc_bf16", "tc_tf32")]
+
+    def _split(self, key):
+        m, n = key.split(":")
+        return m, int(n).bit_length() - 1
+
+    def run_part(self, key):
+        m, lg = self._split(key)
+        u = self.units[lg]
+        if m == "plain":
+            u.exec(self.y[lg], self.x[lg], batch=self.batch)
+        else:
+            u.exec_tensor_core(self.y[lg], self.x[lg], batch=self.batch, precision=m[3:])
+
+    def part_bytes(self, key):
+        _, lg = self._split(key)
+        return (self.batch << lg) * B_PT
+
+    def bytes_per_step(self):
+        return sum(self.part_bytes(p) for p in self.parts())
+
+    def accuracy(self):
+        """rel L2 / max-abs / tone-bin error vs FP64 per N and form (first 16 rows)."""
+        import torch
+        out = {}
+        for lg in self.log_ns:
+            n = 1 << lg
+            z, k = self.z[lg]
+            want = np.fft.fft(z, axis=-1)
+            for m in ("plain", "tc_bf16", "tc_tf32"):
+                self.run_part(f"{m}:{n}")
+                torch.cuda.synchronize()
+                a = self.y[lg][: 16 * 2 * n].cpu().numpy().astype(np.float64).reshape(16, -1, 2, 8)
+                got = (a[:, :, 0, :] + 1j * a[:, :, 1, :]).reshape(16, n)
+                rel = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+                mx = float(np.abs(got - want).max())
+                tone = float(np.abs(got[np.arange(16), k] - want[np.arange(16), k]).max())
+                out[f"{m}:{n}"] = {"rel_l2": rel, "max_abs": mx, "tone_bin_abs": tone}
+        return out
+
+    def e2e(self, torch, stream):
+        return None
+
+    def launches(self):
+        return len(self.parts())
+
+    def cpu_reference(self, budget_s=12.0):
+        c2 = C2Sweep()
+        c2.log_ns = list(self.log_ns)
+        return c2.cpu_reference(budget_s)
+
+
+class C5Ragged:
+    """Ragged batch: one persistent launch (graph) vs per-size plain launches."""
+    name = "c5"
+    n_fft, n_xc = 10000, 500
+
+    def config(self, world):
+        return {"workload": "C5: 10,000 complex64 FFTs, N log-uniform 2^8..2^18, plus 500 correlations "
+                            "(S log-uniform 2^12..2^20, K log-uniform 64..8192, N_fft = next pow2 >= 2K), "
+                            "N(0,1) seed 5; one persistent launch from a device work queue replayed as a CUDA "
+                            "graph, vs per-size plain launches",
+                "global_batch_points": None, "parallelism": f"independent shards x{world}"}
+
+    def setup(self, dev, rank):
+        import torch
+        from packed_b200 import fft_unit, fxcorr_unit, ragged_batch, vector
+        rng = np.random.default_rng(5)
+        lgs = np.floor(rng.uniform(8, 19, self.n_fft)).astype(int)
+        self.groups = {}
+        for lg in sorted(set(lgs.tolist())):
+            cnt = int((lgs == lg).sum())
+            n = 1 << lg
+            src = torch.randn(cnt * 2 * n, device=dev)
+            self.groups[lg] = (cnt, src, torch.empty_like(src), fft_unit(n))
+        ffts = []
+        for lg, (cnt, src, dst, _) in self.groups.items():
+            n = 1 << lg
+            for i in range(cnt):
+                ffts.append((dst[i * 2 * n:(i + 1) * 2 * n], src[i * 2 * n:(i + 1) * 2 * n], n))
+        self.xcs, self.xunits = [], []
+        s_all = np.floor(2 ** rng.uniform(12, 20, self.n_xc)).astype(int) // 8 * 8
+        k_all = np.floor(2 ** rng.uniform(6, 13, self.n_xc)).astype(int)
+        self.xc_points = int(s_all.sum())
+        for s, k in zip(s_all, k_all):
+            nf = max(128, 1 << int(np.ceil(np.log2(2 * k))))
+            taps = vector.from_complex(rng.standard_normal(k) + 1j * rng.standard_normal(k), device=dev)
+            x = torch.randn(2 * int(s), device=dev)
+            y = torch.empty_like(x)
+            self.xcs.append((y, x, int(s), taps, nf))
+            self.xunits.append(fxcorr_unit(taps, nf))
+        self.batch = ragged_batch(ffts, self.xcs)
+        self.fft_points = sum(cnt << lg for lg, (cnt, _, _, _) in self.groups.items())
+
+    def parts(self):
+        return ["ragged_graph", "plain_per_size"]
+
+    def run_part(self, key):
+        if key == "ragged_graph":
+            self.batch()
+        else:
+            for lg, (cnt, src, dst, u) in self.groups.items():
+                u.exec(dst, src, batch=cnt)
+            for (y, x, s, _, _), u in zip(self.xcs, self.xunits):
+                u.exec(y, x, s)
+
+    def part_bytes(self, key):
+        return (self.fft_points + self.xc_points) * B_PT
+
+    def bytes_per_step(self):
+        return self.part_bytes("ragged_graph")
+
+    def e2e(self, torch, stream):
+        return None
+
+    def launches(self):
+        return 1 + len(self.groups) + self.n_xc
+
+    def cpu_reference(self, budget_s=12.0):
+        c2 = C2Sweep()
+        c2.log_ns = list(range(8, 19))
+        return c2.cpu_reference(budget_s)
+
+
+WORKLOADS = {"c2": C2Sweep, "c1": C1, "c3": C3Fxcorr, "c4": C4TensorCore, "c5": C5Ragged}
 
 
 # ----------------------------------------------------------------- driver
@@ -400,6 +559,15 @@ def main() -> None:
     pk = peaks()
     ms_step = res["ms"] / args.steps
     value = wl.bytes_per_step() * world / (ms_step / 1e3) / 1e9
+    if wl.name in ("c4", "c5"):
+        # the step runs several alternative forms of the same work: report the
+        # headline form's own time (c5: the ragged graph; c4: the fastest form)
+        means = {p: statistics.mean(v) for p, v in res["per"].items()}
+        if wl.name == "c5":
+            ms_step = means["ragged_graph"]
+        else:
+            ms_step = sum(min(means[f"{m}:{1 << lg}"] for m in ("plain", "tc_bf16", "tc_tf32")) for lg in wl.log_ns)
+        value = wl.bytes_per_step() * world / (ms_step / 1e3) / 1e9
     mean = {p: statistics.mean(v) for p, v in res["per"].items()}
     top = max(mean, key=mean.get)
     ach = wl.part_bytes(top) / (mean[top] / 1e3) / 1e9
@@ -419,6 +587,8 @@ def main() -> None:
                      "kernel": f"{wl.name}:{top}", "algorithmic_bytes": wl.part_bytes(top)},
         "clocks": res["clocks"], "e2e": res["e2e"], "gpu_launches": wl.launches() * args.steps,
     }
+    if hasattr(wl, "accuracy"):
+        line["accuracy_vs_fp64"] = wl.accuracy()
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = wl.cpu_reference()
     print(json.dumps(line))
