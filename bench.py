@@ -523,6 +523,8 @@ def main() -> None:
     wl = WORKLOADS[args.workload]()
     if args.points is not None and hasattr(wl, "points"):
         wl.points = 1 << args.points
+    if args.points is not None and hasattr(wl, "channels"):
+        wl.channels = max(1, (1 << args.points) // wl.length)
     if args.sizes and hasattr(wl, "log_ns"):
         wl.log_ns = [int(v) for v in args.sizes.split(",")]
     config = wl.config(world)

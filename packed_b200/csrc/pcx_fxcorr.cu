@@ -43,10 +43,12 @@ int launch_xc(const xc_args& a, const void* tw, cudaStream_t st, int sms, bool a
     using C             = xcfg<T, LOGN>;
     constexpr int bytes = fxcorr_smem_bytes<T, LOGN, C::EPT, C::M>();
     auto          kern  = k_fxcorr<T, LOGN, C::EPT, C::M>;
-    PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    if (attr_only) return PCX_OK;
+    if (attr_only) {
+        PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        return PCX_OK;
+    }
     int per_sm = 0;
-    PCX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, bytes));
+    PCX_CUDA_TRY(occupancy_cached(reinterpret_cast<const void*>(kern), C::NT, bytes, &per_sm));
     const long long groups = (a.total + C::M - 1) / C::M;
     const long long grid   = std::max<long long>(1, std::min<long long>(groups, (long long)std::max(per_sm, 1) * sms));
     kern<<<(unsigned)grid, C::NT, bytes, st>>>(a, reinterpret_cast<const cpx<T>*>(tw));
@@ -59,8 +61,10 @@ int launch_kg(const kg_args& a, const void* tw, cudaStream_t st, int grid, bool 
     using C             = xcfg<T, LOGN>;
     constexpr int bytes = fxcorr_smem_bytes<T, LOGN, C::EPT, 1>();
     auto          kern  = k_fxcorr_kgrad<T, LOGN, C::EPT>;
-    PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    if (attr_only) return PCX_OK;
+    if (attr_only) {
+        PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        return PCX_OK;
+    }
     kern<<<(unsigned)grid, C::P::TT, bytes, st>>>(a, reinterpret_cast<const cpx<T>*>(tw));
     PCX_CUDA_TRY(cudaGetLastError());
     return PCX_OK;

@@ -5,10 +5,54 @@
 
 #include <cuda_runtime.h>
 #include <exception>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 
 namespace pcxg {
+
+// Resident CTAs per SM for (kernel, block size, dynamic smem), queried once per
+// device and cached: the occupancy query costs microseconds, which dominates a
+// small-batch exec if repeated on every launch.
+inline cudaError_t occupancy_cached(const void* kern, int nt, int bytes, int* per_sm) {
+    using key_t = std::tuple<int, const void*, int, int>;
+    static std::mutex             mu;
+    static std::map<key_t, int>   cache;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const key_t k{dev, kern, nt, bytes};
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(k);
+        if (it != cache.end()) { *per_sm = it->second; return cudaSuccess; }
+    }
+    int n = 0;
+    e     = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, nt, bytes);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    cache[k] = n;
+    *per_sm  = n;
+    return cudaSuccess;
+}
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (device, kernel).
+inline cudaError_t smem_attr_cached(const void* kern, int bytes) {
+    using key_t = std::tuple<int, const void*>;
+    static std::mutex           mu;
+    static std::map<key_t, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = done.find(key_t{dev, kern});
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done[key_t{dev, kern}] = bytes;
+    return e;
+}
+
 struct v2_args;
 struct v3_args;
 }

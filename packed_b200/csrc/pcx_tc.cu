@@ -345,7 +345,7 @@ template<int LOGN, int PREC>
 cudaError_t launch_tc(const tc::tc_args& a, cudaStream_t st) {
     using C   = tc::tc_cfg<LOGN, PREC>;
     auto kern = tc::k_tcfft<LOGN, PREC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    cudaError_t e = smem_attr_cached(reinterpret_cast<const void*>(kern), C::SMEM);
     if (e != cudaSuccess) return e;
     const long long grid = (a.batch + C::T - 1) / C::T;
     if (grid == 0) return cudaSuccess;

@@ -25,7 +25,7 @@ inline cudaError_t set_smem(K kern, int bytes) {
 template<class K>
 inline cudaError_t persistent_grid(K kern, int nt, int bytes, long long tiles, int sms, unsigned* grid) {
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, bytes);
+    cudaError_t e = occupancy_cached(reinterpret_cast<const void*>(kern), nt, bytes, &per_sm);
     if (e != cudaSuccess) return e;
     const long long g = std::min<long long>(tiles, (long long)std::max(per_sm, 1) * sms);
     *grid             = (unsigned)std::max<long long>(g, 1);
