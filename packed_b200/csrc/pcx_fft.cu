@@ -3,6 +3,7 @@
 // FFT entry points of the C ABI (include/pcx_cuda.h).
 #include "pcx_fft_kernels.cuh"
 #include "pcx_fft_v2.cuh"
+#include "pcx_fourstep.cuh"
 #include "pcx_host.hpp"
 
 #include <algorithm>
@@ -246,6 +247,20 @@ static int plan_init_tables(pcx_plan_s* p) {
                 PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_row[i], cudaEventDisableTiming));
             }
             PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+            // one launch for all chunks of a batch
+            if (pcx_fourstep(f64, p->log_n1, p->log_n2, fs_args{}, 0, p->sms, true, &p->fs_tc, &p->fs_tr) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                p->fs_tc = p->fs_tr = 0;
+            }
+            // N = 8192 in FP32 also has a one-pass form (64 KB rows in shared memory)
+            v3_args z3{};
+            if (pcx_v3_single(f64, log_n, z3, 0, p->sms, true) == cudaSuccess) {
+                int e3 = 0;
+                PCX_CUDA_TRY(pcx_v2_stage_twiddles(log_n, nullptr, f64, 0, &e3));
+                PCX_CUDA_TRY(cudaMalloc(&p->stw_one, (size_t)std::max(e3, 2) * eb));
+                PCX_CUDA_TRY(pcx_v2_stage_twiddles(log_n, p->stw_one, f64, 0, &e3));
+            }
         }
     }
     PCX_CUDA_TRY(cudaDeviceSynchronize());
@@ -303,6 +318,8 @@ extern "C" int pcx_plan_create(pcx_plan* plan, size_t n, int dtype, int order, s
 void pcx_plan_s::release() {
     if (tw) cudaFree(tw);
     if (stw) cudaFree(stw);
+    if (stw_one) cudaFree(stw_one);
+    if (fs_ctr) cudaFree(fs_ctr);
     if (scratch) cudaFree(scratch);
     if (side) cudaStreamDestroy(side);
     for (int i = 0; i < 2; ++i) {
@@ -314,7 +331,10 @@ void pcx_plan_s::release() {
     err = nullptr;
     tw      = nullptr;
     stw     = nullptr;
-    scratch = nullptr;
+    stw_one  = nullptr;
+    fs_ctr   = nullptr;
+    fs_ctr_n = 0;
+    scratch  = nullptr;
     side    = nullptr;
 }
 
@@ -468,6 +488,29 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         return PCX_OK;
     }
 
+    if (p->stw_one && src_len == n && io.lp_src == lp_def && io.lp_dst == lp_def &&
+        (batch == 1 || (sstride % vreals == 0 && dstride % vreals == 0))) {
+        // one-pass form of a two-pass size
+        v3_args t3{};
+        t3.src        = src;
+        t3.dst        = dst;
+        t3.src_stride = (long long)sstride;
+        t3.dst_stride = (long long)dstride;
+        t3.batch      = (long long)batch;
+        t3.conj_in    = io.conj_in;
+        t3.conj_out   = io.conj_out;
+        t3.order_in   = io.order_in;
+        t3.order_out  = io.order_out;
+        t3.scale      = io.scale;
+        t3.stw        = p->stw_one;
+        t3.error      = p->err;
+        cudaError_t e = pcx_v3_single(f64, p->log_n, t3, st, p->sms, false);
+        if (e != cudaErrorNotSupported) {
+            PCX_CUDA_TRY(e);
+            return PCX_OK;
+        }
+    }
+
     // Four-step through L2-sized chunks of scratch.  With two scratch buffers
     // the passes are pipelined over two streams: the column pass of chunk c+1
     // (caller's stream) runs beside the row pass of chunk c (side stream).
@@ -508,6 +551,61 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     const bool col_hot = direct && src_len == n && io.lp_src == lp_def;
     const bool use_tma = std::getenv("PCX_NO_TMA") == nullptr;
     const bool row_hot = direct && io.order_out == 0 && io.lp_dst == lp_def;
+
+    // One launch over the whole batch (plan-owned scratch slots and counters);
+    // PCX_FOURSTEP=chunked selects the two-launch chunk pipeline below.
+    const char* fs_env = std::getenv("PCX_FOURSTEP");
+    if (!ws && col_hot && row_hot && use_tma && p->fs_tc > 0 && !(fs_env && std::strcmp(fs_env, "chunked") == 0)) {
+        const long long per_t = p->fs_tc + p->fs_tr;
+        // a row tile runs about `rounds` rounds of items (one item per CTA)
+        // after its transform's column tiles, and a slot is rewritten about as
+        // long after its row tiles, so both dependencies have usually cleared
+        // by the time the copy warp reaches them
+        const char*     re     = std::getenv("PCX_FS_ROUNDS");
+        const long long rounds = re && std::atol(re) > 0 ? std::atol(re) : 3;
+        long long       lag    = (rounds * p->sms + per_t - 1) / per_t;
+        lag                    = std::max<long long>(1, std::min<long long>(lag, (long long)batch));
+        const long long nslot  = std::min<long long>((long long)batch, 2 * lag + 2);
+        std::lock_guard<std::mutex> g(p->mu);
+        const size_t need = (size_t)nslot * per;
+        if (p->scratch_bytes < need) {
+            if (p->scratch) cudaFree(p->scratch);
+            p->scratch       = nullptr;
+            p->scratch_bytes = 0;
+            PCX_CUDA_TRY(cudaMalloc(&p->scratch, need));
+            p->scratch_bytes = need;
+        }
+        if (p->fs_ctr_n < 2 * batch) {
+            if (p->fs_ctr) cudaFree(p->fs_ctr);
+            p->fs_ctr   = nullptr;
+            p->fs_ctr_n = 0;
+            PCX_CUDA_TRY(cudaMalloc(&p->fs_ctr, 2 * batch * sizeof(int)));
+            p->fs_ctr_n = 2 * batch;
+        }
+        PCX_CUDA_TRY(cudaMemsetAsync(p->fs_ctr, 0, 2 * batch * sizeof(int), st));
+        fs_args a{};
+        a.src        = src;
+        a.dst        = dst;
+        a.src_stride = (long long)sstride;
+        a.dst_stride = (long long)dstride;
+        a.batch      = (long long)batch;
+        a.conj_in    = io.conj_in;
+        a.conj_out   = io.conj_out;
+        a.scale      = io.scale;
+        a.stw1       = p->stw1;
+        a.stw2       = p->stw2;
+        a.tw_hi      = p->tw_hi;
+        a.tw_lo      = p->tw_lo;
+        a.tw_b       = p->tw_b;
+        a.scratch    = p->scratch;
+        a.nslot      = (int)nslot;
+        a.lag        = (int)lag;
+        a.col_done   = p->fs_ctr;
+        a.row_done   = p->fs_ctr + batch;
+        a.error      = p->err;
+        PCX_CUDA_TRY(pcx_fourstep(f64, p->log_n1, p->log_n2, a, st, p->sms, false, nullptr, nullptr));
+        return PCX_OK;
+    }
 
     std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
     if (nbuf == 2) {

@@ -20,12 +20,25 @@
 namespace pcxg {
 
 // ---- per-stage twiddle tables ------------------------------------------------
-// Stage S >= 1 of splan P has Ns = 2^nsbits(S) butterfly positions k and
-// radix R; its table holds W_{Ns*R}^(j*k) at [k*R + j] (j = 0 unused).
+// Stage S >= 1 of splan P has Ns = 2^nsbits(S) butterfly positions k and radix
+// R.  Its twiddles are W^(j*k), W = W_{Ns*R}, j = 1..R-1.  Writing j = 4m + i
+// (i, m < 4), W^(jk) = W^(ik) * W^(4mk), so the table keeps, per position k,
+// only the factors (generated in FP64, rounded once):
+//   R = 16: W^k, W^2k, W^3k, W^4k, W^8k, W^12k
+//   R = 8:  W^k, W^2k, W^3k, W^4k
+//   R = 4:  W^k, W^2k, W^3k, 1
+//   R = 2:  W^k, 1
+// and a butterfly forms each twiddle as one entry or the product of two.  That
+// is 48 bytes per radix-16 butterfly instead of 120, and the entries of
+// consecutive positions are contiguous (16-byte vector loads).
+__host__ __device__ constexpr int stw_q(int rb) { return rb == 4 ? 6 : (rb == 1 ? 2 : 4); }
+__host__ __device__ constexpr int stw_mult(int rb, int q) {
+    return q < 3 ? ((q + 1) < (1 << rb) ? q + 1 : 0) : (rb == 4 ? 4 * (q - 2) : (rb == 3 && q == 3 ? 4 : 0));
+}
 template<class P>
 __host__ __device__ constexpr int stage_tw_offset(int S) {
     int off = 0;
-    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) * (1 << P::rbits(s));
+    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) * stw_q(P::rbits(s));
     return off;
 }
 template<class P>
@@ -34,62 +47,121 @@ __host__ __device__ constexpr int stage_tw_size() {
 }
 
 template<class T>
-__global__ void k_stage_twiddles(cpx<T>* out, int ns, int r, int log_nsr) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= ns * r) return;
-    const int       k = q / r, j = q - k * r;
-    const long long e = (long long)j * k;
+__global__ void k_stage_twiddles(cpx<T>* out, int ns, int rb, int log_nsr) {
+    const int q  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nq = stw_q(rb);
+    if (q >= ns * nq) return;
+    const int       k = q / nq, slot = q - k * nq;
+    const long long e = (long long)stw_mult(rb, slot) * k;
     double          s, c;
     sincospi(2.0 * (double)e / (double)(1LL << log_nsr), &s, &c);
     out[q] = {T(c), T(-s)};
 }
 
-template<class T>
-__device__ __forceinline__ void ldg2(const cpx<T>* p, cpx<T>& a, cpx<T>& b);
-template<>
-__device__ __forceinline__ void ldg2(const cpx<float>* p, cpx<float>& a, cpx<float>& b) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-    a              = {v.x, v.y};
-    b              = {v.z, v.w};
+// Two consecutive table entries; SH: the table is in shared memory.
+template<bool SH, class T>
+__device__ __forceinline__ void ld2(const cpx<T>* p, cpx<T>& a, cpx<T>& b) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = SH ? *reinterpret_cast<const float4*>(p) : __ldg(reinterpret_cast<const float4*>(p));
+        a              = {v.x, v.y};
+        b              = {v.z, v.w};
+    } else {
+        if constexpr (SH) {
+            a = p[0];
+            b = p[1];
+        } else {
+            a = ldg_cpx(p);
+            b = ldg_cpx(p + 1);
+        }
+    }
 }
-template<>
-__device__ __forceinline__ void ldg2(const cpx<double>* p, cpx<double>& a, cpx<double>& b) {
-    a = ldg_cpx(p);
-    b = ldg_cpx(p + 1);
+template<class T>
+__device__ __forceinline__ void ldg2(const cpx<T>* p, cpx<T>& a, cpx<T>& b) {
+    ld2<false>(p, a, b);
 }
 
-template<class P, int S, class T, int E>
-__device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ stw) {
+// Twiddle j of a radix-R butterfly from its table factors f[0..Q-1].
+template<int RB, int J, class T>
+__device__ __forceinline__ cpx<T> stw_factor(const cpx<T>* f) {
+    constexpr int i = J & 3, m = J >> 2;
+    if constexpr (RB <= 2) {
+        return f[J - 1];
+    } else if constexpr (RB == 3) {
+        if constexpr (m == 0) return f[i - 1];
+        else if constexpr (i == 0) return f[3];
+        else return cmul(f[3], f[i - 1]);
+    } else {
+        if constexpr (m == 0) return f[i - 1];
+        else if constexpr (i == 0) return f[2 + m];
+        else return cmul(f[2 + m], f[i - 1]);
+    }
+}
+
+// Stage-S table factors of thread t (G butterflies): f[g*Q + q].
+template<class P, int S, bool SH = false, class T>
+__device__ __forceinline__ void load_stage_tw(cpx<T>* f, int t, const cpx<T>* __restrict__ stw) {
     constexpr int RB  = P::rbits(S);
-    constexpr int R   = 1 << RB;
+    constexpr int Q   = stw_q(RB);
     constexpr int NSB = P::nsbits(S);
-    constexpr int G   = E / R;
+    constexpr int G   = P::E / (1 << RB);
+    static_for<G>([&](auto gc) {
+        constexpr int g  = decltype(gc)::value;
+        const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
+        const cpx<T>* tw = stw + stage_tw_offset<P>(S) + k * Q;
+        static_for<Q / 2>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            ld2<SH>(tw + 2 * q, f[g * Q + 2 * q], f[g * Q + 2 * q + 1]);
+        });
+    });
+}
+
+// Butterflies of stage S >= 1 with preloaded table factors.
+template<class P, int S, class T, int E>
+__device__ __forceinline__ void stage_apply_tw(cpx<T> (&v)[E], const cpx<T>* f) {
+    constexpr int RB = P::rbits(S);
+    constexpr int R  = 1 << RB;
+    constexpr int Q  = stw_q(RB);
+    constexpr int G  = E / R;
     static_for<G>([&](auto gc) {
         constexpr int g = decltype(gc)::value;
         cpx<T>        a[R];
-        static_for<R>([&](auto jc) {
-            constexpr int j = decltype(jc)::value;
-            a[j]            = v[g + j * G];
+        a[0] = v[g];
+        static_for<R - 1>([&](auto jc) {
+            constexpr int j = decltype(jc)::value + 1;
+            a[j]            = cmul(v[g + j * G], stw_factor<RB, j>(f + g * Q));
         });
-        if constexpr (NSB > 0) {
-            const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
-            const cpx<T>* tw = stw + stage_tw_offset<P>(S) + k * R;
-            cpx<T>        w[R];
-            static_for<R / 2>([&](auto jc) {
-                constexpr int j = decltype(jc)::value;
-                ldg2(tw + 2 * j, w[2 * j], w[2 * j + 1]);
-            });
-            static_for<R - 1>([&](auto jc) {
-                constexpr int j = decltype(jc)::value + 1;
-                a[j]            = cmul(a[j], w[j]);
-            });
-        }
         dft<R, 1, 0>(a);
         static_for<R>([&](auto jc) {
             constexpr int j = decltype(jc)::value;
             v[g + j * G]    = a[j];
         });
     });
+}
+
+template<class P, int S, class T, int E>
+__device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ stw) {
+    constexpr int NSB = P::nsbits(S);
+    if constexpr (NSB > 0) {
+        cpx<T> f[(E >> P::rbits(S)) * stw_q(P::rbits(S))];
+        load_stage_tw<P, S>(f, t, stw);
+        stage_apply_tw<P, S>(v, f);
+    } else {
+        constexpr int R = 1 << P::rbits(S);
+        constexpr int G = E / R;
+        static_for<G>([&](auto gc) {
+            constexpr int g = decltype(gc)::value;
+            cpx<T>        a[R];
+            static_for<R>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                a[j]            = v[g + j * G];
+            });
+            dft<R, 1, 0>(a);
+            static_for<R>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                v[g + j * G]    = a[j];
+            });
+        });
+    }
 }
 
 // Exchange-buffer index with the padding (one slot per 16) split into a
@@ -98,69 +170,72 @@ __device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const c
 // pattern here: offsets are multiples of 16, or the base is).
 __device__ __forceinline__ int pad16(int l) { return l + (l >> 4); }
 
-// Stage-S twiddles of thread t (radix R, G butterflies): w[g*R + j].
-template<class P, int S, class T>
-__device__ __forceinline__ void load_stage_tw(cpx<T>* w, int t, const cpx<T>* __restrict__ stw) {
-    constexpr int RB  = P::rbits(S);
-    constexpr int R   = 1 << RB;
-    constexpr int NSB = P::nsbits(S);
-    constexpr int G   = P::E / R;
-    static_for<G>([&](auto gc) {
-        constexpr int g  = decltype(gc)::value;
-        const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
-        const cpx<T>* tw = stw + stage_tw_offset<P>(S) + k * R;
-        static_for<R / 2>([&](auto jc) {
-            constexpr int j = decltype(jc)::value;
-            ldg2(tw + 2 * j, w[g * R + 2 * j], w[g * R + 2 * j + 1]);
-        });
-    });
+// Barrier of the threads that share the exchange buffer: the whole block
+// (BARN = 0) or named barrier 1 over the first BARN threads (the compute
+// warps of a block that also has a copy warp).
+template<int BARN>
+__device__ __forceinline__ void xch_sync() {
+    if constexpr (BARN == 0) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync 1, %0;" ::"n"(BARN) : "memory");
+    }
 }
 
-// Butterflies of stage S >= 1 with preloaded twiddles.
-template<class P, int S, class T, int E>
-__device__ __forceinline__ void stage_apply_tw(cpx<T> (&v)[E], const cpx<T>* w) {
-    constexpr int RB = P::rbits(S);
-    constexpr int R  = 1 << RB;
-    constexpr int G  = E / R;
-    static_for<G>([&](auto gc) {
-        constexpr int g = decltype(gc)::value;
-        cpx<T>        a[R];
-        a[0] = v[g];
-        static_for<R - 1>([&](auto jc) {
-            constexpr int j = decltype(jc)::value + 1;
-            a[j]            = cmul(v[g + j * G], w[g * R + j]);
-        });
-        dft<R, 1, 0>(a);
-        static_for<R>([&](auto jc) {
-            constexpr int j = decltype(jc)::value;
-            v[g + j * G]    = a[j];
-        });
-    });
-}
-
-// Stages 1..NST-1 through the exchange buffer; each stage's twiddles are
-// requested before the exchange barriers so their latency overlaps them.
-template<class P, class X, class T, int E>
+// Stages 1..NST-1 through the exchange buffer.  SH: the stage tables are in
+// shared memory, and each stage's factors are loaded after the exchange
+// (short latency, registers stay free); global tables are requested before
+// the exchange barriers so their latency overlaps them.
+template<class P, class X, bool SH = false, int BARN = 0, class T, int E>
 __device__ __forceinline__ void run_stages_tab(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
                                                const cpx<T>* __restrict__ stw) {
     static_for<P::NST - 1>([&](auto sc) {
-        constexpr int S = decltype(sc)::value;
-        constexpr int G = E / (1 << P::rbits(S));
-        cpx<T>        w[E];
-        load_stage_tw<P, S + 1>(w, t, stw);
-        __syncthreads();
+        constexpr int S  = decltype(sc)::value;
+        constexpr int G  = E / (1 << P::rbits(S));
+        constexpr int RB = P::rbits(S + 1);
+        cpx<T>        f[(E >> RB) * stw_q(RB)];
+        if constexpr (!SH) load_stage_tw<P, S + 1, SH>(f, t, stw);
+        xch_sync<BARN>();
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             constexpr int g = i % G, j = i / G;
             xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
         });
-        __syncthreads();
+        xch_sync<BARN>();
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             v[i]            = xch[X::idx(m, t + i * P::TT)];
         });
-        stage_apply_tw<P, S + 1>(v, w);
+        if constexpr (SH) load_stage_tw<P, S + 1, SH>(f, t, stw);
+        stage_apply_tw<P, S + 1>(v, f);
     });
+}
+
+// Copy a stage table into shared memory (16-byte units; the caller syncs).
+template<class P, class T>
+__device__ __forceinline__ void stage_tw_to_smem(cpx<T>* dst, const void* src, int tid, int nt) {
+    constexpr int U = stage_tw_size<P>() * (int)sizeof(cpx<T>) / 16;
+    static_assert((stage_tw_size<P>() * (int)sizeof(cpx<T>)) % 16 == 0, "table in 16-byte units");
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4*       d = reinterpret_cast<uint4*>(dst);
+    for (int i = tid; i < U; i += nt) d[i] = __ldg(s + i);
+}
+template<class P, class T>
+__host__ __device__ constexpr int stage_tw_smem_bytes() {
+    return stage_tw_size<P>() * (int)sizeof(cpx<T>);
+}
+
+// Whether a kernel whose own shared memory is `base` bytes (MINB resident CTAs
+// per SM wanted) can also hold a `tab`-byte stage table without losing
+// residency: 228 KB per SM, 227 KB per CTA, 1 KB reserved per CTA.
+__host__ __device__ constexpr int smem_align16(int b) { return (b + 15) & ~15; }
+__host__ __device__ constexpr bool stw_fits(int base, int tab, int minb) {
+    const int per   = smem_align16(base) + 1024 + 256;
+    int       ctas  = 233472 / per;
+    ctas            = ctas < minb ? ctas : minb;
+    ctas            = ctas < 1 ? 1 : ctas;
+    const int total = smem_align16(base) + tab;
+    return total <= 232448 && ctas * (total + 1024 + 256) <= 233472;
 }
 
 // b^i for i = 0..15 by repeated squaring (at most five products deep).
@@ -178,6 +253,26 @@ __device__ __forceinline__ void powers16(cpx<T> b, cpx<T> (&p)[16]) {
     static_for<7>([&](auto ic) {
         constexpr int i = decltype(ic)::value + 1;
         p[8 + i]        = cmul(p[8], p[i]);
+    });
+}
+
+// out(i, v[i] * base * u^i) for i < E (E a multiple of 4), with u^i formed as
+// u^(4a) * u^b from short product chains (u^4a: a products of u^4; then at
+// most two more), so only a few complex values are live at a time.
+template<int E, class T, class F>
+__device__ __forceinline__ void apply_fourstep_tw(const cpx<T> (&v)[E], cpx<T> base, cpx<T> u, F&& out) {
+    static_assert(E % 4 == 0, "groups of four");
+    const cpx<T> u2 = cmul(u, u);
+    const cpx<T> u4 = cmul(u2, u2);
+    cpx<T>       wa = base;
+    static_for<E / 4>([&](auto ac) {
+        constexpr int a  = decltype(ac)::value * 4;
+        const cpx<T>  w1 = cmul(wa, u);
+        out(std::integral_constant<int, a>{}, cmul(v[a], wa));
+        out(std::integral_constant<int, a + 1>{}, cmul(v[a + 1], w1));
+        out(std::integral_constant<int, a + 2>{}, cmul(v[a + 2], cmul(wa, u2)));
+        out(std::integral_constant<int, a + 3>{}, cmul(v[a + 3], cmul(w1, u2)));
+        if constexpr (a + 4 < E) wa = cmul(wa, u4);
     });
 }
 
@@ -391,16 +486,29 @@ template<int TT>
 __host__ __device__ constexpr int single3_pad() {
     return TT >= 32 ? 0 : (TT >= 8 ? 8 : 4);
 }
+// Resident CTAs per SM a single-pass launch is built for (registers: 128 per
+// thread either way).
+__host__ __device__ constexpr int single3_minb(int nt) { return nt >= 512 ? 1 : 2; }
 template<class T, int LOGL, int NT>
-__host__ __device__ constexpr int single3_smem() {
+__host__ __device__ constexpr int single3_base_smem() {
     using P          = splan<LOGL>;
     constexpr int M  = NT / P::TT;
     constexpr int RS = 2 * P::L + single3_pad<P::TT>();
     return 2 * M * RS * (int)sizeof(T) + xch_blocked<P::L, M>::size * (int)sizeof(cpx<T>);
 }
+template<class T, int LOGL, int NT>
+__host__ __device__ constexpr bool single3_tws() {
+    return stw_fits(single3_base_smem<T, LOGL, NT>(), stage_tw_smem_bytes<splan<LOGL>, T>(), single3_minb(NT));
+}
+template<class T, int LOGL, int NT>
+__host__ __device__ constexpr int single3_smem() {
+    return single3_tws<T, LOGL, NT>()
+               ? smem_align16(single3_base_smem<T, LOGL, NT>()) + stage_tw_smem_bytes<splan<LOGL>, T>()
+               : single3_base_smem<T, LOGL, NT>();
+}
 
 template<class T, int LOGL, int LP, int NT>
-__global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
+__global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
     using P             = splan<LOGL>;
     constexpr int L     = P::L;
     constexpr int E     = P::E;
@@ -420,7 +528,9 @@ __global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
     cpx<T>*          xch = reinterpret_cast<cpx<T>*>(in0 + 2 * TILE);
     T*               stg = reinterpret_cast<T*>(xch);
     __shared__ uint64_t full[2];
-    const auto*      stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    constexpr bool   SH  = single3_tws<T, LOGL, NT>();
+    cpx<T>*          tws = reinterpret_cast<cpx<T>*>(smem + smem_align16(single3_base_smem<T, LOGL, NT>()));
+    const auto*      stw = SH ? tws : reinterpret_cast<const cpx<T>*>(a.stw);
     const T*         src = reinterpret_cast<const T*>(a.src);
     T*               dst = reinterpret_cast<T*>(a.dst);
     const int        tid = threadIdx.x;
@@ -430,6 +540,7 @@ __global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
     const bool       contig_in  = PADR == 0 && a.src_stride == 2 * L;
     const bool       contig_out = PADR == 0 && a.dst_stride == 2 * L;
 
+    if constexpr (SH) stage_tw_to_smem<P, T>(tws, a.stw, tid, NT);
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -481,7 +592,7 @@ __global__ void __launch_bounds__(NT, 2) k_single3(v3_args a) {
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < ntile) issue(tile + 2 * (long long)gridDim.x, s);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X>(v, xch, m, t, stw);
+        run_stages_tab<P, X, SH>(v, xch, m, t, stw);
         __syncthreads();    // exchange reads done: reuse the buffer as staging
         {
             constexpr int S   = P::NST - 1;
@@ -543,6 +654,26 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
         : "memory");
 }
 
+// The same copy with an L2 eviction-priority hint (an L2::evict_first policy
+// for data read once, so it does not push the four-step scratch out of L2).
+__device__ __forceinline__ void tma_load_3d_hint(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar,
+                                                 uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(
+            smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// Drop a 128-byte line from L2 without writing it back (its data are dead).
+__device__ __forceinline__ void l2_discard(const void* p) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
 struct v3_pass_args {
     v2_args   base;
     long long row0;    // first batch row of this launch in the tensor map (column pass)
@@ -552,6 +683,21 @@ struct v3_pass_args {
 template<class T, int LOGN1>
 __host__ __device__ constexpr int col3_boxy() {
     return (1 << LOGN1) < 256 ? (1 << LOGN1) : 256;
+}
+
+template<class T, int LOGN1, int C>
+__host__ __device__ constexpr int col3_base_smem() {
+    return 2 * (1 << LOGN1) * 2 * C * (int)sizeof(T) + xch_interleaved<(1 << LOGN1), C>::size * (int)sizeof(cpx<T>);
+}
+template<class T, int LOGN1, int C>
+__host__ __device__ constexpr bool col3_tws() {
+    return stw_fits(col3_base_smem<T, LOGN1, C>(), stage_tw_smem_bytes<splan<LOGN1>, T>(), 1);
+}
+template<class T, int LOGN1, int C>
+__host__ __device__ constexpr int col3_smem() {
+    return col3_tws<T, LOGN1, C>()
+               ? smem_align16(col3_base_smem<T, LOGN1, C>()) + stage_tw_smem_bytes<splan<LOGN1>, T>()
+               : col3_base_smem<T, LOGN1, C>();
 }
 
 template<class T, int LOGN1, int LOGN2, int LP, int C, int NT>
@@ -574,7 +720,9 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
     cpx<T>*             xch = reinterpret_cast<cpx<T>*>(in0 + 2 * TILE);
     __shared__ uint64_t full[2];
     const v2_args&      a   = pa.base;
-    const auto*         stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    constexpr bool      SH  = col3_tws<T, LOGN1, C>();
+    cpx<T>*             tws = reinterpret_cast<cpx<T>*>(smem + smem_align16(col3_base_smem<T, LOGN1, C>()));
+    const auto*         stw = SH ? tws : reinterpret_cast<const cpx<T>*>(a.stw);
     const auto*         thi = reinterpret_cast<const cpx<T>*>(a.tw_hi);
     const auto*         tlo = reinterpret_cast<const cpx<T>*>(a.tw_lo);
     const auto*         tb  = reinterpret_cast<const cpx<T>*>(a.tw_b);
@@ -583,6 +731,7 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
     const int           t   = tid / C;
     const long long     tiles = a.batch * TPR;
 
+    if constexpr (SH) stage_tw_to_smem<P, T>(tws, a.stw, tid, NT);
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -594,8 +743,11 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
         const int       c0  = (int)(tile - row * TPR) * C;
         T*              buf = in0 + s * TILE;
         mbar_arrive_expect_tx(&full[s], TILE * (int)sizeof(T));
+        const uint64_t pol = l2_evict_first_policy();
 #pragma unroll
-        for (int y = 0; y < N1; y += BOXY) tma_load_3d(buf + y * SEG, &tmap, 2 * c0, y, (int)(pa.row0 + row), &full[s]);
+        for (int y = 0; y < N1; y += BOXY) {
+            tma_load_3d_hint(buf + y * SEG, &tmap, 2 * c0, y, (int)(pa.row0 + row), &full[s], pol);
+        }
     };
     if (tid == 0) {
         if ((long long)blockIdx.x < tiles) issue(blockIdx.x, 0);
@@ -628,25 +780,37 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
         fence_proxy_async_smem();
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < tiles) issue(tile + 2 * (long long)gridDim.x, s);
+        // four-step twiddle inputs: requested now, used after the stages
+        const uint32_t e0 = (uint32_t)t * (uint32_t)n2;
+        const cpx<T>   th = ldg_cpx(thi + (e0 >> LOGN2));
+        const cpx<T>   tl = ldg_cpx(tlo + (e0 & (N2 - 1)));
+        const cpx<T>   tu = ldg_cpx(tb + n2);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X>(v, xch, c, t, stw);
-        const uint32_t e0   = (uint32_t)t * (uint32_t)n2;
-        const cpx<T>   base = cmul(ldg_cpx(thi + (e0 >> LOGN2)), ldg_cpx(tlo + (e0 & (N2 - 1))));
-        cpx<T>         bp[16];
-        powers16(ldg_cpx(tb + n2), bp);
-        cpx<T>*        dst  = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
-        static_for<E>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            cpx<T>        w = base;
-            if constexpr (i > 0) w = cmul(base, bp[i]);
-            dst[(long long)i * TT * N2] = cmul(v[i], w);
+        run_stages_tab<P, X, SH>(v, xch, c, t, stw);
+        cpx<T>* dst = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
+        apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<T> o) {
+            constexpr int i             = decltype(ic)::value;
+            dst[(long long)i * TT * N2] = o;
         });
     }
 }
 
-template<class T, int LOGN1, int C>
-__host__ __device__ constexpr int col3_smem() {
-    return 2 * (1 << LOGN1) * 2 * C * (int)sizeof(T) + xch_interleaved<(1 << LOGN1), C>::size * (int)sizeof(cpx<T>);
+
+
+template<class T, int LOGN2, int CR, int G8>
+__host__ __device__ constexpr int row3_base_smem() {
+    return 2 * CR * ((1 << LOGN2) + 2) * (int)sizeof(cpx<T>) +
+           xch_grouped<(1 << LOGN2), CR, G8>::size * (int)sizeof(cpx<T>);
+}
+template<class T, int LOGN2, int CR, int G8>
+__host__ __device__ constexpr bool row3_tws() {
+    return stw_fits(row3_base_smem<T, LOGN2, CR, G8>(), stage_tw_smem_bytes<splan<LOGN2>, T>(), 1);
+}
+template<class T, int LOGN2, int CR, int G8>
+__host__ __device__ constexpr int row3_smem() {
+    return row3_tws<T, LOGN2, CR, G8>()
+               ? smem_align16(row3_base_smem<T, LOGN2, CR, G8>()) + stage_tw_smem_bytes<splan<LOGN2>, T>()
+               : row3_base_smem<T, LOGN2, CR, G8>();
 }
 
 template<class T, int LOGN1, int LOGN2, int LP, int CR, int G8, int NT>
@@ -668,7 +832,9 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
     cpx<T>*             xch = in0 + 2 * TILE;
     __shared__ uint64_t full[2];
     const v2_args&      a   = pa.base;
-    const auto*         stw = reinterpret_cast<const cpx<T>*>(a.stw);
+    constexpr bool      SH  = row3_tws<T, LOGN2, CR, G8>();
+    cpx<T>*             tws = reinterpret_cast<cpx<T>*>(smem + smem_align16(row3_base_smem<T, LOGN2, CR, G8>()));
+    const auto*         stw = SH ? tws : reinterpret_cast<const cpx<T>*>(a.stw);
     const int           tid = threadIdx.x;
     const int           mlo = tid % G8;
     const int           t   = (tid / G8) % TT;
@@ -677,6 +843,7 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
     const long long     tiles = a.batch * TPR;
     const cpx<T>*       src = reinterpret_cast<const cpx<T>*>(a.src);
 
+    if constexpr (SH) stage_tw_to_smem<P, T>(tws, a.stw, tid, NT);
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -713,6 +880,14 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
         const int       r0  = (int)(tile - row * TPR) * CR;
         const int       k1  = r0 + m;
         const cpx<T>*   in  = in0 + s * TILE + m * RSI + t;
+        {
+            // The tile's rows of four-step scratch have landed in shared memory
+            // and are never read again: drop their L2 lines without write-back.
+            const char* g = reinterpret_cast<const char*>(src + row * (a.src_stride / 2) + (long long)r0 * N2);
+            if ((reinterpret_cast<uintptr_t>(g) & 127) == 0) {
+                for (int q = tid; q < CR * ROWB / 128; q += NT) l2_discard(g + (size_t)q * 128);
+            }
+        }
         cpx<T>          v[E];
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
@@ -722,22 +897,17 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < tiles) issue(tile + 2 * (long long)gridDim.x, s);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X>(v, xch, m, t, stw);
+        run_stages_tab<P, X, SH>(v, xch, m, t, stw);
         T*      dst = reinterpret_cast<T*>(a.dst) + row * a.dst_stride + pk<LP>(t * N1 + k1);
         const T sc  = T(a.scale);
         const T sim = a.conj_out ? -sc : sc;
         static_for<E>([&](auto ic) {
-            constexpr int i           = decltype(ic)::value;
-            dst[2 * i * TT * N1]      = v[i].re * sc;
-            dst[2 * i * TT * N1 + PK] = v[i].im * sim;
+            constexpr int i = decltype(ic)::value;
+            __stcs(dst + 2 * i * TT * N1, v[i].re * sc);    // streaming: keep L2 for the scratch
+            __stcs(dst + 2 * i * TT * N1 + PK, v[i].im * sim);
         });
     }
 }
 
-template<class T, int LOGN2, int CR, int G8>
-__host__ __device__ constexpr int row3_smem() {
-    return 2 * CR * ((1 << LOGN2) + 2) * (int)sizeof(cpx<T>) +
-           xch_grouped<(1 << LOGN2), CR, G8>::size * (int)sizeof(cpx<T>);
-}
 
 }    // namespace pcxg

@@ -1,0 +1,55 @@
+// Instantiations and launch of the one-launch four-step kernel (k_fourstep).
+#include "pcx_fourstep.cuh"
+#include "pcx_v2_launch.cuh"
+
+namespace pcxg {
+
+template<class T, int LOGN1, int LOGN2>
+static cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc, int* tr) {
+    using F = fs_cfg<T, LOGN1, LOGN2>;
+    static_assert(F::SMEM <= 232448, "shared memory per block");
+    static_assert(F::STAGE % 128 == 0, "TMA destinations stay 128-byte aligned");
+    auto kern = k_fourstep<T, LOGN1, LOGN2>;
+    if (tc) *tc = F::TC;
+    if (tr) *tr = F::TR;
+    if (attr_only) return set_smem(kern, F::SMEM);
+    const long long items = a.batch * (F::TC + F::TR);
+    if (items == 0) return cudaSuccess;
+    // 3-D view of the source: [transform][n1][2*N2 reals], box = 64 bytes x min(N1, 256) rows
+    CUtensorMap      map;
+    const cuuint64_t dims[3]    = {(cuuint64_t)2 << LOGN2, (cuuint64_t)1 << LOGN1, (cuuint64_t)a.batch};
+    const long long  ss         = a.batch > 1 ? a.src_stride : (2LL << (LOGN1 + LOGN2));    // unused when 1 row
+    const cuuint64_t strides[2] = {((cuuint64_t)2 << LOGN2) * sizeof(T), (cuuint64_t)ss * sizeof(T)};
+    const cuuint32_t box[3]     = {(cuuint32_t)(2 * F::C), (cuuint32_t)F::BOXY, 1};
+    const cuuint32_t estr[3]    = {1, 1, 1};
+    cudaError_t      e = encode_tensor_map(&map, sizeof(T) == 8, 3, const_cast<void*>(a.src), dims, strides, box, estr);
+    if (e != cudaSuccess) return e;
+    unsigned grid = 0;
+    e             = persistent_grid(kern, F::NT + 32, F::SMEM, items, sms, &grid);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, F::NT + 32, F::SMEM, st>>>(map, a);
+    return cudaGetLastError();
+}
+
+template<class T>
+static cudaError_t dispatch_fs(int l1, int l2, const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc,
+                               int* tr) {
+    switch (l1 * 32 + l2) {
+    case 7 * 32 + 7: return launch_fs<T, 7, 7>(a, st, sms, attr_only, tc, tr);
+    case 8 * 32 + 7: return launch_fs<T, 8, 7>(a, st, sms, attr_only, tc, tr);
+    case 8 * 32 + 8: return launch_fs<T, 8, 8>(a, st, sms, attr_only, tc, tr);
+    case 9 * 32 + 8: return launch_fs<T, 9, 8>(a, st, sms, attr_only, tc, tr);
+    case 9 * 32 + 9: return launch_fs<T, 9, 9>(a, st, sms, attr_only, tc, tr);
+    case 10 * 32 + 9: return launch_fs<T, 10, 9>(a, st, sms, attr_only, tc, tr);
+    case 10 * 32 + 10: return launch_fs<T, 10, 10>(a, st, sms, attr_only, tc, tr);
+    default: return cudaErrorNotSupported;
+    }
+}
+
+}    // namespace pcxg
+
+cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
+                         bool attr_only, int* col_tiles, int* row_tiles) {
+    return f64 ? pcxg::dispatch_fs<double>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles)
+               : pcxg::dispatch_fs<float>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles);
+}

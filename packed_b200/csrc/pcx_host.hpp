@@ -108,6 +108,11 @@ struct pcx_plan_s {
     void*  stw1     = nullptr;    // stage twiddles of the column pass (N1)
     void*  stw2     = nullptr;    // stage twiddles of the row pass (N2)
     void*  tw_b     = nullptr;    // W_{16*N2}^m, m < 16*N2
+    void*  stw_one  = nullptr;    // stage twiddles of a one-pass form of a two-pass size (N = 8192)
+    int    fs_tc    = 0;          // one-launch four-step: column and row tiles per transform (0: none)
+    int    fs_tr    = 0;
+    int*   fs_ctr   = nullptr;    // its dependency counters, 2 per transform
+    size_t fs_ctr_n = 0;
     int    sms      = 148;
     int*   err      = nullptr;    // device flag: a bounded wait in a kernel gave up
 
@@ -137,6 +142,11 @@ cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bo
 // Hot-path launches (pcx_v2_*.cu); cudaErrorNotSupported when no variant exists.
 cudaError_t pcx_v2_single(bool f64, int log_n, const pcxg::v2_args& a, cudaStream_t st, bool attr_only);
 cudaError_t pcx_v3_single(bool f64, int log_n, const pcxg::v3_args& a, cudaStream_t st, int sms, bool attr_only);
+namespace pcxg {
+struct fs_args;
+}
+cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
+                         bool attr_only, int* col_tiles, int* row_tiles);
 cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only);
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,

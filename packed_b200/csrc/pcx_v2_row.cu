@@ -92,9 +92,9 @@ template<int LOGL, class T>
 cudaError_t gen_stage(void* out, cudaStream_t st) {
     using P = pcxg::splan<LOGL>;
     for (int s = 1; s < P::NST; ++s) {
-        const int ns = 1 << P::nsbits(s), r = 1 << P::rbits(s);
+        const int ns = 1 << P::nsbits(s), nq = pcxg::stw_q(P::rbits(s));
         auto*     o  = static_cast<pcxg::cpx<T>*>(out) + pcxg::stage_tw_offset<P>(s);
-        pcxg::k_stage_twiddles<T><<<(ns * r + 255) / 256, 256, 0, st>>>(o, ns, r, P::nsbits(s) + P::rbits(s));
+        pcxg::k_stage_twiddles<T><<<(ns * nq + 255) / 256, 256, 0, st>>>(o, ns, P::rbits(s), P::nsbits(s) + P::rbits(s));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -31,7 +31,7 @@ static cudaError_t dispatch(int log_n, const v2_args& a, cudaStream_t st, bool a
 
 template<class T, int LOGL>
 static cudaError_t launch3(const v3_args& a, cudaStream_t st, int sms, bool attr_only) {
-    constexpr int NT    = 256;
+    constexpr int NT    = LOGL >= 13 ? 512 : 256;    // 16 elements per thread
     constexpr int M     = NT / splan<LOGL>::TT;
     constexpr int bytes = single3_smem<T, LOGL, NT>();
     auto          kern  = k_single3<T, LOGL, v2cfg<T>::LP, NT>;
@@ -56,6 +56,9 @@ static cudaError_t dispatch3(int log_n, const v3_args& a, cudaStream_t st, int s
     case 10: return launch3<T, 10>(a, st, sms, attr_only);
     case 11: return launch3<T, 11>(a, st, sms, attr_only);
     case 12: return launch3<T, 12>(a, st, sms, attr_only);
+    case 13:
+        if constexpr (sizeof(T) == 4) return launch3<T, 13>(a, st, sms, attr_only);    // 64 KB per row
+        return cudaErrorNotSupported;
     default: return cudaErrorNotSupported;
     }
 }

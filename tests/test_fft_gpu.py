@@ -247,3 +247,38 @@ def test_full_size_roundtrip_and_parseval(log_n):
     unit.exec(got, to_dev(rows, F32), batch=rows.shape[0])
     want = O.fft_packed(rows, n)
     assert rel_l2(O.unpack(got.cpu().numpy().reshape(rows.shape), n, 8), O.unpack(want, n, 8)) < 2e-6
+
+
+@pytest.mark.parametrize("log_n,batch", [(14, 1), (14, 300), (15, 37), (16, 64), (17, 5), (18, 9), (19, 3), (20, 6),
+                                         (20, 1)])
+@pytest.mark.parametrize("dtype", [F32, F64])
+def test_one_launch_four_step_matches_chunked(log_n, batch, dtype, monkeypatch):
+    """The one-launch four-step (all chunks in one persistent grid, device
+    dependency counters, a copy warp per CTA) against the chunked two-launch
+    pipeline: the same arithmetic, so bit-identical, and both against the
+    oracle on a few rows."""
+    n = 1 << log_n
+    if dtype == F64 and batch > 16:
+        batch = 16
+    p = 8 if dtype == F32 else 4
+    rng = np.random.default_rng(300 + log_n)
+    z = normal_cx(rng, batch, n)
+    x = O.pack(z, p, NPD[dtype])
+    unit = fft_unit(n, dtype=dtype)
+    outs = {}
+    for mode in ("chunked", "one-launch"):
+        if mode == "chunked":
+            monkeypatch.setenv("PCX_FOURSTEP", "chunked")
+        else:
+            monkeypatch.delenv("PCX_FOURSTEP", raising=False)
+        fwd = run(unit, x, batch, direction=0)
+        inv = run(unit, fwd, batch, direction=1)
+        outs[mode] = (fwd, inv)
+        unit.status()
+    assert np.array_equal(outs["chunked"][0], outs["one-launch"][0])
+    assert np.array_equal(outs["chunked"][1], outs["one-launch"][1])
+    k = min(batch, 2)
+    want = O.fft_packed(x[:k], n, pack_src=p, pack_dst=p, dtype=NPD[dtype])
+    tol = TOL[NPD[dtype]]
+    assert rel_l2(O.unpack(outs["one-launch"][0][:k], n, p), O.unpack(want, n, p)) < tol
+    assert rel_l2(O.unpack(outs["one-launch"][1], n, p), z) < tol
