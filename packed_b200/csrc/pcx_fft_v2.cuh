@@ -171,12 +171,15 @@ __device__ __forceinline__ void stage_compute_tab(cpx<T> (&v)[E], int t, const c
 __device__ __forceinline__ int pad16(int l) { return l + (l >> 4); }
 
 // Barrier of the threads that share the exchange buffer: the whole block
-// (BARN = 0) or named barrier 1 over the first BARN threads (the compute
-// warps of a block that also has a copy warp).
+// (BARN = 0), the warp (BARN < 0: each transform's threads and exchange rows
+// stay inside one warp) or named barrier 1 over the first BARN threads (the
+// compute warps of a block that also has a copy warp).
 template<int BARN>
 __device__ __forceinline__ void xch_sync() {
     if constexpr (BARN == 0) {
         __syncthreads();
+    } else if constexpr (BARN < 0) {
+        __syncwarp();
     } else {
         asm volatile("bar.sync 1, %0;" ::"n"(BARN) : "memory");
     }

@@ -1,9 +1,12 @@
 // Host side of the overlap-save correlator: handle creation (kernel spectrum
 // computed on the device), the fused correlation launch and its adjoint.
+#include "pcx_fxcorr2d.cuh"
 #include "pcx_fxcorr_kernels.cuh"
 #include "pcx_host.hpp"
+#include "pcx_v2_launch.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 
 using namespace pcxg;
@@ -24,6 +27,12 @@ struct pcx_fxcorr_s {
     size_t      gscratch_bytes = 0;
     int         sms            = 0;
     int         device         = 0;
+    // FP32, N = 2^13 or 2^14: in-CTA four-step form (pcx_fxcorr2d.cuh)
+    void*       x2d            = nullptr;    // one allocation: K permuted | stage tables | twiddles
+    const void* x2_kperm       = nullptr;
+    const void* x2_stw1        = nullptr;
+    const void* x2_stw2        = nullptr;
+    const void* x2_tws         = nullptr;
 };
 
 namespace {
@@ -116,6 +125,62 @@ __global__ void k_scale_pack(const cpx<T>* __restrict__ src, int k, int lp, T* _
     dst[o + P]  = src[i].im;
 }
 
+// K / N from natural order k = k1 + N1*k2 to row-major [k1][k2].
+__global__ void k_perm_spectrum(const cpx<float>* __restrict__ ks, cpx<float>* __restrict__ kp, int log_n1,
+                                int log_n2) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (1 << (log_n1 + log_n2))) return;
+    const int k1 = q >> log_n2, k2 = q & ((1 << log_n2) - 1);
+    kp[q]        = ks[k1 + (k2 << log_n1)];
+}
+
+template<int LOGN>
+int launch_xc2(const xc2_args& a, cudaStream_t st, int sms, bool attr_only) {
+    using C   = xc2_cfg<LOGN>;
+    auto kern = k_fxcorr2d<LOGN>;
+    if (attr_only) {
+        PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        return PCX_OK;
+    }
+    int per_sm = 0;
+    PCX_CUDA_TRY(occupancy_cached(reinterpret_cast<const void*>(kern), C::NT, C::SMEM, &per_sm));
+    const long long grid = std::max<long long>(1, std::min<long long>(a.base.total, (long long)std::max(per_sm, 1) * sms));
+    kern<<<(unsigned)grid, C::NT, C::SMEM, st>>>(a);
+    PCX_CUDA_TRY(cudaGetLastError());
+    return PCX_OK;
+}
+
+// Tables of the in-CTA four-step form; false when it does not apply.
+template<int LOGN>
+int init_xc2(pcx_fxcorr_s* h) {
+    using C         = xc2_cfg<LOGN>;
+    int e1 = 0, e2 = 0;
+    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN1, nullptr, false, 0, &e1));
+    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN2, nullptr, false, 0, &e2));
+    e1                  = (e1 + 1) / 2 * 2;    // 16-byte sections
+    e2                  = (e2 + 1) / 2 * 2;
+    const size_t ntw    = (size_t)C::NB + C::N2 + C::N1;
+    const size_t entries = (size_t)C::N + e1 + e2 + ntw;
+    PCX_CUDA_TRY(cudaMalloc(&h->x2d, entries * sizeof(cpx<float>)));
+    auto* base   = static_cast<cpx<float>*>(h->x2d);
+    auto* kp     = base;
+    auto* s1     = kp + C::N;
+    auto* s2     = s1 + e1;
+    auto* tws    = s2 + e2;
+    k_perm_spectrum<<<(C::N + 255) / 256, 256>>>(static_cast<const cpx<float>*>(h->kspec), kp, C::LOGN1, C::LOGN2);
+    PCX_CUDA_TRY(cudaGetLastError());
+    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN1, s1, false, 0, &e1));
+    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN2, s2, false, 0, &e2));
+    PCX_CUDA_TRY(pcx_gen_twiddles(tws, C::NB, LOGN, 1, false, 0));
+    PCX_CUDA_TRY(pcx_gen_twiddles(tws + C::NB, C::N2, LOGN, C::TT1, false, 0));
+    PCX_CUDA_TRY(pcx_gen_twiddles(tws + C::NB + C::N2, C::N1, LOGN, C::TT2, false, 0));
+    h->x2_kperm = kp;
+    h->x2_stw1  = s1;
+    h->x2_stw2  = s2;
+    h->x2_tws   = tws;
+    return launch_xc2<LOGN>(xc2_args{}, 0, 0, true);
+}
+
 int check_pack(int pack) {
     if (pack < 1 || (pack & (pack - 1)) != 0) {
         return pcx_fail(PCX_ERR_INVALID, "pack size (which is " + std::to_string(pack) + ") is not a power of two");
@@ -182,6 +247,19 @@ int run_xc(pcx_fxcorr_s* h, void* dst, const void* src, size_t len, int pack, si
     a.counter     = h->ctl;
     a.error       = reinterpret_cast<int*>(h->ctl + 1);
     a.kspec       = h->kspec;
+    // in-CTA four-step form: FP32, pack 8, windows on whole packs, rows of
+    // packs 16-byte aligned
+    const bool x2 = h->x2d && pack == 8 && a.in_shift % 8 == 0 &&
+                    (channels == 1 || sstride % 4 == 0) && reinterpret_cast<uintptr_t>(src) % 16 == 0;
+    if (x2) {
+        xc2_args b{};
+        b.base  = a;
+        b.kperm = h->x2_kperm;
+        b.stw1  = h->x2_stw1;
+        b.stw2  = h->x2_stw2;
+        b.tws   = h->x2_tws;
+        return h->log_n == 14 ? launch_xc2<14>(b, st, h->sms, false) : launch_xc2<13>(b, st, h->sms, false);
+    }
     return h->dtype == PCX_F64 ? dispatch_xc<double>(h->log_n, a, h->tw, st, h->sms, false)
                                : dispatch_xc<float>(h->log_n, a, h->tw, st, h->sms, false);
 }
@@ -237,6 +315,10 @@ extern "C" int pcx_fxcorr_create(pcx_fxcorr* out, const void* g, size_t k, int p
         rc = dtype == PCX_F64 ? dispatch_kg<double>(log_n, kg_args{}, nullptr, 0, 0, true)
                               : dispatch_kg<float>(log_n, kg_args{}, nullptr, 0, 0, true);
         if (rc) return fail(rc);
+        if (dtype == PCX_F32 && (log_n == 13 || log_n == 14) && std::getenv("PCX_XC_GENERAL") == nullptr) {
+            rc = log_n == 14 ? init_xc2<14>(h) : init_xc2<13>(h);
+            if (rc) return fail(rc);
+        }
         e = cudaDeviceSynchronize();
         if (e != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
         *out = h;
@@ -251,6 +333,7 @@ extern "C" int pcx_fxcorr_destroy(pcx_fxcorr h) {
     if (h->kspec) cudaFree(h->kspec);
     if (h->ctl) cudaFree(h->ctl);
     if (h->gscratch) cudaFree(h->gscratch);
+    if (h->x2d) cudaFree(h->x2d);
     delete h;
     return PCX_OK;
 }

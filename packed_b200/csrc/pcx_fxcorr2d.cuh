@@ -1,0 +1,312 @@
+// Overlap-save correlation for FP32 blocks of N = N1 * N2 = 2^13 or 2^14
+// points (reference fxcorr.hpp:102-136), one block per CTA at a time.
+//
+// The N-point window sits in shared memory as N1 rows of N2 samples.  Its
+// forward FFT is a four-step inside the CTA, and the inverse runs the same
+// steps backwards, so no step needs the spectrum in natural order:
+//   1. columns: N1-point FFT of every column n2, times W_N^(k1*n2);
+//   2. rows:    N2-point FFT of every row k1 gives X[k1 + N1*k2] in
+//               registers; times conj(K) (K = FFT(g)/N, stored row-major in
+//               the same (k1, k2) order so the loads are coalesced); the
+//               inverse N2-point FFT of the row (as FFT of the conjugate) and
+//               times W_N^(k1*n2) again (the conjugate form of W_N^-(k1*n2));
+//   3. columns: N1-point FFT of every column gives conj(y[n1*N2 + n2]),
+//               written straight to the output.
+// (y[n] = (1/N) sum_k Y[k] W_N^-(nk) with n = n1*N2 + n2, k = k1 + N1*k2
+// splits as W_N1^-(n1*k1) * W_N^-(n2*k1) * W_N2^-(n2*k2).)
+// Each sub-FFT belongs to a group of TT threads inside one warp, 16 points
+// per thread, exchanging through a private padded buffer with warp barriers
+// only; block barriers separate the steps.  The window rows arrive by 1-D
+// bulk copies of the packed signal (one per row of 64-byte packs, converted
+// in place to interleaved complex); rows that reach outside the signal are
+// filled by the threads, with zeros outside.  Once step 3 has read the
+// window, the copies of the CTA's next block start, so they land while step
+// 3 finishes.
+//
+// In place, a block's outputs overwrite samples that the previous block's
+// window reads, so every block publishes "window loaded" (the call's epoch in
+// flags[item]) and waits for its predecessors before writing, as the general
+// kernel does; the waits are bounded (about one second).
+#pragma once
+
+#include "pcx_fft_v2.cuh"
+#include "pcx_fxcorr_kernels.cuh"
+
+namespace pcxg {
+
+template<int LOGN>
+struct xc2_cfg {
+    static constexpr int LOGN1 = (LOGN + 1) / 2;
+    static constexpr int LOGN2 = LOGN / 2;
+    static constexpr int N1    = 1 << LOGN1;
+    static constexpr int N2    = 1 << LOGN2;
+    static constexpr int N     = N1 * N2;
+    using P1                   = splan<LOGN1>;
+    using P2                   = splan<LOGN2>;
+    static constexpr int NT    = 512;
+    static constexpr int TT1   = P1::TT;
+    static constexpr int TT2   = P2::TT;
+    static constexpr int G1    = NT / TT1;    // column groups per round
+    static constexpr int G2    = NT / TT2;    // row groups per round
+    static constexpr int R1    = N2 / G1;     // column rounds
+    static constexpr int R2    = N1 / G2;     // row rounds
+    static constexpr int RS    = N2 + 2;      // window row stride (complex), 2 mod 16
+    static constexpr int WIN   = N1 * RS * 8;
+    using X1                   = xch_blocked<N1, G1>;
+    using X2                   = xch_blocked<N2, G2>;
+    static constexpr int XB    = (X1::size > X2::size ? X1::size : X2::size) * 8;
+    static constexpr int TB1   = stage_tw_smem_bytes<P1, float>();
+    static constexpr int TB2   = stage_tw_smem_bytes<P2, float>();
+    static constexpr int NB    = N / 16;      // W_N^e, e < N/16 (= TT1*N2 = TT2*N1)
+    static constexpr int SMEM  = WIN + XB + TB1 + TB2 + (NB + N2 + N1) * 8;
+    static_assert(P1::E == 16 && P2::E == 16, "16 points per thread");
+    static_assert(TT1 <= 32 && TT2 <= 32 && TT2 >= 2, "sub-FFT groups inside one warp");
+    static_assert(R1 >= 1 && R2 >= 1 && G1 * R1 == N2 && G2 * R2 == N1, "rounds");
+    static_assert(TT1 * N2 == NB && TT2 * N1 == NB, "twiddle split");
+    static_assert(WIN % 16 == 0 && XB % 16 == 0 && TB1 % 16 == 0 && TB2 % 16 == 0, "16-byte sections");
+};
+
+struct xc2_args {
+    xc_args     base;
+    const void* kperm;    // K[k1 + N1*k2] / N at [k1*N2 + k2]
+    const void* stw1;     // stage tables of the N1- and N2-point FFTs
+    const void* stw2;
+    const void* tws;      // W_N^e (e < N/16), W_N^(TT1*n2) (n2 < N2), W_N^(TT2*k1) (k1 < N1)
+};
+
+template<int LOGN>
+__global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
+    using F            = xc2_cfg<LOGN>;
+    using P1           = typename F::P1;
+    using P2           = typename F::P2;
+    constexpr int N1   = F::N1;
+    constexpr int N2   = F::N2;
+    constexpr int NT   = F::NT;
+    constexpr int TT1  = F::TT1;
+    constexpr int TT2  = F::TT2;
+    constexpr int RS   = F::RS;
+    constexpr int E    = 16;
+    const xc_args& a   = A.base;
+    extern __shared__ __align__(128) unsigned char smem[];
+    cpx<float>*          win  = reinterpret_cast<cpx<float>*>(smem);
+    cpx<float>*          xch  = reinterpret_cast<cpx<float>*>(smem + F::WIN);
+    cpx<float>*          tw1  = reinterpret_cast<cpx<float>*>(smem + F::WIN + F::XB);
+    cpx<float>*          tw2  = tw1 + F::TB1 / 8;
+    cpx<float>*          fwb  = tw2 + F::TB2 / 8;    // W_N^e
+    cpx<float>*          fwu1 = fwb + F::NB;         // W_N^(TT1*n2)
+    cpx<float>*          fwu2 = fwu1 + N2;           // W_N^(TT2*k1)
+    __shared__ uint64_t  full;
+    __shared__ long long s_item;
+    __shared__ int       s_rlo;
+    __shared__ int       s_rhi;
+    __shared__ int       s_abort;
+    const int            tid  = threadIdx.x;
+    const float*         src  = reinterpret_cast<const float*>(a.src);
+    float*               dst  = reinterpret_cast<float*>(a.dst);
+    const cpx<float>*    kp   = reinterpret_cast<const cpx<float>*>(A.kperm);
+
+    // constant tables into shared memory
+    stage_tw_to_smem<P1, float>(tw1, A.stw1, tid, NT);
+    stage_tw_to_smem<P2, float>(tw2, A.stw2, tid, NT);
+    for (int i = tid; i < (F::NB + N2 + N1) / 2; i += NT) {
+        reinterpret_cast<uint4*>(fwb)[i] = __ldg(reinterpret_cast<const uint4*>(A.tws) + i);
+    }
+    if (tid == 0) {
+        mbar_init(&full, 1);
+        fence_barrier_init();
+    }
+
+    // channel and window start (samples) of an item
+    auto item_pos = [&](long long item, long long& ch, long long& b0) {
+        ch = item / a.nblk;
+        b0 = (item - ch * a.nblk) * a.step - a.in_shift;
+    };
+    // thread 0: claim the next item and start the copies of its rows that lie
+    // inside [0, len); the threads fill the others
+    auto claim_and_copy = [&]() {
+        const long long item = (long long)atomicAdd(a.counter, 1u);
+        s_item               = item;
+        if (item >= a.total) return;
+        long long ch, b0;
+        item_pos(item, ch, b0);
+        long long r_lo = b0 >= 0 ? 0 : (-b0 + N2 - 1) / N2;
+        long long r_hi = b0 + (long long)N1 * N2 <= a.len ? N1 : (a.len - b0) / N2;
+        r_lo           = r_lo > N1 ? N1 : r_lo;
+        r_hi           = r_hi < r_lo ? r_lo : (r_hi > N1 ? N1 : r_hi);
+        s_rlo          = (int)r_lo;
+        s_rhi          = (int)r_hi;
+        mbar_arrive_expect_tx(&full, (uint32_t)(r_hi - r_lo) * (N2 * 8));
+        const float* base = src + ch * a.src_stride + 2 * b0;    // packed: 2 reals per sample
+        for (long long r = r_lo; r < r_hi; ++r) bulk_g2s(win + r * RS, base + 2 * r * N2, N2 * 8, &full);
+    };
+
+    __syncthreads();
+    if (tid == 0) claim_and_copy();
+    uint32_t phase = 0;
+    for (;;) {
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= a.total) break;
+        const int r_lo = s_rlo, r_hi = s_rhi;
+        long long ch, b0;
+        item_pos(item, ch, b0);
+        // rows outside the copied range: packed samples, zeros outside [0, len)
+        if (r_hi - r_lo < N1) {
+            for (int q = tid; q < N1 * N2; q += NT) {
+                const int r = q / N2, c = q - r * N2;
+                if (r >= r_lo && r < r_hi) continue;
+                const long long pos = b0 + q;
+                float           re = 0.f, im = 0.f;
+                if (pos >= 0 && pos < a.len) {
+                    const long long o = ch * a.src_stride + ((pos >> 3) << 4) + (pos & 7);
+                    re                = src[o];
+                    im                = src[o + 8];
+                }
+                float* row                         = reinterpret_cast<float*>(win + r * RS);
+                row[((c >> 3) << 4) + (c & 7)]     = re;
+                row[((c >> 3) << 4) + (c & 7) + 8] = im;
+            }
+        }
+        const bool ok = mbar_wait_bounded(&full, phase);
+        if (__syncthreads_or(!ok)) {
+            // give up: record it and let the copies in flight land first
+            if (tid == 0) {
+                atomicExch(a.error, 1);
+                mbar_wait_bounded(&full, phase, 100000000ull);
+            }
+            __syncthreads();
+            return;
+        }
+        phase ^= 1;
+        if (a.inplace && tid == 0) {
+            __threadfence();
+            st_release(a.flags + item, a.epoch);    // this window is loaded
+        }
+        // packed -> interleaved, in place, one 64-byte pack per thread and step
+        for (int q = tid; q < N1 * N2 / 8; q += NT) {
+            const int    r  = q / (N2 / 8), p = q - r * (N2 / 8);
+            float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
+            const float4 r0 = w[0], r1 = w[1], i0 = w[2], i1 = w[3];
+            w[0]            = make_float4(r0.x, i0.x, r0.y, i0.y);
+            w[1]            = make_float4(r0.z, i0.z, r0.w, i0.w);
+            w[2]            = make_float4(r1.x, i1.x, r1.y, i1.y);
+            w[3]            = make_float4(r1.z, i1.z, r1.w, i1.w);
+        }
+        __syncthreads();
+
+        // ---------------- step 1: columns, forward, times W_N^(k1*n2)
+        {
+            const int g = tid / TT1, t = tid % TT1;
+            for (int rd = 0; rd < F::R1; ++rd) {
+                const int  n2 = rd * F::G1 + g;
+                cpx<float> v[E];
+                static_for<E>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    v[i]            = win[(t + i * TT1) * RS + n2];
+                });
+                stage_compute_tab<P1, 0>(v, t, tw1);
+                run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                apply_fourstep_tw(v, fwb[t * n2], fwu1[n2], [&](auto ic, cpx<float> o) {
+                    constexpr int i              = decltype(ic)::value;
+                    win[(t + i * TT1) * RS + n2] = o;
+                });
+            }
+        }
+        __syncthreads();
+
+        // ---------------- step 2: rows; spectrum times conj(K) or K; inverse rows
+        {
+            // the U groups of a half-warp take rows S apart, so their window
+            // rows fall in disjoint banks (RS = 2 mod 16)
+            constexpr int S  = TT2 / 2;
+            constexpr int U  = 16 / TT2;
+            const int     g  = tid / TT2, t = tid % TT2;
+            const int     bb = g / U, u = g % U;
+            const int     r0 = (bb / S) * 8 + (bb % S) + u * S;
+            for (int rd = 0; rd < F::R2; ++rd) {
+                const int  k1 = rd * F::G2 + r0;
+                cpx<float> v[E];
+                static_for<E>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    v[i]            = win[k1 * RS + t + i * TT2];
+                });
+                stage_compute_tab<P2, 0>(v, t, tw2);
+                run_stages_tab<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+                // v[i] = X[k1 + N1*k2], k2 = t + i*TT2: conj(X * conj(K)) or conj(X * K)
+                static_for<E>([&](auto ic) {
+                    constexpr int    i = decltype(ic)::value;
+                    const cpx<float> k = ldg_cpx(kp + k1 * N2 + t + i * TT2);
+                    const cpx<float> c = {v[i].re, -v[i].im};
+                    v[i]               = a.conj_kernel ? cmul(c, k) : cmulc(c, k);
+                });
+                stage_compute_tab<P2, 0>(v, t, tw2);
+                run_stages_tab<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+                // v[i] at n2 = t + i*TT2, times W_N^(k1*n2) = W_N^(k1*t) * W_N^(TT2*k1)^i
+                apply_fourstep_tw(v, fwb[k1 * t], fwu2[k1], [&](auto ic, cpx<float> o) {
+                    constexpr int i           = decltype(ic)::value;
+                    win[k1 * RS + t + i * TT2] = o;
+                });
+            }
+        }
+        __syncthreads();
+
+        // ---------------- step 3: columns again; outputs y = conj(.)
+        if (a.inplace) {
+            // the outputs overwrite samples of the windows of the hwait
+            // previous blocks of this channel: wait until those are loaded
+            if (tid == 0) {
+                s_abort              = 0;
+                const long long blk  = item % a.nblk;
+                for (int d = 1; d <= a.hwait && d <= blk && !s_abort; ++d) {
+                    const unsigned* f = a.flags + (item - d);
+                    if (ld_acquire(f) == a.epoch) continue;
+                    const unsigned long long t0 = globaltimer_ns();
+                    while (ld_acquire(f) != a.epoch) {
+                        if (globaltimer_ns() - t0 > XC_WAIT_NS) {
+                            atomicExch(a.error, 1);
+                            s_abort = 1;
+                            break;
+                        }
+                        __nanosleep(256);
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_abort) return;    // every thread leaves together; no copy is in flight
+        }
+        {
+            const int       g    = tid / TT1, t = tid % TT1;
+            const long long e0   = b0 + a.in_shift - a.out_shift;    // output position of window index 0
+            float*          d    = dst + ch * a.dst_stride;
+            for (int rd = 0; rd < F::R1; ++rd) {
+                const int  n2 = rd * F::G1 + g;
+                cpx<float> v[E];
+                static_for<E>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    v[i]            = win[(t + i * TT1) * RS + n2];
+                });
+                if (rd == F::R1 - 1) {
+                    // the window is read: start the next block's copies
+                    fence_proxy_async_smem();
+                    __syncthreads();
+                    if (tid == 0) claim_and_copy();
+                }
+                stage_compute_tab<P1, 0>(v, t, tw1);
+                run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                static_for<E>([&](auto ic) {
+                    constexpr int i  = decltype(ic)::value;
+                    const int     n  = (t + i * TT1) * N2 + n2;    // window index
+                    const int     mo = n - a.out_shift;
+                    if (mo >= 0 && mo < a.step && e0 + n < a.len) {
+                        const long long e = e0 + n;
+                        const long long o = ((e >> 3) << 4) + (e & 7);
+                        __stcs(d + o, v[i].re);
+                        __stcs(d + o + 8, -v[i].im);
+                    }
+                });
+            }
+        }
+    }
+}
+
+}    // namespace pcxg
