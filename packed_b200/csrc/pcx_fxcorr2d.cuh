@@ -182,9 +182,11 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
             __threadfence();
             st_release(a.flags + item, a.epoch);    // this window is loaded
         }
-        // packed -> interleaved, in place, one 64-byte pack per thread and step
+        // packed -> interleaved, in place, one 64-byte pack per thread and step;
+        // consecutive threads take consecutive rows (row stride 65 x 16 bytes),
+        // so each quarter-warp's 16-byte accesses hit eight distinct bank groups
         for (int q = tid; q < N1 * N2 / 8; q += NT) {
-            const int    r  = q / (N2 / 8), p = q - r * (N2 / 8);
+            const int    r  = q % N1, p = q / N1;
             float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
             const float4 r0 = w[0], r1 = w[1], i0 = w[2], i1 = w[3];
             w[0]            = make_float4(r0.x, i0.x, r0.y, i0.y);
