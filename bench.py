@@ -159,16 +159,9 @@ class C2Sweep:
                 "d2h_bytes_per_step": nb, "ms_per_step": ms}
 
     def launches(self):
-        total = 0
-        for lg, u in self.units.items():
-            b = self.points >> lg
-            if lg <= 12:
-                total += 2
-            else:
-                ws = u.workspace_size(b)
-                chunk = max(1, ws // (2 * (1 << lg) * 8))
-                total += 2 * 2 * ((b + chunk - 1) // chunk)
-        return total
+        # one kernel per transform direction: a one-pass kernel for N <= 8192,
+        # the one-launch four-step above
+        return 2 * len(self.log_ns)
 
     def cpu_reference(self, budget_s=12.0):
         import ctypes
@@ -567,9 +560,12 @@ def main() -> None:
         means = {p: statistics.mean(v) for p, v in res["per"].items()}
         if wl.name == "c5":
             ms_step = means["ragged_graph"]
+            nbytes  = wl.bytes_per_step()
         else:
+            # one transform of each size, in its fastest form
             ms_step = sum(min(means[f"{m}:{1 << lg}"] for m in ("plain", "tc_bf16", "tc_tf32")) for lg in wl.log_ns)
-        value = wl.bytes_per_step() * world / (ms_step / 1e3) / 1e9
+            nbytes  = sum(wl.part_bytes(f"plain:{1 << lg}") for lg in wl.log_ns)
+        value = nbytes * world / (ms_step / 1e3) / 1e9
     mean = {p: statistics.mean(v) for p, v in res["per"].items()}
     top = max(mean, key=mean.get)
     ach = wl.part_bytes(top) / (mean[top] / 1e3) / 1e9
