@@ -124,6 +124,11 @@ class C2Sweep:
         self.x = torch.randn(2 * self.points, device=dev, generator=g)
         self.y = torch.empty_like(self.x)
         self.units = {lg: fft_unit(1 << lg) for lg in self.log_ns}
+        # autotuner: time each size's forms on this batch, keep the fastest
+        self.forms = {str(1 << lg): u.tune(self.points >> lg) for lg, u in self.units.items()
+                      if self.tune and lg > 12}
+
+    tune = True
 
     def bytes_per_step(self):
         return len(self.log_ns) * self.points * B_PT * 2
@@ -510,6 +515,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=None, help="log2 complex points per buffer (profiling captures)")
     ap.add_argument("--sizes", type=str, default=None, help="comma list of log2 N (profiling captures)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (built-in form choice)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -520,6 +526,8 @@ def main() -> None:
         wl.channels = max(1, (1 << args.points) // wl.length)
     if args.sizes and hasattr(wl, "log_ns"):
         wl.log_ns = [int(v) for v in args.sizes.split(",")]
+    if args.no_tune:
+        wl.tune = False
     config = wl.config(world)
 
     if args.impl == "reference":
@@ -546,6 +554,8 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     res = run(args, wl, rank, world)
+    if getattr(wl, "forms", None):
+        config["forms"] = wl.forms    # the autotuner's choice per four-step size
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -76,6 +76,24 @@ int pcx_plan_status(pcx_plan plan);
 /* Bytes of scratch an exec of this plan uses for `batch` rows (0 for n <= 4096). */
 size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
 
+/* Forms of a transform larger than 4096 points (pcx_plan_tune). */
+#define PCX_FORM_DEFAULT 0  /* built-in choice */
+#define PCX_FORM_ONEPASS 1  /* one shared-memory pass (FP32 n = 8192) */
+#define PCX_FORM_FUSED 2    /* four-step, the whole batch in one persistent launch */
+#define PCX_FORM_CHUNKED 3  /* four-step, two launches per L2-sized scratch chunk */
+
+/*
+ * Autotuner (no reference counterpart: the reference picks its radix
+ * schedule at compile time).  Times the forms this plan supports, and their
+ * tile-schedule / chunk-size variants, on `batch` rows of scratch data
+ * (forward, natural order, default pack; at most 512 MB per buffer) on
+ * `stream`, and makes the fastest the plan's form for later execs that use
+ * the plan's own scratch (pcx_fft_exec).  Allocates and frees its buffers;
+ * synchronises.  *form_out (if not NULL) receives the PCX_FORM_* chosen.
+ * A plan for n <= 4096 has one form: PCX_FORM_DEFAULT, nothing is timed.
+ */
+int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* form_out);
+
 /*
  * Batched transform of `batch` rows.  Replaces
  *   fft_unit::fft_raw<PD,PS>(dest, src[, src_size])     fft.hpp:624-681

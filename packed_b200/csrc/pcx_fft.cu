@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 #include <string>
 
 namespace pcxg {
@@ -362,6 +363,88 @@ extern "C" int pcx_plan_status(pcx_plan plan) {
     });
 }
 
+extern "C" int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* form_out) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        pcx_plan_s* p = plan;
+        if (form_out) *form_out = p->form;
+        if (!p->two_pass || batch == 0) return PCX_OK;
+        struct cand {
+            int    form;
+            int    rounds;
+            size_t chunk;
+        };
+        std::vector<cand> cands;
+        if (p->stw_one) cands.push_back({PCX_FORM_ONEPASS, 3, 0});
+        if (p->fs_tc > 0) {
+            for (int r: {2, 3, 6}) cands.push_back({PCX_FORM_FUSED, r, 0});
+        }
+        for (size_t mb: {24, 48}) cands.push_back({PCX_FORM_CHUNKED, 3, mb << 20});
+        const size_t eb   = p->elem_bytes();
+        const size_t rows = std::max<size_t>(1, std::min(batch, ((size_t)512 << 20) / (p->n * eb)));
+        const size_t bytes = rows * p->n * eb;
+        cudaStream_t st    = static_cast<cudaStream_t>(stream);
+        void *       x = nullptr, *y = nullptr;
+        cudaEvent_t  e0 = nullptr, e1 = nullptr;
+        auto         cleanup = [&]() {
+            if (x) cudaFree(x);
+            if (y) cudaFree(y);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        };
+        const int   keep_form = p->form, keep_rounds = p->fs_rounds;
+        const size_t keep_chunk = p->chunk_bytes;
+        cudaError_t e = cudaMalloc(&x, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&y, bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, bytes, st);
+        if (e == cudaSuccess) e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        if (e != cudaSuccess) {
+            cleanup();
+            return pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e));
+        }
+        const size_t row = 2 * p->n;
+        float        best_ms = 0.f;
+        cand         best    = {keep_form, keep_rounds, keep_chunk};
+        for (const cand& c: cands) {
+            p->form        = c.form;
+            p->fs_rounds   = c.rounds;
+            p->chunk_bytes = c.chunk;
+            int rc = PCX_OK;
+            for (int w = 0; w < 2 && rc == PCX_OK; ++w) {
+                rc = pcx_fft_run(p, y, x, p->n, p->dtype == PCX_F64 ? 4 : 8, p->dtype == PCX_F64 ? 4 : 8,
+                                 PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
+            }
+            if (rc == PCX_OK) e = cudaEventRecord(e0, st);
+            for (int it = 0; it < 3 && rc == PCX_OK && e == cudaSuccess; ++it) {
+                rc = pcx_fft_run(p, y, x, p->n, p->dtype == PCX_F64 ? 4 : 8, p->dtype == PCX_F64 ? 4 : 8,
+                                 PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
+            }
+            if (rc == PCX_OK && e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (rc == PCX_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (rc == PCX_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (rc != PCX_OK || e != cudaSuccess) {
+                p->form        = keep_form;
+                p->fs_rounds   = keep_rounds;
+                p->chunk_bytes = keep_chunk;
+                cleanup();
+                return rc != PCX_OK ? rc : pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e));
+            }
+            if (best_ms == 0.f || ms < best_ms) {
+                best_ms = ms;
+                best    = c;
+            }
+        }
+        p->form        = best.form;
+        p->fs_rounds   = best.rounds;
+        p->chunk_bytes = best.chunk;
+        cleanup();
+        if (form_out) *form_out = p->form;
+        return PCX_OK;
+    });
+}
+
 extern "C" size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch) {
     if (!plan || !plan->two_pass) return 0;
     return 2 * plan->chunk_rows(batch) * plan->n * plan->elem_bytes();
@@ -488,7 +571,8 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         return PCX_OK;
     }
 
-    if (p->stw_one && src_len == n && io.lp_src == lp_def && io.lp_dst == lp_def &&
+    const bool tuned_one = ws || p->form == PCX_FORM_DEFAULT || p->form == PCX_FORM_ONEPASS;
+    if (p->stw_one && tuned_one && src_len == n && io.lp_src == lp_def && io.lp_dst == lp_def &&
         (batch == 1 || (sstride % vreals == 0 && dstride % vreals == 0))) {
         // one-pass form of a two-pass size
         v3_args t3{};
@@ -516,6 +600,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     // (caller's stream) runs beside the row pass of chunk c (side stream).
     size_t       chunk = chunk_cap ? std::min(chunk_cap, p->chunk_rows(batch)) : p->chunk_rows(batch);
     const size_t per   = n * eb;
+    if (!ws && p->chunk_bytes > 0) chunk = std::max<size_t>(1, std::min(batch, p->chunk_bytes / per));
     void*        scr   = ws;
     int          nbuf  = 2;
     if (!scr) {
@@ -555,14 +640,16 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     // One launch over the whole batch (plan-owned scratch slots and counters);
     // PCX_FOURSTEP=chunked selects the two-launch chunk pipeline below.
     const char* fs_env = std::getenv("PCX_FOURSTEP");
-    if (!ws && col_hot && row_hot && use_tma && p->fs_tc > 0 && !(fs_env && std::strcmp(fs_env, "chunked") == 0)) {
+    const bool tuned_fused = p->form == PCX_FORM_DEFAULT || p->form == PCX_FORM_FUSED;
+    if (!ws && tuned_fused && col_hot && row_hot && use_tma && p->fs_tc > 0 &&
+        !(fs_env && std::strcmp(fs_env, "chunked") == 0)) {
         const long long per_t = p->fs_tc + p->fs_tr;
         // a row tile runs about `rounds` rounds of items (one item per CTA)
         // after its transform's column tiles, and a slot is rewritten about as
         // long after its row tiles, so both dependencies have usually cleared
         // by the time the copy warp reaches them
         const char*     re     = std::getenv("PCX_FS_ROUNDS");
-        const long long rounds = re && std::atol(re) > 0 ? std::atol(re) : 3;
+        const long long rounds = re && std::atol(re) > 0 ? std::atol(re) : p->fs_rounds;
         long long       lag    = (rounds * p->sms + per_t - 1) / per_t;
         lag                    = std::max<long long>(1, std::min<long long>(lag, (long long)batch));
         const long long nslot  = std::min<long long>((long long)batch, 2 * lag + 2);

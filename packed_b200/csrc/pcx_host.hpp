@@ -113,6 +113,10 @@ struct pcx_plan_s {
     int    fs_tr    = 0;
     int*   fs_ctr   = nullptr;    // its dependency counters, 2 per transform
     size_t fs_ctr_n = 0;
+    // form of the plan-owned-scratch path for n > 4096, set by pcx_plan_tune
+    int    form        = 0;    // PCX_FORM_*: 0 built-in choice
+    int    fs_rounds   = 3;    // one-launch four-step: dependency distance in rounds of tiles
+    size_t chunk_bytes = 0;    // chunked four-step: scratch per buffer (0: 24 MB)
     int    sms      = 148;
     int*   err      = nullptr;    // device flag: a bounded wait in a kernel gave up
 

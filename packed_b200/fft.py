@@ -157,6 +157,14 @@ class fft_unit:
     def workspace_size(self, batch: int = 1) -> int:
         return int(_lib.lib().pcx_plan_workspace_size(self._plan, batch))
 
+    FORMS = {0: "default", 1: "one-pass", 2: "one-launch four-step", 3: "chunked four-step"}
+
+    def tune(self, batch: int = 1, stream=None) -> str:
+        """Time this size's forms on `batch` rows and keep the fastest (pcx_plan_tune)."""
+        form = ctypes.c_int(0)
+        _lib.check(_lib.lib().pcx_plan_tune(self._plan, batch, _stream_ptr(stream), ctypes.byref(form)))
+        return self.FORMS.get(form.value, str(form.value))
+
     # ---------------------------------------------------------- raw calls
     def exec(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
              batch: int = 1, pack_dst: int | None = None, pack_src: int | None = None, src_len: int = 0,

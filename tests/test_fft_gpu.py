@@ -282,3 +282,27 @@ def test_one_launch_four_step_matches_chunked(log_n, batch, dtype, monkeypatch):
     tol = TOL[NPD[dtype]]
     assert rel_l2(O.unpack(outs["one-launch"][0][:k], n, p), O.unpack(want, n, p)) < tol
     assert rel_l2(O.unpack(outs["one-launch"][1], n, p), z) < tol
+
+
+@pytest.mark.parametrize("log_n,batch", [(13, 64), (14, 40), (16, 8), (20, 3)])
+def test_tune_picks_a_form_and_keeps_parity(log_n, batch):
+    """pcx_plan_tune times the forms of the size and keeps the fastest; the
+    transform stays within the FP32 bar of the oracle whatever it picked."""
+    n = 1 << log_n
+    unit = fft_unit(n, dtype=F32)
+    form = unit.tune(batch)
+    assert form in ("one-pass", "one-launch four-step", "chunked four-step")
+    rng = np.random.default_rng(400 + log_n)
+    z = normal_cx(rng, batch, n)
+    x = O.pack(z, 8)
+    got = run(unit, x, batch, direction=0)
+    unit.status()
+    k = min(batch, 2)
+    want = O.fft_packed(x[:k], n, pack_src=8, pack_dst=8)
+    assert rel_l2(O.unpack(got[:k], n, 8), O.unpack(want, n, 8)) < TOL[np.float32]
+    back = run(unit, got, batch, direction=1)
+    assert rel_l2(O.unpack(back, n, 8), z) < TOL[np.float32]
+
+
+def test_tune_small_size_has_one_form():
+    assert fft_unit(1024).tune(16) == "default"
