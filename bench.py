@@ -330,12 +330,14 @@ class C3Fxcorr:
 class C4TensorCore:
     """Tensor-core split-precision FFT against the plain FP32 path, batch 4096."""
     name = "c4"
-    log_ns = [8, 10, 12]
+    log_ns = [8, 10, 12, 14, 16]
+    tc_max = 12    # the tensor-core form covers N <= 4096
     batch = 4096
 
     def config(self, world):
-        return {"workload": "C4: N in {256, 1024, 4096}, batch 4096, complex64 N(0,1) + 1e-3 tone at a seeded bin "
-                            "(seed 4); tensor-core split-bf16 and split-tf32 forward vs plain FP32 forward",
+        return {"workload": "C4: N in {256, 1024, 4096, 16384, 65536}, batch 4096, complex64 N(0,1) + 1e-3 tone at "
+                            "a seeded bin (seed 4); tensor-core split-bf16 and split-tf32 forward (N <= 4096) vs "
+                            "plain FP32 forward",
                 "global_batch_points": sum(self.batch << lg for lg in self.log_ns) * world,
                 "l2": "inputs 8-128 MiB per size; timed steps back to back",
                 "parallelism": f"independent shards x{world}"}
@@ -347,19 +349,32 @@ class C4TensorCore:
         rng = np.random.default_rng(4)
         for lg in self.log_ns:
             n = 1 << lg
-            z = rng.standard_normal((self.batch, n)) + 1j * rng.standard_normal((self.batch, n))
-            k = rng.integers(0, n, self.batch)
+            # the first 16 rows (the accuracy sample) come from numpy; the rest,
+            # same distribution, from the device generator
+            rows = 16 if lg > self.tc_max else self.batch
+            z = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
+            k = rng.integers(0, n, rows)
             z += 1e-3 * np.exp(2j * np.pi * k[:, None] * np.arange(n)[None, :] / n)
-            a = np.zeros((self.batch, n // 8, 2, 8), np.float32)
-            a[:, :, 0, :] = z.real.reshape(self.batch, -1, 8)
-            a[:, :, 1, :] = z.imag.reshape(self.batch, -1, 8)
+            a = np.zeros((rows, n // 8, 2, 8), np.float32)
+            a[:, :, 0, :] = z.real.reshape(rows, -1, 8)
+            a[:, :, 1, :] = z.imag.reshape(rows, -1, 8)
             self.z[lg] = (z[:16], k[:16])
-            self.x[lg] = torch.as_tensor(a.reshape(-1)).to(dev)
+            if rows == self.batch:
+                self.x[lg] = torch.as_tensor(a.reshape(-1)).to(dev)
+            else:
+                g = torch.Generator(device=dev).manual_seed(4)
+                self.x[lg] = torch.randn(self.batch * 2 * n, device=dev, generator=g)
+                self.x[lg][: rows * 2 * n] = torch.as_tensor(a.reshape(-1)).to(dev)
             self.y[lg] = torch.empty_like(self.x[lg])
             self.units[lg] = fft_unit(n)
+            if lg > 12:
+                self.units[lg].tune(self.batch)
+
+    def forms_of(self, lg):
+        return ("plain", "tc_bf16", "tc_tf32") if lg <= self.tc_max else ("plain",)
 
     def parts(self):
-        return [f"{m}:{1 << lg}" for lg in self.log_ns for m in ("plain", "tc_bf16", "tc_tf32")]
+        return [f"{m}:{1 << lg}" for lg in self.log_ns for m in self.forms_of(lg)]
 
     def _split(self, key):
         m, n = key.split(":")
@@ -388,7 +403,7 @@ class C4TensorCore:
             n = 1 << lg
             z, k = self.z[lg]
             want = np.fft.fft(z, axis=-1)
-            for m in ("plain", "tc_bf16", "tc_tf32"):
+            for m in self.forms_of(lg):
                 self.run_part(f"{m}:{n}")
                 torch.cuda.synchronize()
                 a = self.y[lg][: 16 * 2 * n].cpu().numpy().astype(np.float64).reshape(16, -1, 2, 8)
@@ -581,7 +596,7 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     res = run(args, wl, rank, world)
-    if getattr(wl, "forms", None):
+    if isinstance(getattr(wl, "forms", None), dict):
         config["forms"] = wl.forms    # the autotuner's choice per four-step size
     if world > 1:
         import torch.distributed as dist
@@ -603,7 +618,7 @@ def main() -> None:
             nbytes  = wl.part_bytes("1024")
         else:
             # one transform of each size, in its fastest form
-            ms_step = sum(min(means[f"{m}:{1 << lg}"] for m in ("plain", "tc_bf16", "tc_tf32")) for lg in wl.log_ns)
+            ms_step = sum(min(means[f"{m}:{1 << lg}"] for m in wl.forms_of(lg)) for lg in wl.log_ns)
             nbytes  = sum(wl.part_bytes(f"plain:{1 << lg}") for lg in wl.log_ns)
         value = nbytes * world / (ms_step / 1e3) / 1e9
     mean = {p: statistics.mean(v) for p, v in res["per"].items()}

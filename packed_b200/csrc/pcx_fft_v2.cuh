@@ -485,6 +485,24 @@ struct v3_args {
     int*        error;    // set when a bounded wait gives up
 };
 
+// Read (re, im) stored `pk_off` reals apart at `o`; lanes with bit SW set
+// fetch the imaginary part first, so the two halves of each shared-memory
+// wavefront hit disjoint banks.
+template<class T, int SW>
+__device__ __forceinline__ cpx<T> lds_swapped(const T* base, int o, int pk_off) {
+    const bool sw = (threadIdx.x & SW) != 0;
+    const T    x0 = base[o + (sw ? pk_off : 0)];
+    const T    x1 = base[o + (sw ? 0 : pk_off)];
+    return {sw ? x1 : x0, sw ? x0 : x1};
+}
+// The matching store.
+template<class T, int SW>
+__device__ __forceinline__ void sts_swapped(T* base, int o, int pk_off, T re, T im) {
+    const bool sw        = (threadIdx.x & SW) != 0;
+    base[o + (sw ? pk_off : 0)] = sw ? im : re;
+    base[o + (sw ? 0 : pk_off)] = sw ? re : im;
+}
+
 template<int TT>
 __host__ __device__ constexpr int single3_pad() {
     return TT >= 32 ? 0 : (TT >= 8 ? 8 : 4);
@@ -523,6 +541,10 @@ __global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
     constexpr int TILE  = M * RS;
     constexpr int ROWB  = 2 * L * (int)sizeof(T);
     constexpr int V     = 16 / (int)sizeof(T);
+    // a warp inside one row: its two halves read reals / imaginaries on
+    // disjoint banks by swapping the order in half of the lanes (rows of fewer
+    // than 32 threads keep the plain order: their rows are padded instead)
+    constexpr int SW    = TT >= 32 ? (sizeof(T) == 8 ? 8 : 16) : 0;
     using X             = xch_blocked<L, M>;
     static_assert(X::size * 2 >= TILE, "staging fits the exchange buffer");
     static_assert((RS * (int)sizeof(T)) % 16 == 0, "rows stay 16-byte aligned");
@@ -588,8 +610,8 @@ __global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
             constexpr int  i  = decltype(ic)::value;
             const uint32_t p  = order_pos(t + i * TT, a.order_in, LOGL);
             const int      o  = m * RS + pk<LP>((int)p);
-            const T        re = in[o], im = in[o + PK];
-            v[i]              = {re, a.conj_in ? -im : im};
+            const cpx<T>   x  = lds_swapped<T, SW>(in, o, PK);    // halves of a warp on disjoint banks
+            v[i]              = {x.re, a.conj_in ? -x.im : x.im};
         });
         fence_proxy_async_smem();
         __syncthreads();    // stage s consumed: refill it with the tile after next
@@ -607,8 +629,7 @@ __global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
                 constexpr int  g = i % G, j = i / G;
                 const uint32_t kf = stage_out_index<P, S>(t, g, j);
                 const int      o  = m * RS + pk<LP>((int)order_pos(kf, a.order_out, LOGL));
-                stg[o]            = v[i].re * sc;
-                stg[o + PK]       = v[i].im * sim;
+                sts_swapped<T, SW>(stg, o, PK, v[i].re * sc, v[i].im * sim);
             });
         }
         __syncthreads();
@@ -637,17 +658,6 @@ namespace pcxg {
 // (column pass: 3-D tensor copies of N1 x 64-byte row segments; row pass:
 // one bulk copy per scratch row into padded rows), outputs are written from
 // registers as in the direct kernels.
-
-// Read (re, im) stored `pk_off` reals apart at `o`; lanes with bit SW set
-// fetch the imaginary part first, so the two halves of each shared-memory
-// wavefront hit disjoint banks.
-template<class T, int SW>
-__device__ __forceinline__ cpx<T> lds_swapped(const T* base, int o, int pk_off) {
-    const bool sw = (threadIdx.x & SW) != 0;
-    const T    x0 = base[o + (sw ? pk_off : 0)];
-    const T    x1 = base[o + (sw ? 0 : pk_off)];
-    return {sw ? x1 : x0, sw ? x0 : x1};
-}
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
     asm volatile(
