@@ -113,6 +113,19 @@ int pcx_fft_exec(pcx_plan plan, void* dst, const void* src, size_t src_len, int 
                  int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,
                  void* stream);
 
+/*
+ * Transform across vectors.  Replaces fft_unit_par::operator()(dest, source)
+ *   (fft.hpp:2167-2572; its own test is disabled in the reference,
+ *   tests/test_fft.cpp:719-754)
+ * dst and src are host arrays of `count` (= plan size) device pointers, each
+ * to a vector of `len` elements at pack pack_dst / pack_src.  For every
+ * element position p < len, the plan's transform of src[0][p] .. src[count-1][p]
+ * is written to dst[0][p] .. dst[count-1][p] (forward, or inverse scaled by
+ * 1/count when normalize).  The plan keeps a gather buffer of len rows.
+ */
+int pcx_fft_par_exec(pcx_plan plan, void* const* dst, const void* const* src, size_t count, size_t len,
+                     int pack_dst, int pack_src, int direction, int normalize, void* stream);
+
 /* As pcx_fft_exec with caller-provided scratch (>= pcx_plan_workspace_size). */
 int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
                     int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,

@@ -20,6 +20,8 @@
 #include "vector.hpp"
 
 #include <memory>
+#include <ranges>
+#include <vector>
 
 namespace pcxo {
 
@@ -271,6 +273,105 @@ private:
     [[no_unique_address]] allocator_type         m_alloc;
     std::unique_ptr<pcx_plan_s, plan_deleter>    m_plan;
     cudaStream_t                                 m_stream = nullptr;
+};
+
+// ---- transform across vectors (reference fft.hpp:2167-2572)
+namespace detail_ {
+template<typename R>
+decltype(auto) range_vector(R&& elem) {
+    if constexpr (std::is_pointer_v<std::remove_cvref_t<R>>) {
+        return *elem;
+    } else {
+        return std::forward<R>(elem);
+    }
+}
+}    // namespace detail_
+
+template<typename T, typename R>
+concept range_of_complex_vector_of =
+    std::ranges::range<R> &&
+    complex_vector_of<T, std::remove_pointer_t<std::remove_cvref_t<std::ranges::range_value_t<R>>>>;
+
+// fft_unit_par(size)(dest, source): dest and source are ranges of `size`
+// vectors of equal length L; for every element position p < L the size-point
+// transform of source[0][p] .. source[size-1][p] goes to dest[0][p] ..
+// dest[size-1][p].  The reference's version is broken (its own test is
+// disabled, tests/test_fft.cpp:719-754); this one computes that definition.
+template<typename T,
+         fft_order Order     = fft_order::normal,
+         typename Allocator  = managed_allocator<T>,
+         uZ NodeSizeStrategy = 4>
+    requires(std::same_as<T, float> || std::same_as<T, double>)
+class fft_unit_par {
+public:
+    using real_type      = T;
+    using allocator_type = Allocator;
+    using size_type      = uZ;
+
+    explicit fft_unit_par(uZ size, allocator_type allocator = allocator_type{})
+    : m_size(size)
+    , m_alloc(allocator) {
+        pcx_plan p = nullptr;
+        detail_::check(pcx_plan_create(&p, size, detail_::dtype_code<T>(), static_cast<int>(Order), 2048));
+        m_plan.reset(p);
+    }
+
+    [[nodiscard]] auto size() const -> uZ { return m_size; }
+    void               set_stream(cudaStream_t s) { m_stream = s; }
+
+    template<typename DestR_, typename SrcR_>
+        requires range_of_complex_vector_of<T, DestR_> && range_of_complex_vector_of<T, SrcR_>
+    void operator()(DestR_& dest, const SrcR_& source) {
+        using dv = std::remove_pointer_t<std::remove_cvref_t<std::ranges::range_value_t<DestR_>>>;
+        using sv = std::remove_pointer_t<std::remove_cvref_t<std::ranges::range_value_t<SrcR_>>>;
+        using dt = cx_vector_traits<dv>;
+        using st = cx_vector_traits<sv>;
+        const uZ nd = static_cast<uZ>(std::ranges::distance(dest));
+        const uZ ns = static_cast<uZ>(std::ranges::distance(source));
+        if (nd != m_size) {
+            throw std::invalid_argument(std::string("destination size (which is ") + std::to_string(nd) +
+                                        " is not equal to fft size (which is " + std::to_string(m_size) + ")");
+        }
+        if (ns != m_size) {
+            throw std::invalid_argument(std::string("source size (which is ") + std::to_string(ns) +
+                                        " is not equal to fft size (which is " + std::to_string(m_size) + ")");
+        }
+        std::vector<void*>       dptr;
+        std::vector<const void*> sptr;
+        std::vector<std::unique_ptr<detail_::device_view<T>>> staged;
+        uZ len = 0;
+        bool first = true;
+        for (auto&& e: dest) {
+            auto&    v = detail_::range_vector(e);
+            const uZ n = dt::size(v);
+            if (first) len = n;
+            first = false;
+            if (n != len) throw std::invalid_argument("all vectors of a parallel transform have the same size");
+            staged.push_back(std::make_unique<detail_::device_view<T>>(dt::re_data(v), detail_::real_size(n, dt::pack_size), false));
+            dptr.push_back(staged.back()->get());
+        }
+        const uZ nstaged_dest = staged.size();
+        for (auto&& e: source) {
+            auto&    v = detail_::range_vector(e);
+            if (st::size(v) != len) throw std::invalid_argument("all vectors of a parallel transform have the same size");
+            staged.push_back(std::make_unique<detail_::device_view<T>>(const_cast<T*>(st::re_data(v)),
+                                                                       detail_::real_size(len, st::pack_size), true));
+            sptr.push_back(staged.back()->get());
+        }
+        detail_::check(pcx_fft_par_exec(m_plan.get(), dptr.data(), sptr.data(), m_size, len, (int)dt::pack_size,
+                                        (int)st::pack_size, PCX_FORWARD, 0, m_stream));
+        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        for (uZ i = 0; i < nstaged_dest; ++i) staged[i]->commit();
+    }
+
+private:
+    struct plan_deleter {
+        void operator()(pcx_plan p) const noexcept { pcx_plan_destroy(p); }
+    };
+    uZ                                        m_size;
+    [[no_unique_address]] allocator_type      m_alloc;
+    std::unique_ptr<pcx_plan_s, plan_deleter> m_plan;
+    cudaStream_t                              m_stream = nullptr;
 };
 
 }    // namespace pcxo

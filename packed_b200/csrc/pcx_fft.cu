@@ -321,6 +321,9 @@ void pcx_plan_s::release() {
     if (stw) cudaFree(stw);
     if (stw_one) cudaFree(stw_one);
     if (fs_ctr) cudaFree(fs_ctr);
+    if (par_buf) cudaFree(par_buf);
+    par_buf   = nullptr;
+    par_bytes = 0;
     if (scratch) cudaFree(scratch);
     if (side) cudaStreamDestroy(side);
     for (int i = 0; i < 2; ++i) {

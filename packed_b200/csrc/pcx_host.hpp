@@ -117,6 +117,10 @@ struct pcx_plan_s {
     int    form        = 0;    // PCX_FORM_*: 0 built-in choice
     int    fs_rounds   = 3;    // one-launch four-step: dependency distance in rounds of tiles
     size_t chunk_bytes = 0;    // chunked four-step: scratch per buffer (0: 24 MB)
+    // transforms across vectors (pcx_fft_par_exec): pointer arrays + gathered rows
+    void*      par_buf   = nullptr;
+    size_t     par_bytes = 0;
+    std::mutex par_mu;
     int    sms      = 148;
     int*   err      = nullptr;    // device flag: a bounded wait in a kernel gave up
 

@@ -263,6 +263,39 @@ class fft_unit:
         return g_in
 
 
+class fft_unit_par(fft_unit):
+    """Transform across vectors (reference fft.hpp:2167-2572).
+
+    ``fft_unit_par(size, dtype=torch.float32, order=fft_order.normal)``;
+    ``unit(dest, source)`` takes two sequences of ``size`` vectors of equal
+    length L and, for every element position p < L, writes the transform of
+    ``source[0][p] .. source[size-1][p]`` to ``dest[0][p] .. dest[size-1][p]``.
+    """
+
+    def __init__(self, size: int, dtype: torch.dtype = torch.float32, order: fft_order = fft_order.normal):
+        super().__init__(size, 2048, dtype, order)
+
+    def __call__(self, dest, source, *, inverse: bool = False, normalized: bool = True, stream=None) -> None:
+        dest, source = list(dest), list(source)
+        for name, vs in (("destination", dest), ("source", source)):
+            if len(vs) != self._n:
+                raise ValueError(f"{name} size (which is {len(vs)} is not equal to fft size (which is {self._n})")
+        length = dest[0].size()
+        for v in dest + source:
+            if v.size() != length:
+                raise ValueError("all vectors of a parallel transform have the same size")
+            if v.dtype != self._dtype:
+                raise TypeError("data type does not match the fft_unit_par")
+        pd, ps = dest[0].pack_size, source[0].pack_size
+        if any(v.pack_size != pd for v in dest) or any(v.pack_size != ps for v in source):
+            raise ValueError("all vectors of one side share one pack size")
+        arr = ctypes.c_void_p * self._n
+        dptr = arr(*[v.data.data_ptr() for v in dest])
+        sptr = arr(*[v.data.data_ptr() for v in source])
+        _lib.check(_lib.lib().pcx_fft_par_exec(self._plan, dptr, sptr, self._n, length, pd, ps, int(inverse),
+                                               int(normalized), _stream_ptr(stream)))
+
+
 class fxcorr_unit:
     """Overlap-save cross-correlator (reference fxcorr.hpp:44-147).
 

@@ -152,6 +152,35 @@ int main() {
         std::vector<cd> back(rows[2 * ny + 1].begin(), rows[2 * ny + 1].begin() + 512);
         expect(rel_err(one, back) < 2e-6, "fft_unit on an md row slice", rel_err(one, back));
     }
+    {    // fft_unit_par (fft.hpp:2167): the reference test's pattern, tests/test_fft.cpp:700-754
+        for (std::size_t size: {64u, 512u, 4096u}) {
+            std::vector<pcxo::vector<float>> st_par(size), out(size);
+            std::vector<cd>                  col(size);
+            for (std::size_t i = 0; i < size; ++i) {
+                st_par[i] = pcxo::vector<float>(128);
+                out[i]    = pcxo::vector<float>(128);
+                auto val  = std::exp(std::complex<float>(0, 2 * pi * i / size * 13.37f));
+                for (std::size_t p = 0; p < 128; ++p) st_par[i][p] = val * float(1 + p % 3);
+                col[i] = cd(val);
+            }
+            pcxo::fft_unit_par<float> par_unit(size);
+            par_unit(out, st_par);
+            const auto      X = dft(col, -1);
+            double          worst = 0;
+            for (std::size_t p: {0u, 1u, 2u, 127u}) {
+                std::vector<std::complex<float>> got(size);
+                std::vector<cd>                  want(size);
+                for (std::size_t i = 0; i < size; ++i) {
+                    got[i]  = out[i][p].value();
+                    want[i] = X[i] * double(1 + p % 3);
+                }
+                worst = std::max(worst, rel_err(got, want));
+            }
+            char what[64];
+            std::snprintf(what, sizeof what, "fft_unit_par size %zu x 128", size);
+            expect(worst < 2e-6, what, worst);
+        }
+    }
     {    // exceptions keep the reference's types and messages
         bool thrown = false;
         try {

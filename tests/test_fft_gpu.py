@@ -306,3 +306,34 @@ def test_tune_picks_a_form_and_keeps_parity(log_n, batch):
 
 def test_tune_small_size_has_one_form():
     assert fft_unit(1024).tune(16) == "default"
+
+
+@pytest.mark.parametrize("n,length,pd,ps,dtype", [(64, 37, 8, 8, F32), (1024, 100, 1, 8, F32), (16384, 9, 8, 2, F32),
+                                                  (8, 5, 4, 4, F32), (256, 33, 4, 1, F64)])
+def test_fft_unit_par_across_vectors(n, length, pd, ps, dtype):
+    """fft_unit_par (reference fft.hpp:2167): for every element position p the
+    n-point transform runs across the n vectors; checked against numpy's FP64
+    FFT along that axis, forward and normalised inverse, mixed pack widths."""
+    from packed_b200 import fft_unit_par
+    npd = np.float64 if dtype == F64 else np.float32
+    rng = np.random.default_rng(500 + n + length)
+    z = normal_cx(rng, n, length)
+    src = [vector.from_complex(z[i], dtype=dtype, pack=ps) for i in range(n)]
+    dst = [vector(length, dtype=dtype, pack=pd) for _ in range(n)]
+    unit = fft_unit_par(n, dtype=dtype)
+    unit(dst, src)
+    torch.cuda.synchronize()
+    got = np.stack([v.to_complex() for v in dst])
+    want = np.fft.fft(z, axis=0)
+    assert rel_l2(got, want) < TOL[npd]
+    back = [vector(length, dtype=dtype, pack=ps) for _ in range(n)]
+    unit(back, dst, inverse=True)
+    torch.cuda.synchronize()
+    assert rel_l2(np.stack([v.to_complex() for v in back]), z) < TOL[npd]
+
+
+def test_fft_unit_par_errors():
+    from packed_b200 import fft_unit_par
+    unit = fft_unit_par(16)
+    with pytest.raises(ValueError, match="is not equal to fft size"):
+        unit([vector(4) for _ in range(15)], [vector(4) for _ in range(16)])
