@@ -552,6 +552,19 @@ WORKLOADS = {"c2": C2Sweep, "c1": C1, "c3": C3Fxcorr, "c4": C4TensorCore, "c5": 
 
 
 # ----------------------------------------------------------------- driver
+def max_over_ranks(torch, dist, value: float, device) -> float:
+    """The slowest rank's step time: every rank transforms its own shard of
+    the same size (weak scaling), and the job is done when the last one is."""
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_rank_step: float, world: int, ms_step: float) -> float:
+    """Aggregate GB/s of all ranks: every rank moves bytes_per_rank_step per step."""
+    return bytes_per_rank_step * world / (ms_step / 1e3) / 1e9
+
+
 def run(args, wl, rank, world):
     import torch
     import torch.distributed as dist
@@ -590,9 +603,7 @@ def run(args, wl, rank, world):
         for p in wl.parts():
             per[p].append(ev[s][p][0].elapsed_time(ev[s][p][1]))
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
+        ms = max_over_ranks(torch, dist, ms, dev)
     e2e = wl.e2e(torch, stream) if rank == 0 else None
     return {"ms": ms, "per": per, "clocks": clk.summary(), "e2e": e2e}
 
@@ -655,7 +666,7 @@ def main() -> None:
         return
     pk = peaks()
     ms_step = res["ms"] / args.steps
-    value = wl.bytes_per_step() * world / (ms_step / 1e3) / 1e9
+    value = whole_job_gbs(wl.bytes_per_step(), world, ms_step)
     if wl.name in ("c1", "c4", "c5"):
         # the step runs several alternative forms of the same work: report the
         # headline form's own time (c5: the ragged graph; c4: the fastest form)
@@ -670,7 +681,7 @@ def main() -> None:
             # one transform of each size, in its fastest form
             ms_step = sum(min(means[f"{m}:{1 << lg}"] for m in wl.forms_of(lg)) for lg in wl.log_ns)
             nbytes  = sum(wl.part_bytes(f"plain:{1 << lg}") for lg in wl.log_ns)
-        value = nbytes * world / (ms_step / 1e3) / 1e9
+        value = whole_job_gbs(nbytes, world, ms_step)
     mean = {p: statistics.mean(v) for p, v in res["per"].items()}
     top = max(mean, key=mean.get)
     ach = wl.part_bytes(top) / (mean[top] / 1e3) / 1e9
