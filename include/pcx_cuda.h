@@ -126,6 +126,36 @@ int pcx_fft_exec(pcx_plan plan, void* dst, const void* src, size_t src_len, int 
 int pcx_fft_par_exec(pcx_plan plan, void* const* dst, const void* const* src, size_t count, size_t len,
                      int pack_dst, int pack_src, int direction, int normalize, void* stream);
 
+/*
+ * Element-wise expression over packed vectors on the device.  Replaces the
+ * evaluation of pcxo::vector expression templates (vector_arithm.hpp:405-1140:
+ * operator+ - * / between vectors and with complex scalars, conj, and
+ * vector::operator=(expression), vector.hpp:177-182) for data the GPU holds.
+ * `ops` is a postfix program of n_ops nodes: PCX_OP_VEC pushes element e of
+ * vecs[arg] (pack vec_packs[arg]), PCX_OP_SCALAR pushes re + i*im, the binary
+ * nodes pop two values and push the result, PCX_OP_CONJ conjugates the top.
+ * The program must leave one value (nesting depth <= 8); element e of dst
+ * (pack pack_dst) receives it, for e < n.  dst may be one of the operands when
+ * their pack widths agree.
+ */
+#define PCX_EXPR_MAX_OPS 32
+#define PCX_EXPR_MAX_VECS 8
+#define PCX_OP_VEC 0
+#define PCX_OP_SCALAR 1
+#define PCX_OP_ADD 2
+#define PCX_OP_SUB 3
+#define PCX_OP_MUL 4
+#define PCX_OP_DIV 5
+#define PCX_OP_CONJ 6
+typedef struct {
+    int    code;
+    int    arg;
+    double re;
+    double im;
+} pcx_expr_op;
+int pcx_vec_eval(int dtype, void* dst, int pack_dst, size_t n, const pcx_expr_op* ops, int n_ops,
+                 const void* const* vecs, const int* vec_packs, int n_vecs, void* stream);
+
 /* As pcx_fft_exec with caller-provided scratch (>= pcx_plan_workspace_size). */
 int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
                     int direction, int normalize, size_t batch, size_t dst_stride, size_t src_stride,

@@ -6,6 +6,7 @@
 #define PCXO_VECTOR_HPP
 
 #include "types.hpp"
+#include "vector_arithm.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -146,6 +147,13 @@ public:
             m_size = other.m_size;
             if (m_ptr) copy_reals(m_ptr, other.m_ptr, real_size(m_size));
         }
+        return *this;
+    }
+    // v = expression: element-wise on the GPU (reference vector.hpp:177-182)
+    template<typename E>
+        requires detail_::vexpr_node<E>
+    auto operator=(const E& expression) -> vector& {
+        pcxo::assign(*this, expression);
         return *this;
     }
     auto operator=(vector&& other) noexcept -> vector& {

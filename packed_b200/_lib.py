@@ -34,6 +34,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_plan_workspace_size": (_sz, [_vp, _sz]),
     "pcx_plan_tune": (_i, [_vp, _sz, _vp, ctypes.POINTER(_i)]),
     "pcx_fft_par_exec": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _sz, _sz, _i, _i, _i, _i, _vp]),
+    "pcx_vec_eval": (_i, [_i, _vp, _i, _sz, _vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i), _i, _vp]),
     "pcx_fft_exec": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),
     "pcx_fft_exec_ws": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp]),
     "pcx_fft_vjp": (_i, [_vp, _vp, _vp, _i, _i, _i, _sz, _sz, _vp]),

@@ -81,6 +81,21 @@ class vector:
         t = torch.as_tensor(host, dtype=dtype).to(device)
         return cls(n, dtype, p, device, t)
 
+    # element-wise arithmetic (lazy expressions, evaluated by assign)
+    def __add__(self, o): return _Expr("add", self, _Expr.wrap(o))
+    def __radd__(self, o): return _Expr("add", _Expr.wrap(o), self)
+    def __sub__(self, o): return _Expr("sub", self, _Expr.wrap(o))
+    def __rsub__(self, o): return _Expr("sub", _Expr.wrap(o), self)
+    def __mul__(self, o): return _Expr("mul", self, _Expr.wrap(o))
+    def __rmul__(self, o): return _Expr("mul", _Expr.wrap(o), self)
+    def __truediv__(self, o): return _Expr("div", self, _Expr.wrap(o))
+    def __rtruediv__(self, o): return _Expr("div", _Expr.wrap(o), self)
+
+    def assign(self, expr, stream=None) -> "vector":
+        """vector = expression (reference vector.hpp:177-182), on the device."""
+        evaluate(self, expr, stream)
+        return self
+
     def to_complex(self) -> np.ndarray:
         p = self.pack_size
         a = self.data.detach().cpu().numpy().astype(np.float64).reshape(-1, 2, p)
@@ -102,6 +117,77 @@ class vector:
         p = self.pack_size
         o = i + (i // p) * p
         return complex(float(self.data[o]), float(self.data[o + p]))
+
+
+# ---------------------------------------------------------------- expressions
+class _Expr:
+    """Element-wise expression over vectors (reference vector_arithm.hpp:405-1140),
+    evaluated on the device by ``vector.assign(expr)`` / ``evaluate``."""
+
+    def __init__(self, kind, *args):
+        self.kind, self.args = kind, args
+
+    @staticmethod
+    def wrap(x):
+        if isinstance(x, (_Expr, vector)):
+            return x
+        return _Expr("scalar", complex(x))
+
+    def __add__(self, o): return _Expr("add", self, _Expr.wrap(o))
+    def __radd__(self, o): return _Expr("add", _Expr.wrap(o), self)
+    def __sub__(self, o): return _Expr("sub", self, _Expr.wrap(o))
+    def __rsub__(self, o): return _Expr("sub", _Expr.wrap(o), self)
+    def __mul__(self, o): return _Expr("mul", self, _Expr.wrap(o))
+    def __rmul__(self, o): return _Expr("mul", _Expr.wrap(o), self)
+    def __truediv__(self, o): return _Expr("div", self, _Expr.wrap(o))
+    def __rtruediv__(self, o): return _Expr("div", _Expr.wrap(o), self)
+
+
+_OPS = {"vec": 0, "scalar": 1, "add": 2, "sub": 3, "mul": 4, "div": 5, "conj": 6}
+
+
+class _ExprOp(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int), ("arg", ctypes.c_int), ("re", ctypes.c_double), ("im", ctypes.c_double)]
+
+
+def conj(x):
+    """Complex conjugate of a vector or expression (lazy)."""
+    return _Expr("conj", _Expr.wrap(x))
+
+
+def evaluate(dest: "vector", expr, stream=None) -> None:
+    """dest = expr, element-wise on the device (pcx_vec_eval)."""
+    ops, vecs = [], []
+
+    def emit(x):
+        if isinstance(x, vector):
+            if x.size() != dest.size():
+                raise ValueError(f"source size (which is {x.size()} is not equal to subrange size (which is "
+                                 f"{dest.size()})")
+            if x.dtype != dest.dtype:
+                raise TypeError("data type does not match")
+            k = next((i for i, v in enumerate(vecs) if v is x), None)
+            if k is None:
+                vecs.append(x)
+                k = len(vecs) - 1
+            ops.append(_ExprOp(0, k, 0.0, 0.0))
+        elif x.kind == "scalar":
+            ops.append(_ExprOp(1, 0, x.args[0].real, x.args[0].imag))
+        elif x.kind == "conj":
+            emit(x.args[0])
+            ops.append(_ExprOp(6, 0, 0.0, 0.0))
+        else:
+            emit(x.args[0])
+            emit(x.args[1])
+            ops.append(_ExprOp(_OPS[x.kind], 0, 0.0, 0.0))
+
+    emit(_Expr.wrap(expr))
+    arr = (_ExprOp * len(ops))(*ops)
+    ptrs = (ctypes.c_void_p * max(1, len(vecs)))(*[v.data.data_ptr() for v in vecs])
+    packs = (ctypes.c_int * max(1, len(vecs)))(*[v.pack_size for v in vecs])
+    _lib.check(_lib.lib().pcx_vec_eval(_dtype_code(dest.dtype), _ptr(dest.data), dest.pack_size, dest.size(),
+                                       ctypes.cast(arr, ctypes.c_void_p), len(ops), ptrs, packs, len(vecs),
+                                       _stream_ptr(stream)))
 
 
 def _ptr(t: torch.Tensor) -> ctypes.c_void_p:

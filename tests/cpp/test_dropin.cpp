@@ -181,6 +181,38 @@ int main() {
             expect(worst < 2e-6, what, worst);
         }
     }
+    {    // vector expressions on the device (vector_arithm.hpp; tests/test_op.cpp:116-131 table)
+        const std::size_t   n = 1000;
+        pcxo::vector<float> a(n), b(n), c(n), out(n);
+        std::vector<cd>     za(n), zb(n), zc(n);
+        for (std::size_t i = 0; i < n; ++i) {
+            za[i] = cd(u(rng), u(rng));
+            zb[i] = cd(2 + u(rng), u(rng));
+            zc[i] = cd(u(rng), u(rng));
+            a[i]  = std::complex<float>(za[i]);
+            b[i]  = std::complex<float>(zb[i]);
+            c[i]  = std::complex<float>(zc[i]);
+        }
+        const std::complex<float> s(0.5f, -1.5f);
+        const cd                  sd(0.5, -1.5);
+        auto check = [&](const char* what, auto&& make_want) {
+            std::vector<cd> want(n);
+            for (std::size_t i = 0; i < n; ++i) want[i] = make_want(i);
+            expect(rel_err(out, want) < 2e-6, what, rel_err(out, want));
+        };
+        out = a + b;
+        check("expr a + b", [&](std::size_t i) { return za[i] + zb[i]; });
+        out = a * pcxo::conj(b);
+        check("expr a * conj(b)", [&](std::size_t i) { return za[i] * std::conj(zb[i]); });
+        out = pcxo::conj(a) / b - c;
+        check("expr conj(a) / b - c", [&](std::size_t i) { return std::conj(za[i]) / zb[i] - zc[i]; });
+        out = s * a + 2.f / c;
+        check("expr s * a + 2 / c", [&](std::size_t i) { return sd * za[i] + 2.0 / zc[i]; });
+        a = a * a;
+        std::vector<cd> sq(n);
+        for (std::size_t i = 0; i < n; ++i) sq[i] = za[i] * za[i];
+        expect(rel_err(a, sq) < 2e-6, "expr a = a * a (in place)", rel_err(a, sq));
+    }
     {    // exceptions keep the reference's types and messages
         bool thrown = false;
         try {

@@ -337,3 +337,37 @@ def test_fft_unit_par_errors():
     unit = fft_unit_par(16)
     with pytest.raises(ValueError, match="is not equal to fft size"):
         unit([vector(4) for _ in range(15)], [vector(4) for _ in range(16)])
+
+
+@pytest.mark.parametrize("dtype", [F32, F64])
+def test_vector_expressions_on_device(dtype):
+    """pcxo::vector expression templates (reference vector_arithm.hpp:405-1140,
+    the binary-operator table of tests/test_op.cpp:116-131): +, -, *, / between
+    vectors and scalars and conj, evaluated on the device (pcx_vec_eval), mixed
+    pack widths, against numpy."""
+    from packed_b200 import conj
+    npd = np.float64 if dtype == F64 else np.float32
+    rng = np.random.default_rng(600)
+    n = 1000
+    za, zb, zc = (normal_cx(rng, n) for _ in range(3))
+    zb += 2.0    # keep divisors away from zero
+    a = vector.from_complex(za, dtype=dtype, pack=8 if dtype == F32 else 4)
+    b = vector.from_complex(zb, dtype=dtype, pack=1)
+    c = vector.from_complex(zc, dtype=dtype, pack=2)
+    s = 0.5 - 1.5j
+    cases = [
+        (lambda: a + b, za + zb), (lambda: a - b, za - zb), (lambda: a * b, za * zb), (lambda: a / b, za / zb),
+        (lambda: a + conj(b), za + np.conj(zb)), (lambda: conj(a) * b, np.conj(za) * zb),
+        (lambda: conj(a) / conj(b), np.conj(za) / np.conj(zb)), (lambda: a * s + c, za * s + zc),
+        (lambda: s / b - conj(c * a), s / zb - np.conj(zc * za)), (lambda: (a + b) * (a - c) / (b * b), (za + zb) * (za - zc) / (zb * zb)),
+    ]
+    out = vector(n, dtype=dtype, pack=4)
+    for expr, want in cases:
+        out.assign(expr())
+        torch.cuda.synchronize()
+        assert rel_l2(out.to_complex(), want) < TOL[npd]
+    a.assign(a * a)    # destination among the operands, same pack
+    torch.cuda.synchronize()
+    assert rel_l2(a.to_complex(), za * za) < TOL[npd]
+    with pytest.raises(ValueError, match="not equal to subrange size"):
+        out.assign(a + vector(n + 1, dtype=dtype))
