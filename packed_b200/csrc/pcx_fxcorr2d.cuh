@@ -278,8 +278,15 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
         }
         {
             const int       g    = tid / TT1, t = tid % TT1;
-            const long long e0   = b0 + a.in_shift - a.out_shift;    // output position of window index 0
-            float*          d    = dst + ch * a.dst_stride;
+            // window index n is output position e0 + n; it is written when
+            // out_shift <= n < out_shift + step and e0 + n < len.  e0 and every
+            // row start are whole packs, so the packed offset of e0 + row*N2 + n2
+            // is 2*(e0 + row*N2) + pk(n2).
+            const long long e0 = b0 + a.in_shift - a.out_shift;
+            const int       lo = a.out_shift;
+            const long long hl = min((long long)a.out_shift + a.step, a.len - e0);
+            const int       hi = (int)max(0LL, min(hl, (long long)N1 * N2));
+            float*          d  = dst + ch * a.dst_stride + 2 * e0;
             for (int rd = 0; rd < F::R1; ++rd) {
                 const int  n2 = rd * F::G1 + g;
                 cpx<float> v[E];
@@ -295,15 +302,13 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 }
                 stage_compute_tab<P1, 0>(v, t, tw1);
                 run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                float* drow = d + 2 * t * N2 + ((n2 >> 3) << 4) + (n2 & 7);
                 static_for<E>([&](auto ic) {
-                    constexpr int i  = decltype(ic)::value;
-                    const int     n  = (t + i * TT1) * N2 + n2;    // window index
-                    const int     mo = n - a.out_shift;
-                    if (mo >= 0 && mo < a.step && e0 + n < a.len) {
-                        const long long e = e0 + n;
-                        const long long o = ((e >> 3) << 4) + (e & 7);
-                        __stcs(d + o, v[i].re);
-                        __stcs(d + o + 8, -v[i].im);
+                    constexpr int i = decltype(ic)::value;
+                    const int     n = (t + i * TT1) * N2 + n2;    // window index
+                    if (n >= lo && n < hi) {
+                        __stcs(drow + 2 * i * TT1 * N2, v[i].re);
+                        __stcs(drow + 2 * i * TT1 * N2 + 8, -v[i].im);
                     }
                 });
             }
