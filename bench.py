@@ -213,9 +213,18 @@ class C2Sweep:
                 "d2h_bytes_per_step": nb, "ms_per_step": ms}
 
     def launches(self):
-        # one kernel per transform direction: a one-pass kernel for N <= 8192,
-        # the one-launch four-step above
-        return 2 * len(self.log_ns)
+        # per direction: one kernel (one pass, or the one-launch four-step), or
+        # two per scratch chunk when the autotuner chose the chunked four-step
+        total = 0
+        for lg, u in self.units.items():
+            f = u.form()
+            if lg > 12 and f["form"] == "chunked four-step":
+                rows = self.points >> lg
+                per = max(1, f["chunk_bytes"] // ((1 << lg) * 8))
+                total += 2 * 2 * ((rows + per - 1) // per)
+            else:
+                total += 2
+        return total
 
     def cpu_reference(self, budget_s=12.0):
         import ctypes

@@ -93,6 +93,9 @@ size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
  * A plan for n <= 4096 has one form: PCX_FORM_DEFAULT, nothing is timed.
  */
 int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* form_out);
+/* The plan's current form (PCX_FORM_*), the one-launch four-step's dependency
+ * distance in rounds of tiles, and the chunked form's scratch bytes per buffer. */
+int pcx_plan_form(pcx_plan plan, int* form, int* rounds, size_t* chunk_bytes);
 
 /*
  * Batched transform of `batch` rows.  Replaces

@@ -33,6 +33,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_plan_status": (_i, [_vp]),
     "pcx_plan_workspace_size": (_sz, [_vp, _sz]),
     "pcx_plan_tune": (_i, [_vp, _sz, _vp, ctypes.POINTER(_i)]),
+    "pcx_plan_form": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_sz)]),
     "pcx_fft_par_exec": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _sz, _sz, _i, _i, _i, _i, _vp]),
     "pcx_vec_eval": (_i, [_i, _vp, _i, _sz, _vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i), _i, _vp]),
     "pcx_fft_exec": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),

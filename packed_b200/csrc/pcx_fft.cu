@@ -448,6 +448,16 @@ extern "C" int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* for
     });
 }
 
+extern "C" int pcx_plan_form(pcx_plan plan, int* form, int* rounds, size_t* chunk_bytes) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        if (form) *form = plan->form;
+        if (rounds) *rounds = plan->fs_rounds;
+        if (chunk_bytes) *chunk_bytes = plan->chunk_bytes ? plan->chunk_bytes : ((size_t)24 << 20);
+        return PCX_OK;
+    });
+}
+
 extern "C" size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch) {
     if (!plan || !plan->two_pass) return 0;
     return 2 * plan->chunk_rows(batch) * plan->n * plan->elem_bytes();

@@ -245,6 +245,12 @@ class fft_unit:
 
     FORMS = {0: "default", 1: "one-pass", 2: "one-launch four-step", 3: "chunked four-step"}
 
+    def form(self) -> dict:
+        """The plan's form (pcx_plan_form): name, tile distance in rounds, chunk scratch bytes."""
+        f, r, c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_size_t(0)
+        _lib.check(_lib.lib().pcx_plan_form(self._plan, ctypes.byref(f), ctypes.byref(r), ctypes.byref(c)))
+        return {"form": self.FORMS.get(f.value, str(f.value)), "rounds": r.value, "chunk_bytes": c.value}
+
     def tune(self, batch: int = 1, stream=None) -> str:
         """Time this size's forms on `batch` rows and keep the fastest (pcx_plan_tune)."""
         form = ctypes.c_int(0)
