@@ -207,14 +207,27 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         *reinterpret_cast<E*>(opB_lo + op_off<PREC, 32>(n, k)) = lo;
     }
     // rows in natural order (conjugated for the inverse); missing rows are zero
-    for (int q = tid; q < T * N; q += NT) {
-        const int r = q / N, e = q % N;
-        cpx<float> v = {0.f, 0.f};
+    // (one 64-byte pack of 8 samples per thread and step, 16-byte loads)
+    for (int q = tid; q < T * N / 8; q += NT) {
+        const int r = q / (N / 8), pk8 = q % (N / 8);
+        float4    r0 = {0.f, 0.f, 0.f, 0.f}, r1 = r0, i0 = r0, i1 = r0;
         if (r < rows) {
-            const float* s = a.src + (row0 + r) * (2 * N) + ((e >> 3) << 4) + (e & 7);
-            v              = {s[0], a.conj ? -s[8] : s[8]};
+            const float4* s = reinterpret_cast<const float4*>(a.src + (row0 + r) * (2 * N) + pk8 * 16);
+            r0              = __ldg(s);
+            r1              = __ldg(s + 1);
+            i0              = __ldg(s + 2);
+            i1              = __ldg(s + 3);
         }
-        work0[q] = v;
+        const float      cj = a.conj ? -1.f : 1.f;
+        cpx<float>*      w  = work0 + r * N + pk8 * 8;
+        w[0] = {r0.x, cj * i0.x};
+        w[1] = {r0.y, cj * i0.y};
+        w[2] = {r0.z, cj * i0.z};
+        w[3] = {r0.w, cj * i0.w};
+        w[4] = {r1.x, cj * i1.x};
+        w[5] = {r1.y, cj * i1.y};
+        w[6] = {r1.z, cj * i1.z};
+        w[7] = {r1.w, cj * i1.w};
     }
     __syncthreads();
     tc_fence_after();
@@ -247,29 +260,49 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         __syncthreads();
     }
 
-    uint32_t phase = 0;
+    uint32_t phase    = 0;
+    int      tw_shift = LOGN - 4 - __ffs(ns) + 1;    // log2(N / (16 ns))
     for (int st = 0; st < C::NTC; ++st) {
         for (int mb = 0; mb < NB; mb += 128) {
             const int  b  = mb + tid;
             const int  tr = b / (N / 16), bl = b % (N / 16);
-            const int  k  = bl % ns;
+            const int  k  = bl & (ns - 1);
             cpx<float> x[16];
+            // twiddle j of the butterfly is W_{16 ns}^(jk): one or two of the six
+            // factors W^(qk), q = 1,2,3,4,8,12, read from the W_N table
+            cpx<float> f[6];
+            if (ns > 1) {
+                const int sh = tw_shift;    // W_{16 ns}^e = W_N^(e * N / (16 ns))
+                f[0]         = ldg_cpx(twN + ((k) << sh));
+                f[1]         = ldg_cpx(twN + ((2 * k) << sh));
+                f[2]         = ldg_cpx(twN + ((3 * k) << sh));
+                f[3]         = ldg_cpx(twN + ((4 * k) << sh));
+                f[4]         = ldg_cpx(twN + ((8 * k) << sh));
+                f[5]         = ldg_cpx(twN + ((12 * k) << sh));
+            }
             static_for<16>([&](auto jc) {
                 constexpr int j = decltype(jc)::value;
                 cpx<float>    v = in[tr * N + bl + j * (N / 16)];
-                if (j > 0 && ns > 1) v = cmul(v, ldg_cpx(twN + ((j * k) * (N / (16 * ns)))));
+                if constexpr (j > 0) {
+                    if (ns > 1) v = cmul(v, stw_factor<4, j>(f));
+                }
                 x[j] = v;
             });
-            // operand rows: reals 0..15 then imaginaries 16..31
-            static_for<16>([&](auto jc) {
-                constexpr int j = decltype(jc)::value;
-                E             h, l;
-                O::split(x[j].re, h, l);
-                *reinterpret_cast<E*>(opA_hi + op_off<PREC, 128>(tid, j))      = h;
-                *reinterpret_cast<E*>(opA_lo + op_off<PREC, 128>(tid, j))      = l;
-                O::split(x[j].im, h, l);
-                *reinterpret_cast<E*>(opA_hi + op_off<PREC, 128>(tid, j + 16)) = h;
-                *reinterpret_cast<E*>(opA_lo + op_off<PREC, 128>(tid, j + 16)) = l;
+            // operand rows (reals 0..15 then imaginaries 16..31), one 16-byte
+            // core-matrix row per store
+            static_for<32 / O::PER_CHUNK>([&](auto cc) {
+                constexpr int c = decltype(cc)::value;
+                E             h[O::PER_CHUNK], l[O::PER_CHUNK];
+                static_for<O::PER_CHUNK>([&](auto qc) {
+                    constexpr int kk = c * O::PER_CHUNK + decltype(qc)::value;
+                    const float   xv = kk < 16 ? x[kk & 15].re : x[kk & 15].im;
+                    O::split(xv, h[decltype(qc)::value], l[decltype(qc)::value]);
+                });
+                uint4 hv, lv;
+                memcpy(&hv, h, 16);
+                memcpy(&lv, l, 16);
+                *reinterpret_cast<uint4*>(opA_hi + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = hv;
+                *reinterpret_cast<uint4*>(opA_lo + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = lv;
             });
             fence_proxy_async_smem();
             tc_fence_before();
@@ -316,6 +349,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         }
         if (aborted) break;
         ns *= 16;
+        tw_shift -= 4;
         cpx<float>* t = in;
         in            = out;
         out           = t;
@@ -323,11 +357,14 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     }
     if (!aborted) {
         const float sc = a.scale, sim = a.conj ? -a.scale : a.scale;
-        for (int q = tid; q < rows * N; q += NT) {
-            const int r = q / N, e = q % N;
-            float*    d = a.dst + (row0 + r) * (2 * N) + ((e >> 3) << 4) + (e & 7);
-            d[0]        = in[q].re * sc;
-            d[8]        = in[q].im * sim;
+        for (int q = tid; q < rows * N / 8; q += NT) {
+            const int         r = q / (N / 8), pk8 = q % (N / 8);
+            const cpx<float>* w = in + r * N + pk8 * 8;
+            float4*           d = reinterpret_cast<float4*>(a.dst + (row0 + r) * (2 * N) + pk8 * 16);
+            d[0] = make_float4(w[0].re * sc, w[1].re * sc, w[2].re * sc, w[3].re * sc);
+            d[1] = make_float4(w[4].re * sc, w[5].re * sc, w[6].re * sc, w[7].re * sc);
+            d[2] = make_float4(w[0].im * sim, w[1].im * sim, w[2].im * sim, w[3].im * sim);
+            d[3] = make_float4(w[4].im * sim, w[5].im * sim, w[6].im * sim, w[7].im * sim);
         }
     }
     tc_fence_before();
@@ -377,6 +414,9 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
             return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form built for 2^8 <= N <= 2^12");
         }
         if (precision != 0 && precision != 1) return pcx_fail(PCX_ERR_INVALID, "precision: 0 bf16x3, 1 tf32x3");
+        if ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) % 16 != 0) {
+            return pcx_fail(PCX_ERR_INVALID, "data pointers must be 16-byte aligned");
+        }
         // full W_N table (the plan's single-pass table)
         tc::tc_args a{};
         a.src   = static_cast<const float*>(src);
