@@ -106,44 +106,53 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- workloads
-def pipelined_e2e(torch, host_in, host_out, chunks, slot_reals, compute):
+def pipelined_e2e(torch, host_in, host_out, chunks, slot_reals, compute, reps=1, warmup=1):
     """Host -> device -> host through the library, chunk by chunk, with the
     copy of chunk c+1 in, the transform of chunk c and the copy of chunk c-1
     out in flight together on three streams (two device slots).
     chunks: (host offset in reals, reals, key); compute(slot_tensor, reals, key,
-    stream) runs the library calls in place on the slot.  Returns ms."""
+    stream) runs the library calls in place on the slot.  The slots and
+    streams are set up once, `warmup` untimed passes over the chunks run
+    first, then `reps` passes back to back are timed.  Returns ms per pass."""
     dev = torch.cuda.current_device()
     slots = [torch.empty(slot_reals, dtype=host_in.dtype, device=dev) for _ in range(2)]
     s_in, s_cmp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
     main = torch.cuda.current_stream()
     freed = [torch.cuda.Event(), torch.cuda.Event()]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(passes):
+        for st in (s_in, s_cmp, s_out):
+            st.wait_stream(main)
+        work = [c for _ in range(passes) for c in chunks]
+        for c, (off, n, key) in enumerate(work):
+            k = c % 2
+            buf = slots[k][:n]
+            if c >= 2:
+                s_in.wait_event(freed[k])
+            with torch.cuda.stream(s_in):
+                buf.copy_(host_in[off:off + n], non_blocking=True)
+                landed = torch.cuda.Event()
+                landed.record(s_in)
+            s_cmp.wait_event(landed)
+            with torch.cuda.stream(s_cmp):
+                compute(buf, n, key, s_cmp)
+                done = torch.cuda.Event()
+                done.record(s_cmp)
+            s_out.wait_event(done)
+            with torch.cuda.stream(s_out):
+                host_out[off:off + n].copy_(buf, non_blocking=True)
+                freed[k].record(s_out)
+        main.wait_stream(s_out)
+
+    if warmup:
+        run(warmup)
     torch.cuda.synchronize()
     e0.record(main)
-    for st in (s_in, s_cmp, s_out):
-        st.wait_stream(main)
-    for c, (off, n, key) in enumerate(chunks):
-        k = c % 2
-        buf = slots[k][:n]
-        if c >= 2:
-            s_in.wait_event(freed[k])
-        with torch.cuda.stream(s_in):
-            buf.copy_(host_in[off:off + n], non_blocking=True)
-            landed = torch.cuda.Event()
-            landed.record(s_in)
-        s_cmp.wait_event(landed)
-        with torch.cuda.stream(s_cmp):
-            compute(buf, n, key, s_cmp)
-            done = torch.cuda.Event()
-            done.record(s_cmp)
-        s_out.wait_event(done)
-        with torch.cuda.stream(s_out):
-            host_out[off:off + n].copy_(buf, non_blocking=True)
-            freed[k].record(s_out)
-    main.wait_stream(s_out)
+    run(reps)
     e1.record(main)
     torch.cuda.synchronize()
-    return e0.elapsed_time(e1)
+    return e0.elapsed_time(e1) / reps
 
 
 class C2Sweep:
@@ -186,6 +195,7 @@ class C2Sweep:
         return self.points * B_PT * 2
 
     e2e_chunks = 8
+    e2e_reps = 1
 
     def e2e(self, torch, stream):
         host_in = torch.empty(2 * self.points, dtype=torch.float32).pin_memory()
@@ -207,7 +217,7 @@ class C2Sweep:
             u.exec(scratch[:n], buf, batch=rows, direction=0, stream=st)
             u.exec(buf, scratch[:n], batch=rows, direction=1, stream=st)
 
-        ms = pipelined_e2e(torch, host_in, host_out, chunks, scratch.numel(), compute)
+        ms = pipelined_e2e(torch, host_in, host_out, chunks, scratch.numel(), compute, reps=self.e2e_reps)
         nb = 2 * self.points * 4 * len(self.log_ns)
         return {"value": self.bytes_per_step() / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nb,
                 "d2h_bytes_per_step": nb, "ms_per_step": ms}
@@ -262,6 +272,7 @@ class C1(C2Sweep):
     log_ns = [10]
     points = 1024 * 64
     e2e_chunks = 1    # 0.5 MB: one copy in, one transform pair, one copy out
+    e2e_reps = 200    # steps timed back to back, each one's copies and transforms overlapping its neighbours
 
     def config(self, world):
         return {"workload": "C1: N=1024, batch 64, forward then inverse (1/N), pack 8, U[-1,1) seed 0; step = "
@@ -390,13 +401,13 @@ class C4TensorCore:
     """Tensor-core split-precision FFT against the plain FP32 path, batch 4096."""
     name = "c4"
     log_ns = [8, 10, 12, 14, 16]
-    tc_max = 12    # the tensor-core form covers N <= 4096
+    tc_max = 16    # the tensor-core form: one pass up to 4096, two passes for 16384 and 65536
     batch = 4096
 
     def config(self, world):
         return {"workload": "C4: N in {256, 1024, 4096, 16384, 65536}, batch 4096, complex64 N(0,1) + 1e-3 tone at "
-                            "a seeded bin (seed 4); tensor-core split-bf16 and split-tf32 forward (N <= 4096) vs "
-                            "plain FP32 forward",
+                            "a seeded bin (seed 4); tensor-core split-bf16 and split-tf32 forward vs plain FP32 "
+                            "forward",
                 "global_batch_points": sum(self.batch << lg for lg in self.log_ns) * world,
                 "l2": "inputs 8-128 MiB per size; timed steps back to back",
                 "parallelism": f"independent shards x{world}"}
@@ -410,7 +421,7 @@ class C4TensorCore:
             n = 1 << lg
             # the first 16 rows (the accuracy sample) come from numpy; the rest,
             # same distribution, from the device generator
-            rows = 16 if lg > self.tc_max else self.batch
+            rows = 16 if lg > 12 else self.batch
             z = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
             k = rng.integers(0, n, rows)
             z += 1e-3 * np.exp(2j * np.pi * k[:, None] * np.arange(n)[None, :] / n)
@@ -477,7 +488,21 @@ class C4TensorCore:
         return None
 
     def launches(self):
-        return len(self.parts())
+        total = 0
+        for key in self.parts():
+            m, lg = self._split(key)
+            chunk = max(1, min(self.batch, (int(os.environ.get("PCX_SCRATCH_MB", "24")) << 20) // ((1 << lg) * 8)))
+            chunks = (self.batch + chunk - 1) // chunk
+            if m != "plain":
+                total += 1 if lg <= 12 else 2 * chunks    # two-pass form: two launches per chunk
+                continue
+            f = self.units[lg].form() if lg > 12 else {"form": "default"}
+            if f["form"] == "chunked four-step":
+                chunk = max(1, f["chunk_bytes"] // ((1 << lg) * 8))
+                total += 2 * ((self.batch + chunk - 1) // chunk)
+            else:
+                total += 1
+        return total
 
     def cpu_reference(self, budget_s=12.0):
         c2 = C2Sweep()

@@ -242,8 +242,13 @@ int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, const void*
  * precision 0: bfloat16 hi + lo, three products (kind::f16);
  * precision 1: tf32 hi + lo, three products (kind::tf32).
  * `batch` contiguous rows of a complex64 plan in natural order, pack 8,
- * 2^8 <= n <= 2^12.  Errors against an FP64 oracle are reported per size by
- * the test suite and the benchmark.
+ * 2^8 <= n <= 2^16.  Up to 2^12 one launch transforms whole rows; 2^13..2^16
+ * run as two passes of 2^6..2^8-point tensor-core transforms (columns, with
+ * the four-step twiddle, into the plan's scratch, then rows out in natural
+ * order), one L2-sized chunk of rows at a time; like pcx_fft_exec with the
+ * plan's scratch, such calls on one plan must not overlap on the GPU.
+ * Errors against an FP64 oracle are reported per size by the test suite and
+ * the benchmark.
  */
 int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int direction, int normalize, size_t batch,
                     int precision, void* stream);

@@ -133,13 +133,28 @@ __device__ __forceinline__ uint32_t op_off(int row, int k) {
 struct tc_args {
     const float* src;
     float*       dst;
-    long long    batch;
+    long long    batch;    // rows (mode 0 and 2) or transforms (mode 1)
     int          conj;
     float        scale;
     const void*  twN;    // W_N^i
     int*         error;
+    // two-pass forms of a transform of N * 2^lg_other points
+    int          lg_other;    // mode 1: log2 of the row length; mode 2: log2 of the rows per transform
+    const void*  tw_hi;       // W_M^(i * 2^lg_other), M = N * 2^lg_other (mode 1)
+    const void*  tw_lo;       // W_M^i, i < 2^lg_other (mode 1)
 };
 
+// Modes of one launch:
+//   0: `batch` contiguous rows of N points, natural order in and out;
+//   1: column pass of a two-pass transform of M = N * C points laid out as
+//      N rows of C (C = 2^lg_other): each CTA transforms T adjacent columns
+//      of one transform, multiplies output k of column c by W_M^(c k) and
+//      writes it back to the same place (the input conjugated for the inverse);
+//   2: row pass: each CTA transforms T rows of N points of the column pass's
+//      output (R = 2^lg_other rows per transform) and writes output k of row
+//      j to element k * R + j, the transform's natural order (the output
+//      conjugated and scaled for the inverse).
+// Modes 1 and 2 read and write whole 8-point packs of T >= 8 adjacent columns.
 // Smem plan: work[2][T*N] complex | A_hi | A_lo (128 x 32) | B_hi | B_lo (32 x 32)
 template<int LOGN, int PREC>
 struct tc_cfg {
@@ -153,8 +168,9 @@ struct tc_cfg {
     static constexpr int SMEM  = 2 * T * N * 8 + 2 * ABYTE + 2 * BBYTE;
 };
 
-template<int LOGN, int PREC>
+template<int LOGN, int PREC, int MODE>
 __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
+    static_assert(MODE == 0 || tc_cfg<LOGN, PREC>::T % 8 == 0, "two-pass modes move whole packs of columns");
     using C  = tc_cfg<LOGN, PREC>;
     using O  = op_traits<PREC>;
     using E  = typename O::elem;
@@ -175,7 +191,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     const int  warp = tid / 32;
     const auto* twN = reinterpret_cast<const cpx<float>*>(a.twN);
     const long long row0 = (long long)blockIdx.x * T;
-    const int       rows = (int)min((long long)T, a.batch - row0);
+    const int       rows = MODE == 1 ? T : (int)min((long long)T, a.batch - row0);
 
     if (warp == 0) {
         tmem_alloc(&tslot, 32);
@@ -206,6 +222,32 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         *reinterpret_cast<E*>(opB_hi + op_off<PREC, 32>(n, k)) = hi;
         *reinterpret_cast<E*>(opB_lo + op_off<PREC, 32>(n, k)) = lo;
     }
+    const bool conj_in  = MODE != 2 && a.conj;
+    const bool conj_out = MODE != 1 && a.conj;
+    if constexpr (MODE == 1) {
+        // T adjacent columns c0.. of one transform, one pack of 8 columns of
+        // one row per thread and step (four 16-byte loads)
+        const long long cols = 1LL << a.lg_other;
+        const long long gpt  = cols / T;
+        const long long tr   = (long long)blockIdx.x / gpt;
+        const long long c0   = ((long long)blockIdx.x % gpt) * T;
+        const float*    base = a.src + tr * (2 * N * cols);
+        const float     cj   = conj_in ? -1.f : 1.f;
+        for (int q = tid; q < T * N / 8; q += NT) {
+            const int     i  = q % N, jg = q / N;
+            const float4* s  = reinterpret_cast<const float4*>(base + 2 * (i * cols + c0 + 8 * jg));
+            const float4  r0 = __ldg(s), r1 = __ldg(s + 1), i0 = __ldg(s + 2), i1 = __ldg(s + 3);
+            cpx<float>*   w  = work0 + (8 * jg) * N + i;
+            w[0 * N]         = {r0.x, cj * i0.x};
+            w[1 * N]         = {r0.y, cj * i0.y};
+            w[2 * N]         = {r0.z, cj * i0.z};
+            w[3 * N]         = {r0.w, cj * i0.w};
+            w[4 * N]         = {r1.x, cj * i1.x};
+            w[5 * N]         = {r1.y, cj * i1.y};
+            w[6 * N]         = {r1.z, cj * i1.z};
+            w[7 * N]         = {r1.w, cj * i1.w};
+        }
+    } else
     // rows in natural order (conjugated for the inverse); missing rows are zero
     // (one 64-byte pack of 8 samples per thread and step, 16-byte loads)
     for (int q = tid; q < T * N / 8; q += NT) {
@@ -218,7 +260,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             i0              = __ldg(s + 2);
             i1              = __ldg(s + 3);
         }
-        const float      cj = a.conj ? -1.f : 1.f;
+        const float      cj = conj_in ? -1.f : 1.f;
         cpx<float>*      w  = work0 + r * N + pk8 * 8;
         w[0] = {r0.x, cj * i0.x};
         w[1] = {r0.y, cj * i0.y};
@@ -355,8 +397,50 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         out           = t;
         __syncthreads();
     }
-    if (!aborted) {
-        const float sc = a.scale, sim = a.conj ? -a.scale : a.scale;
+    if (!aborted && MODE == 1) {
+        const int         lgo  = a.lg_other;
+        const long long   cols = 1LL << lgo;
+        const long long   gpt  = cols / T;
+        const long long   tr   = (long long)blockIdx.x / gpt;
+        const int         c0   = (int)(((long long)blockIdx.x % gpt) * T);
+        const cpx<float>* th   = reinterpret_cast<const cpx<float>*>(a.tw_hi);
+        const cpx<float>* tl   = reinterpret_cast<const cpx<float>*>(a.tw_lo);
+        float*            base = a.dst + tr * (2 * N * cols);
+        for (int q = tid; q < T * N / 8; q += NT) {
+            const int k = q % N, jg = q / N;
+            float     re[8], im[8];
+            static_for<8>([&](auto ec) {
+                constexpr int  e  = decltype(ec)::value;
+                const uint32_t ex = (uint32_t)(c0 + 8 * jg + e) * (uint32_t)k;    // < M
+                const cpx<float> t =
+                    cmul(ldg_cpx(th + (ex >> lgo)), ldg_cpx(tl + (ex & (uint32_t)(cols - 1))));
+                const cpx<float> o = cmul(in[(8 * jg + e) * N + k], t);
+                re[e]              = o.re;
+                im[e]              = o.im;
+            });
+            float4* d = reinterpret_cast<float4*>(base + 2 * (k * cols + c0 + 8 * jg));
+            d[0]      = make_float4(re[0], re[1], re[2], re[3]);
+            d[1]      = make_float4(re[4], re[5], re[6], re[7]);
+            d[2]      = make_float4(im[0], im[1], im[2], im[3]);
+            d[3]      = make_float4(im[4], im[5], im[6], im[7]);
+        }
+    } else if (!aborted && MODE == 2) {
+        const float     sc   = a.scale, sim = conj_out ? -a.scale : a.scale;
+        const long long R    = 1LL << a.lg_other;    // rows per transform; T divides R
+        const long long tr   = row0 / R;
+        const long long j0   = row0 % R;
+        float*          base = a.dst + tr * (2 * N * R);
+        for (int q = tid; q < T * N / 8; q += NT) {
+            const int         k = q % N, jg = q / N;
+            const cpx<float>* w = in + (8 * jg) * N + k;
+            float4*           d = reinterpret_cast<float4*>(base + 2 * (k * R + j0 + 8 * jg));
+            d[0] = make_float4(w[0 * N].re * sc, w[1 * N].re * sc, w[2 * N].re * sc, w[3 * N].re * sc);
+            d[1] = make_float4(w[4 * N].re * sc, w[5 * N].re * sc, w[6 * N].re * sc, w[7 * N].re * sc);
+            d[2] = make_float4(w[0 * N].im * sim, w[1 * N].im * sim, w[2 * N].im * sim, w[3 * N].im * sim);
+            d[3] = make_float4(w[4 * N].im * sim, w[5 * N].im * sim, w[6 * N].im * sim, w[7 * N].im * sim);
+        }
+    } else if (!aborted) {
+        const float sc = a.scale, sim = conj_out ? -a.scale : a.scale;
         for (int q = tid; q < rows * N / 8; q += NT) {
             const int         r = q / (N / 8), pk8 = q % (N / 8);
             const cpx<float>* w = in + r * N + pk8 * 8;
@@ -378,13 +462,14 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
 using namespace pcxg;
 
 namespace {
-template<int LOGN, int PREC>
+template<int LOGN, int PREC, int MODE>
 cudaError_t launch_tc(const tc::tc_args& a, cudaStream_t st) {
     using C   = tc::tc_cfg<LOGN, PREC>;
-    auto kern = tc::k_tcfft<LOGN, PREC>;
+    auto kern = tc::k_tcfft<LOGN, PREC, MODE>;
     cudaError_t e = smem_attr_cached(reinterpret_cast<const void*>(kern), C::SMEM);
     if (e != cudaSuccess) return e;
-    const long long grid = (a.batch + C::T - 1) / C::T;
+    // mode 1: one CTA per T columns of a transform; otherwise per T rows
+    const long long grid = MODE == 1 ? a.batch * ((1LL << a.lg_other) / C::T) : (a.batch + C::T - 1) / C::T;
     if (grid == 0) return cudaSuccess;
     kern<<<(unsigned)grid, tc::NT, C::SMEM, st>>>(a);
     return cudaGetLastError();
@@ -392,11 +477,21 @@ cudaError_t launch_tc(const tc::tc_args& a, cudaStream_t st) {
 template<int PREC>
 cudaError_t dispatch_tc(int log_n, const tc::tc_args& a, cudaStream_t st) {
     switch (log_n) {
-    case 8: return launch_tc<8, PREC>(a, st);
-    case 9: return launch_tc<9, PREC>(a, st);
-    case 10: return launch_tc<10, PREC>(a, st);
-    case 11: return launch_tc<11, PREC>(a, st);
-    case 12: return launch_tc<12, PREC>(a, st);
+    case 8: return launch_tc<8, PREC, 0>(a, st);
+    case 9: return launch_tc<9, PREC, 0>(a, st);
+    case 10: return launch_tc<10, PREC, 0>(a, st);
+    case 11: return launch_tc<11, PREC, 0>(a, st);
+    case 12: return launch_tc<12, PREC, 0>(a, st);
+    default: return cudaErrorNotSupported;
+    }
+}
+// passes of the two-pass form: sub-transforms of 2^6..2^8 points
+template<int PREC, int MODE>
+cudaError_t dispatch_tc_pass(int log_n, const tc::tc_args& a, cudaStream_t st) {
+    switch (log_n) {
+    case 6: return launch_tc<6, PREC, MODE>(a, st);
+    case 7: return launch_tc<7, PREC, MODE>(a, st);
+    case 8: return launch_tc<8, PREC, MODE>(a, st);
     default: return cudaErrorNotSupported;
     }
 }
@@ -410,12 +505,57 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
         if (plan->dtype != PCX_F32 || plan->order != PCX_ORDER_NORMAL) {
             return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form: complex64, natural order");
         }
-        if (plan->log_n < 8 || plan->log_n > 12) {
-            return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form built for 2^8 <= N <= 2^12");
+        const bool two = plan->two_pass && plan->log_n1 >= 6 && plan->log_n1 <= 8 && plan->log_n2 >= 6 &&
+                         plan->log_n2 <= 8;
+        if (!two && (plan->log_n < 8 || plan->log_n > 12)) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form built for 2^8 <= N <= 2^16");
         }
         if (precision != 0 && precision != 1) return pcx_fail(PCX_ERR_INVALID, "precision: 0 bf16x3, 1 tf32x3");
         if ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) % 16 != 0) {
             return pcx_fail(PCX_ERR_INVALID, "data pointers must be 16-byte aligned");
+        }
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (two) {
+            // column pass into the plan's scratch (one L2-sized chunk of
+            // transforms at a time), row pass out to dst in natural order
+            const size_t per   = plan->n * sizeof(cpx<float>);
+            const size_t chunk = plan->chunk_rows(batch);
+            std::lock_guard<std::mutex> g(plan->mu);
+            if (plan->scratch_bytes < chunk * per) {
+                if (plan->scratch) cudaFree(plan->scratch);
+                plan->scratch       = nullptr;
+                plan->scratch_bytes = 0;
+                PCX_CUDA_TRY(cudaMalloc(&plan->scratch, chunk * per));
+                plan->scratch_bytes = chunk * per;
+            }
+            for (size_t r0 = 0; r0 < batch; r0 += chunk) {
+                const size_t rows = std::min(chunk, batch - r0);
+                tc::tc_args  c{};
+                c.src      = static_cast<const float*>(src) + r0 * 2 * plan->n;
+                c.dst      = static_cast<float*>(plan->scratch);
+                c.batch    = (long long)rows;
+                c.conj     = direction == PCX_INVERSE;
+                c.scale    = 1.0f;
+                c.twN      = plan->twN1;
+                c.error    = plan->err;
+                c.lg_other = plan->log_n2;
+                c.tw_hi    = plan->tw_hi;
+                c.tw_lo    = plan->tw_lo;
+                tc::tc_args r = c;
+                r.src      = static_cast<const float*>(plan->scratch);
+                r.dst      = static_cast<float*>(dst) + r0 * 2 * plan->n;
+                r.batch    = (long long)(rows << plan->log_n1);
+                r.scale    = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
+                r.twN      = plan->twN2;
+                r.lg_other = plan->log_n1;
+                cudaError_t e1 = precision == 0 ? dispatch_tc_pass<tc::PREC_BF16, 1>(plan->log_n1, c, st)
+                                                : dispatch_tc_pass<tc::PREC_TF32, 1>(plan->log_n1, c, st);
+                PCX_CUDA_TRY(e1);
+                cudaError_t e2 = precision == 0 ? dispatch_tc_pass<tc::PREC_BF16, 2>(plan->log_n2, r, st)
+                                                : dispatch_tc_pass<tc::PREC_TF32, 2>(plan->log_n2, r, st);
+                PCX_CUDA_TRY(e2);
+            }
+            return PCX_OK;
         }
         // full W_N table (the plan's single-pass table)
         tc::tc_args a{};
@@ -426,7 +566,6 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
         a.scale = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
         a.twN   = plan->twL;
         a.error = plan->err;
-        cudaStream_t st = static_cast<cudaStream_t>(stream);
         cudaError_t  e  = precision == 0 ? dispatch_tc<tc::PREC_BF16>(plan->log_n, a, st)
                                          : dispatch_tc<tc::PREC_TF32>(plan->log_n, a, st);
         PCX_CUDA_TRY(e);

@@ -23,7 +23,7 @@ def c4_input(rng, b, n):
     return z, k
 
 
-@pytest.mark.parametrize("log_n", [8, 9, 10, 11, 12])
+@pytest.mark.parametrize("log_n", [8, 9, 10, 11, 12, 13, 14, 15, 16])
 @pytest.mark.parametrize("precision", ["bf16", "tf32"])
 def test_tc_fft_accuracy(log_n, precision):
     n = 1 << log_n
@@ -48,3 +48,30 @@ def test_tc_fft_accuracy(log_n, precision):
     back = torch.empty_like(y)
     unit.exec_tensor_core(back, y, batch=b, direction=1, precision=precision)
     assert rel_l2(O.unpack(back.cpu().numpy(), n, 8), z) < 2 * bound
+
+
+@pytest.mark.parametrize("log_n", [14, 16])
+def test_tc_two_pass_matches_plain_and_chunks(log_n):
+    """The two-pass form agrees with the plain path, in place, and across
+    scratch chunks (a batch several times the chunk)."""
+    n = 1 << log_n
+    b = 3 * ((24 << 20) // (8 * n)) + 5    # several 24 MB chunks and a ragged last one
+    g = torch.Generator(device="cuda").manual_seed(14)
+    x = torch.randn(b * 2 * n, device="cuda", generator=g)
+    unit = fft_unit(n)
+    want = torch.empty_like(x)
+    unit.exec(want, x, batch=b)
+    y = x.clone()
+    unit.exec_tensor_core(y, y, batch=b, precision="tf32")    # in place
+    torch.cuda.synchronize()
+    unit.status()
+    err = (torch.linalg.vector_norm(y.double() - want.double()) / torch.linalg.vector_norm(want.double())).item()
+    assert err < TOL[np.float32]
+
+
+def test_tc_sizes_outside_the_form_are_refused():
+    for n in (128, 1 << 17):
+        unit = fft_unit(n)
+        x = torch.zeros(2 * n, device="cuda")
+        with pytest.raises(NotImplementedError, match="tensor-core form"):
+            unit.exec_tensor_core(x, x, batch=1)
