@@ -195,7 +195,6 @@ class C2Sweep:
         return self.points * B_PT * 2
 
     e2e_chunks = 8
-    e2e_reps = 1
 
     def e2e(self, torch, stream):
         host_in = torch.empty(2 * self.points, dtype=torch.float32).pin_memory()
@@ -217,7 +216,7 @@ class C2Sweep:
             u.exec(scratch[:n], buf, batch=rows, direction=0, stream=st)
             u.exec(buf, scratch[:n], batch=rows, direction=1, stream=st)
 
-        ms = pipelined_e2e(torch, host_in, host_out, chunks, scratch.numel(), compute, reps=self.e2e_reps)
+        ms = pipelined_e2e(torch, host_in, host_out, chunks, scratch.numel(), compute)
         nb = 2 * self.points * 4 * len(self.log_ns)
         return {"value": self.bytes_per_step() / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nb,
                 "d2h_bytes_per_step": nb, "ms_per_step": ms}
@@ -271,8 +270,6 @@ class C1(C2Sweep):
     name = "c1"
     log_ns = [10]
     points = 1024 * 64
-    e2e_chunks = 1    # 0.5 MB: one copy in, one transform pair, one copy out
-    e2e_reps = 200    # steps timed back to back, each one's copies and transforms overlapping its neighbours
 
     def config(self, world):
         return {"workload": "C1: N=1024, batch 64, forward then inverse (1/N), pack 8, U[-1,1) seed 0; step = "
@@ -314,6 +311,47 @@ class C1(C2Sweep):
             self.graph.replay()
         else:
             C2Sweep.run_part(self, "1024")
+
+    def e2e(self, torch, stream):
+        """Host -> device -> host per step: the copy in from pinned memory, the
+        forward and inverse exec calls and the copy out, captured together in
+        one CUDA graph (the step is launch-bound: 0.5 MB each way) and
+        replayed back to back."""
+        host_in = torch.empty(self.x.numel(), dtype=torch.float32).pin_memory()
+        host_in.copy_(self.x.cpu())
+        host_out = torch.empty_like(host_in).pin_memory()
+        buf, tmp = torch.empty_like(self.x), torch.empty_like(self.x)
+        u = self.units[10]
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+
+        def step():
+            buf.copy_(host_in, non_blocking=True)
+            u.exec(tmp, buf, batch=64, direction=0)
+            u.exec(buf, tmp, batch=64, direction=1)
+            host_out.copy_(buf, non_blocking=True)
+
+        with torch.cuda.stream(s):
+            for _ in range(3):
+                step()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                step()
+            for _ in range(3):
+                g.replay()
+        torch.cuda.synchronize()
+        reps = 500
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        with torch.cuda.stream(s):
+            for _ in range(reps):
+                g.replay()
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        nb = self.x.numel() * 4
+        return {"value": self.bytes_per_step() / (ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nb,
+                "d2h_bytes_per_step": nb, "ms_per_step": ms, "form": "CUDA graph of copy in, exec x2, copy out"}
 
     def launches(self):
         return 4    # two kernels per form
