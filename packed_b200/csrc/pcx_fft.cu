@@ -249,8 +249,8 @@ static int plan_init_tables(pcx_plan_s* p) {
             }
             PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
             // one launch for all chunks of a batch
-            if (pcx_fourstep(f64, p->log_n1, p->log_n2, fs_args{}, 0, p->sms, true, &p->fs_tc, &p->fs_tr) !=
-                cudaSuccess) {
+            if (pcx_fourstep(f64, p->log_n1, p->log_n2, fs_args{}, 0, p->sms, true, &p->fs_tc, &p->fs_tr,
+                             &p->fs_per_sm) != cudaSuccess) {
                 cudaGetLastError();
                 p->fs_tc = p->fs_tr = 0;
             }
@@ -663,7 +663,8 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         // by the time the copy warp reaches them
         const char*     re     = std::getenv("PCX_FS_ROUNDS");
         const long long rounds = re && std::atol(re) > 0 ? std::atol(re) : p->fs_rounds;
-        long long       lag    = (rounds * p->sms + per_t - 1) / per_t;
+        const long long ctas   = (long long)p->sms * std::max(1, p->fs_per_sm);
+        long long       lag    = (rounds * ctas + per_t - 1) / per_t;
         lag                    = std::max<long long>(1, std::min<long long>(lag, (long long)batch));
         const long long nslot  = std::min<long long>((long long)batch, 2 * lag + 2);
         std::lock_guard<std::mutex> g(p->mu);
@@ -703,7 +704,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         a.col_done   = p->fs_ctr;
         a.row_done   = p->fs_ctr + batch;
         a.error      = p->err;
-        PCX_CUDA_TRY(pcx_fourstep(f64, p->log_n1, p->log_n2, a, st, p->sms, false, nullptr, nullptr));
+        PCX_CUDA_TRY(pcx_fourstep(f64, p->log_n1, p->log_n2, a, st, p->sms, false, nullptr, nullptr, nullptr));
         return PCX_OK;
     }
 

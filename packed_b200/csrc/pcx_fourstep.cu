@@ -5,14 +5,20 @@
 namespace pcxg {
 
 template<class T, int LOGN1, int LOGN2>
-static cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc, int* tr) {
+static cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc, int* tr,
+                             int* per_sm) {
     using F = fs_cfg<T, LOGN1, LOGN2>;
     static_assert(F::SMEM <= 232448, "shared memory per block");
+    static_assert(F::MINB * (F::SMEM + 1024 + 256) <= 233472, "blocks per SM fit the shared memory");
     static_assert(F::STAGE % 128 == 0, "TMA destinations stay 128-byte aligned");
     auto kern = k_fourstep<T, LOGN1, LOGN2>;
     if (tc) *tc = F::TC;
     if (tr) *tr = F::TR;
-    if (attr_only) return set_smem(kern, F::SMEM);
+    if (attr_only) {
+        cudaError_t e = set_smem(kern, F::SMEM);
+        if (e == cudaSuccess && per_sm) e = occupancy_cached(reinterpret_cast<const void*>(kern), F::NT + 32, F::SMEM, per_sm);
+        return e;
+    }
     const long long items = a.batch * (F::TC + F::TR);
     if (items == 0) return cudaSuccess;
     // 3-D view of the source: [transform][n1][2*N2 reals], box = 64 bytes x min(N1, 256) rows
@@ -33,15 +39,15 @@ static cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool at
 
 template<class T>
 static cudaError_t dispatch_fs(int l1, int l2, const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc,
-                               int* tr) {
+                               int* tr, int* per_sm) {
     switch (l1 * 32 + l2) {
-    case 7 * 32 + 7: return launch_fs<T, 7, 7>(a, st, sms, attr_only, tc, tr);
-    case 8 * 32 + 7: return launch_fs<T, 8, 7>(a, st, sms, attr_only, tc, tr);
-    case 8 * 32 + 8: return launch_fs<T, 8, 8>(a, st, sms, attr_only, tc, tr);
-    case 9 * 32 + 8: return launch_fs<T, 9, 8>(a, st, sms, attr_only, tc, tr);
-    case 9 * 32 + 9: return launch_fs<T, 9, 9>(a, st, sms, attr_only, tc, tr);
-    case 10 * 32 + 9: return launch_fs<T, 10, 9>(a, st, sms, attr_only, tc, tr);
-    case 10 * 32 + 10: return launch_fs<T, 10, 10>(a, st, sms, attr_only, tc, tr);
+    case 7 * 32 + 7: return launch_fs<T, 7, 7>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 8 * 32 + 7: return launch_fs<T, 8, 7>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 8 * 32 + 8: return launch_fs<T, 8, 8>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 9 * 32 + 8: return launch_fs<T, 9, 8>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 9 * 32 + 9: return launch_fs<T, 9, 9>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 10 * 32 + 9: return launch_fs<T, 10, 9>(a, st, sms, attr_only, tc, tr, per_sm);
+    case 10 * 32 + 10: return launch_fs<T, 10, 10>(a, st, sms, attr_only, tc, tr, per_sm);
     default: return cudaErrorNotSupported;
     }
 }
@@ -49,7 +55,7 @@ static cudaError_t dispatch_fs(int l1, int l2, const fs_args& a, cudaStream_t st
 }    // namespace pcxg
 
 cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
-                         bool attr_only, int* col_tiles, int* row_tiles) {
-    return f64 ? pcxg::dispatch_fs<double>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles)
-               : pcxg::dispatch_fs<float>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles);
+                         bool attr_only, int* col_tiles, int* row_tiles, int* blocks_per_sm) {
+    return f64 ? pcxg::dispatch_fs<double>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm)
+               : pcxg::dispatch_fs<float>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm);
 }

@@ -58,7 +58,11 @@ template<class T, int LOGN1, int LOGN2>
 struct fs_cfg {
     static constexpr int N1   = 1 << LOGN1;
     static constexpr int N2   = 1 << LOGN2;
-    static constexpr int TILE = 65536 / (int)sizeof(cpx<T>);
+    // Two blocks per SM with 32 KB tiles while a column tile still spans
+    // whole 32-byte sectors of its rows (N1 <= 512): the two blocks' barrier
+    // phases run independently, so one issues while the other waits.
+    static constexpr int MINB = LOGN1 <= 9 ? 2 : 1;
+    static constexpr int TILE = 65536 / MINB / (int)sizeof(cpx<T>);
     static constexpr int G8   = 64 / (2 * (int)sizeof(T));
     static constexpr int LP   = G8 == 8 ? 3 : 2;
     static constexpr int C    = (TILE >> LOGN1) > G8 ? (TILE >> LOGN1) : G8;    // columns per column tile
@@ -79,7 +83,7 @@ struct fs_cfg {
     static constexpr int BASE = 2 * STAGE + XB;
     static constexpr int TB1  = stage_tw_smem_bytes<P1, T>();
     static constexpr int TB2  = stage_tw_smem_bytes<P2, T>();
-    static constexpr bool SH  = stw_fits(BASE, TB1 + TB2, 1);
+    static constexpr bool SH  = stw_fits(BASE, TB1 + TB2, MINB);
     static constexpr int SMEM = SH ? BASE + TB1 + TB2 : BASE;
     static constexpr int BOXY = N1 < 256 ? N1 : 256;
 };
@@ -142,7 +146,7 @@ __device__ __forceinline__ fs_item fs_decode(long long j, long long batch, int l
 }
 
 template<class T, int LOGN1, int LOGN2>
-__global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, 1)
+__global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LOGN1, LOGN2>::MINB)
     k_fourstep(const __grid_constant__ CUtensorMap tmap, fs_args a) {
     using F            = fs_cfg<T, LOGN1, LOGN2>;
     using P1           = typename F::P1;

@@ -111,6 +111,7 @@ struct pcx_plan_s {
     void*  stw_one  = nullptr;    // stage twiddles of a one-pass form of a two-pass size (N = 8192)
     int    fs_tc    = 0;          // one-launch four-step: column and row tiles per transform (0: none)
     int    fs_tr    = 0;
+    int    fs_per_sm = 1;         // its resident blocks per SM
     int*   fs_ctr   = nullptr;    // its dependency counters, 2 per transform
     size_t fs_ctr_n = 0;
     // form of the plan-owned-scratch path for n > 4096, set by pcx_plan_tune
@@ -154,7 +155,7 @@ namespace pcxg {
 struct fs_args;
 }
 cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
-                         bool attr_only, int* col_tiles, int* row_tiles);
+                         bool attr_only, int* col_tiles, int* row_tiles, int* blocks_per_sm);
 cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only);
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
