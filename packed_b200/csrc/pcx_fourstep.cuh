@@ -334,12 +334,22 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
     for (long long j = blockIdx.x; j < items; j += G, ++k) {
         const int      s   = (int)(k & 1);
         const uint32_t par = (uint32_t)((k >> 1) & 1);
+        const fs_item it = fs_decode(j, a.batch, a.lag, TC, TR);
+        // column tile: the four-step twiddle inputs are requested before the
+        // tile's data is waited for, and used after the stages
+        cpx<T> th{}, tl{}, tu{};
+        if (!it.row) {
+            const int      n2 = it.tile * C + tid % C;
+            const uint32_t e0 = (uint32_t)(tid / C) * (uint32_t)n2;
+            th                = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_hi) + (e0 >> LOGN2));
+            tl                = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_lo) + (e0 & (N2 - 1)));
+            tu                = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_b) + n2);
+        }
         // all compute warps leave together when any of them gave up
         if (compute_any_failed<NT>(!mbar_wait_bounded(&full[s], par))) {
             if (tid == 0) atomicExch(a.error, 1);
             return;
         }
-        const fs_item it = fs_decode(j, a.batch, a.lag, TC, TR);
         if (!it.row) {
             // ---------------- column tile: N1-point DFTs down C columns
             constexpr int E    = P1::E;
@@ -358,10 +368,6 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
-            const uint32_t e0 = (uint32_t)t * (uint32_t)n2;
-            const cpx<T>   th = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_hi) + (e0 >> LOGN2));
-            const cpx<T>   tl = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_lo) + (e0 & (N2 - 1)));
-            const cpx<T>   tu = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_b) + n2);
             stage_compute_tab<P1, 0>(v, t, stw1);
             run_stages_tab<P1, typename F::X1, SH, NT>(v, xch, c, t, stw1);
             const bool sok = mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1));
