@@ -109,6 +109,9 @@ int pcx_plan_form(pcx_plan plan, int* form, int* rounds, size_t* chunk_bytes);
  * the inverse by 1/n.  The out-of-place inverse computes the mathematically
  * correct inverse for every order (the reference's differs, fft.hpp:863-915).
  * stream: a cudaStream_t (NULL = legacy default stream).
+ * Pack widths: any power of two up to n for n <= 4096; up to 16 above, where
+ * widths beyond the two-pass kernels' own (8 for float, 4 for double) are
+ * changed in an extra pass over the rows (a wider source needs src_len = n).
  * Uses the plan's own scratch for n > 4096: concurrent execs of one plan on
  * different streams must use pcx_fft_exec_ws with separate workspaces.
  */

@@ -472,6 +472,44 @@ int check_pack(int pack, const char* what) {
     }
     return PCX_OK;
 }
+
+// Pack width change of `rows` rows of 2 * n reals (packs of at most 16, the
+// reference's widest; avx2_common.hpp:243-435 converts between its widths in
+// the FFT's loads and stores).  Each warp moves 32 consecutive reals of a row:
+// whole blocks of 2 * max(pack) reals, so the permutation stays inside the
+// warp, and every lane reads before any lane writes (dst may be src).
+template<class T>
+__global__ void k_repack(T* dst, const T* src, int lp_to, int lp_from, long long chunks, long long rows,
+                         long long dstride, long long sstride) {
+    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (w >= chunks * rows) return;    // uniform over the warp
+    const long long r  = w / chunks;
+    const long long o  = (w - r * chunks) * 32 + lane;    // offset of this real, source layout
+    const T         v  = src[r * sstride + o];
+    const long long e  = ((o >> (lp_from + 1)) << lp_from) | (o & ((1LL << lp_from) - 1));
+    const long long im = (o >> lp_from) & 1;
+    const long long d  = ((e >> lp_to) << (lp_to + 1)) + (e & ((1LL << lp_to) - 1)) + (im << lp_to);
+    __syncwarp();
+    dst[r * dstride + d] = v;
+}
+
+int repack(bool f64, void* dst, const void* src, int pack_to, int pack_from, size_t n, size_t rows,
+           size_t dstride, size_t sstride, cudaStream_t st) {
+    const long long chunks = (long long)(2 * n / 32);
+    const long long warps  = chunks * (long long)rows;
+    const unsigned  grid   = (unsigned)((warps * 32 + 255) / 256);
+    const int       lt = __builtin_ctz(pack_to), lf = __builtin_ctz(pack_from);
+    if (f64) {
+        k_repack<double><<<grid, 256, 0, st>>>(static_cast<double*>(dst), static_cast<const double*>(src), lt, lf,
+                                                chunks, (long long)rows, (long long)dstride, (long long)sstride);
+    } else {
+        k_repack<float><<<grid, 256, 0, st>>>(static_cast<float*>(dst), static_cast<const float*>(src), lt, lf,
+                                               chunks, (long long)rows, (long long)dstride, (long long)sstride);
+    }
+    PCX_CUDA_TRY(cudaGetLastError());
+    return PCX_OK;
+}
 }    // namespace
 
 int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int pd, int ps, int dir, int norm,
@@ -495,9 +533,11 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         return pcx_fail(PCX_ERR_UNSUPPORTED, "pack size larger than fft size is not supported");
     }
     const int cmin = p->dtype == PCX_F64 ? kcfg<double>::CMIN : kcfg<float>::CMIN;
-    if (p->two_pass && (pd > cmin || ps > cmin)) {
-        return pcx_fail(PCX_ERR_UNSUPPORTED, "pack sizes above " + std::to_string(cmin) +
-                                                 " are not supported for fft_size > 4096");
+    const bool wide = p->two_pass && (pd > cmin || ps > cmin);
+    if (wide && (pd > 16 || ps > 16 || (ps > cmin && src_len != n))) {
+        return pcx_fail(PCX_ERR_UNSUPPORTED, "pack sizes above " + std::to_string(ps > cmin && src_len != n ? cmin : 16) +
+                                                 " are not supported for fft_size > 4096" +
+                                                 (src_len != n ? " with a short source" : ""));
     }
     if (batch == 0) return PCX_OK;
     if (!dst || !src) return pcx_fail(PCX_ERR_INVALID, "null data pointer");
@@ -511,6 +551,25 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
     const size_t row_d = n * 2, row_s = n * 2;
     if (batch > 1 && (dstride < row_d || sstride < (src_len == n ? row_s : 0))) {
         return pcx_fail(PCX_ERR_INVALID, "row stride smaller than a row");
+    }
+    if (wide) {
+        // the two-pass kernels read and write packs of up to `cmin`: a wider
+        // source is repacked into dst first, a wider destination after
+        const bool   f64 = p->dtype == PCX_F64;
+        const size_t ds = batch > 1 ? dstride : row_d, ss = batch > 1 ? sstride : row_s;
+        const void*  s2 = src;
+        size_t       ss2 = ss;
+        if (ps > cmin) {
+            if (int rc = repack(f64, dst, src, cmin, ps, n, batch, ds, ss, st)) return rc;
+            s2  = dst;
+            ss2 = ds;
+        }
+        if (int rc = pcx_fft_run(p, dst, s2, src_len, std::min(pd, cmin), std::min(ps, cmin), dir, norm, batch, ds,
+                                 ss2, ws, ws_bytes, st, extra_scale, chunk_cap)) {
+            return rc;
+        }
+        if (pd > cmin) return repack(f64, dst, dst, pd, cmin, n, batch, ds, ds, st);
+        return PCX_OK;
     }
     const bool   inv   = dir == PCX_INVERSE;
     const double scale = (inv && norm ? 1.0 / (double)n : 1.0) * extra_scale;

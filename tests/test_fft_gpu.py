@@ -138,7 +138,7 @@ def test_pack_conversion_and_strides(n):
     z = normal_cx(rng, b, n)
     unit = fft_unit(n)
     want = np.fft.fft(z, axis=-1)
-    for ps, pd in ((1, 8), (8, 1), (2, 4), (4, 4), (8, 8)):
+    for ps, pd in ((1, 8), (8, 1), (2, 4), (4, 4), (8, 8), (16, 8), (8, 16), (16, 16), (1, 16), (16, 2)):
         pad_s, pad_d = 16, 48
         rs, rd = real_size(n, ps) + pad_s, real_size(n, pd) + pad_d
         src = np.zeros((b, rs), np.float32)
@@ -371,3 +371,31 @@ def test_vector_expressions_on_device(dtype):
     assert rel_l2(a.to_complex(), za * za) < TOL[npd]
     with pytest.raises(ValueError, match="not equal to subrange size"):
         out.assign(a + vector(n + 1, dtype=dtype))
+
+
+@pytest.mark.parametrize("n", [8192, 1 << 14, 1 << 17])
+def test_pack16_two_pass_sizes(n):
+    """Pack widths above the four-step kernels' own (8 reals for float, 4 for
+    double) are repacked around the transform: FP32 and FP64, in place and
+    out of place, forward and inverse."""
+    rng = np.random.default_rng(16)
+    b = 2
+    z = normal_cx(rng, b, n)
+    want = np.fft.fft(z, axis=-1)
+    for dt, npd, packs in ((F32, np.float32, ((16, 16), (16, 4), (2, 16))), (F64, np.float64, ((8, 8), (16, 4), (4, 16)))):
+        unit = fft_unit(n, dtype=dt)
+        tol = TOL[npd]
+        for ps, pd in packs:
+            x = to_dev(O.pack(z, ps, npd), dt)
+            y = torch.empty((b, real_size(n, pd)), dtype=dt, device="cuda")
+            unit.exec(y, x, batch=b, pack_src=ps, pack_dst=pd)
+            assert rel_l2(O.unpack(y.cpu().numpy(), n, pd), want) < tol, (dt, ps, pd)
+            back = torch.empty((b, real_size(n, ps)), dtype=dt, device="cuda")
+            unit.exec(back, y, batch=b, direction=1, pack_src=pd, pack_dst=ps)
+            assert rel_l2(O.unpack(back.cpu().numpy(), n, ps), z) < tol, (dt, ps, pd)
+            if ps == pd:    # in place
+                unit.exec(x, x, batch=b, pack_src=ps, pack_dst=pd)
+                assert rel_l2(O.unpack(x.cpu().numpy(), n, pd), want) < tol, (dt, ps, pd)
+        with pytest.raises(NotImplementedError, match="pack sizes above 16"):
+            big = torch.zeros(2 * n, dtype=dt, device="cuda")
+            unit.exec(big, big, pack_src=32, pack_dst=32)
