@@ -106,6 +106,13 @@ int main() {
         expect(rel_err(dst, y) < 2e-6, "fxcorr_unit(dest, src)", rel_err(dst, y));
         xc(f);
         expect(rel_err(f, y) < 2e-6, "fxcorr_unit(vector) in place", rel_err(f, y));
+        // a host std::vector<std::complex<float>> (pack 1), in place and out of place
+        std::vector<std::complex<float>> sv(s), so(s);
+        for (std::size_t i = 0; i < s; ++i) sv[i] = std::complex<float>(fd[i]);
+        xc(so, sv);
+        expect(rel_err(so, y) < 2e-6, "fxcorr_unit(std::vector dest, src)", rel_err(so, y));
+        xc(sv);
+        expect(rel_err(sv, y) < 2e-6, "fxcorr_unit(std::vector) in place", rel_err(sv, y));
     }
     {    // md::dynamic_storage (mdstorage.hpp): rows as vectors and batched row transforms
         enum class ax { x, y, z };
