@@ -617,7 +617,10 @@ __global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < ntile) issue(tile + 2 * (long long)gridDim.x, s);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X, SH>(v, xch, m, t, stw);
+        // a transform's TT <= 32 threads share one warp and its own exchange
+        // block: its exchanges need only that warp's barrier (the block-wide
+        // barriers before and after them order the stage and staging reuse)
+        run_stages_tab<P, X, SH, (TT <= 32 ? -1 : 0)>(v, xch, m, t, stw);
         __syncthreads();    // exchange reads done: reuse the buffer as staging
         {
             constexpr int S   = P::NST - 1;
