@@ -445,7 +445,7 @@ class C4TensorCore:
     def config(self, world):
         return {"workload": "C4: N in {256, 1024, 4096, 16384, 65536}, batch 4096, complex64 N(0,1) + 1e-3 tone at "
                             "a seeded bin (seed 4); tensor-core split-bf16 and split-tf32 forward vs plain FP32 "
-                            "forward",
+                            "forward; each part replayed from a CUDA graph of its exec call",
                 "global_batch_points": sum(self.batch << lg for lg in self.log_ns) * world,
                 "l2": "inputs 8-128 MiB per size; timed steps back to back",
                 "parallelism": f"independent shards x{world}"}
@@ -477,6 +477,26 @@ class C4TensorCore:
             self.units[lg] = fft_unit(n)
             if lg > 12:
                 self.units[lg].tune(self.batch)
+        # each part is one exec call of 8-512 MB; the small ones take a few
+        # microseconds on the GPU, less than the host needs to issue them, so
+        # every part is captured once in a CUDA graph and replayed
+        self.graphs = {}
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for key in self.parts():
+                for _ in range(2):
+                    self._call(key)
+                g = torch.cuda.CUDAGraph()
+                try:
+                    with torch.cuda.graph(g, stream=s):
+                        self._call(key)
+                    self.graphs[key] = g
+                except RuntimeError:    # a form that cannot be captured runs directly
+                    torch.cuda.synchronize()
+                    self.graphs[key] = None
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
 
     def forms_of(self, lg):
         return ("plain", "tc_bf16", "tc_tf32") if lg <= self.tc_max else ("plain",)
@@ -488,13 +508,20 @@ class C4TensorCore:
         m, n = key.split(":")
         return m, int(n).bit_length() - 1
 
-    def run_part(self, key):
+    def _call(self, key):
         m, lg = self._split(key)
         u = self.units[lg]
         if m == "plain":
             u.exec(self.y[lg], self.x[lg], batch=self.batch)
         else:
             u.exec_tensor_core(self.y[lg], self.x[lg], batch=self.batch, precision=m[3:])
+
+    def run_part(self, key):
+        g = self.graphs[key]
+        if g is None:
+            self._call(key)
+        else:
+            g.replay()
 
     def part_bytes(self, key):
         _, lg = self._split(key)
