@@ -1,6 +1,6 @@
 // Tensor Memory Accelerator (bulk copy) and mbarrier primitives, inline PTX
-// for sm_100a.  No cluster multicast anywhere: every copy names this CTA's
-// own shared memory and one global address.
+// for sm_100a.  Every copy names this CTA's own shared memory and one global
+// address of this GPU.
 #pragma once
 
 #include <cuda.h>
