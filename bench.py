@@ -444,7 +444,8 @@ class C4TensorCore:
 
     def config(self, world):
         return {"workload": "C4: N in {256, 1024, 4096, 16384, 65536}, batch 4096, complex64 N(0,1) + 1e-3 tone at "
-                            "a seeded bin (seed 4); tensor-core split-bf16 and split-tf32 forward vs plain FP32 "
+                            "a seeded bin (seed 4); tensor-core split-bf16 (2 parts, 3 products), split-tf32 and "
+                            "split-bf16 (3 parts, 6 products) forward vs plain FP32 "
                             "forward; each part replayed from a CUDA graph of its exec call",
                 "global_batch_points": sum(self.batch << lg for lg in self.log_ns) * world,
                 "l2": "inputs 8-128 MiB per size; timed steps back to back",
@@ -499,7 +500,7 @@ class C4TensorCore:
         torch.cuda.synchronize()
 
     def forms_of(self, lg):
-        return ("plain", "tc_bf16", "tc_tf32") if lg <= self.tc_max else ("plain",)
+        return ("plain", "tc_bf16", "tc_tf32", "tc_bf16x6") if lg <= self.tc_max else ("plain",)
 
     def parts(self):
         return [f"{m}:{1 << lg}" for lg in self.log_ns for m in self.forms_of(lg)]

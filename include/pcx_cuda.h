@@ -243,7 +243,9 @@ int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, const void*
  * stages as dense 32x32 real DFT-matrix products on the tensor cores
  * (tcgen05.mma, FP32 accumulation in tensor memory) with split operands,
  * precision 0: bfloat16 hi + lo, three products (kind::f16);
- * precision 1: tf32 hi + lo, three products (kind::tf32).
+ * precision 1: tf32 hi + lo, three products (kind::tf32);
+ * precision 2: bfloat16 hi + mid + lo, the six products up to second order
+ *              (kind::f16), FP32-level accuracy from bfloat16 operands.
  * `batch` contiguous rows of a complex64 plan in natural order, pack 8,
  * 2^8 <= n <= 2^16.  Up to 2^12 one launch transforms whole rows; 2^13..2^16
  * run as two passes of 2^6..2^8-point tensor-core transforms (columns, with

@@ -8,7 +8,9 @@
 // Operands are split so that the products recover FP32-level accuracy:
 //   PREC_BF16: x = hi + lo in bfloat16, D = Xh Ah + Xh Al + Xl Ah (three
 //              products, kind::f16);
-//   PREC_TF32: the same split in tf32 (kind::tf32).
+//   PREC_TF32: the same split in tf32 (kind::tf32);
+//   PREC_BF16X6: x = hi + mid + lo in bfloat16 and the six products whose
+//              parts add up to at most the second order (kind::f16).
 // The dropped lo*lo term and the representation error of hi + lo set the
 // accuracy (about 2^-16 per stage for bfloat16, 2^-21 for tf32).
 //
@@ -25,7 +27,7 @@ namespace pcxg {
 namespace tc {
 
 constexpr int NT = 128;
-enum : int { PREC_BF16 = 0, PREC_TF32 = 1 };
+enum : int { PREC_BF16 = 0, PREC_TF32 = 1, PREC_BF16X6 = 2 };
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
@@ -44,7 +46,7 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 template<int PREC>
 __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     const uint32_t z = 0;
-    if constexpr (PREC == PREC_BF16) {
+    if constexpr (PREC != PREC_TF32) {
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d),
@@ -91,19 +93,41 @@ struct op_traits;
 template<>
 struct op_traits<PREC_BF16> {
     using elem                      = uint16_t;
+    static constexpr int NS         = 2;    // parts of each operand
     static constexpr int K_PER_MMA  = 16;
     static constexpr int PER_CHUNK  = 8;    // elements per 16-byte core-matrix row
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
-    __device__ static void split(float x, elem& hi, elem& lo) {
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-        hi                    = __bfloat16_as_ushort(h);
-        lo                    = __bfloat16_as_ushort(l);
+    __device__ static elem bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+    __device__ static float fl(elem e) { return __bfloat162float(__ushort_as_bfloat16(e)); }
+    __device__ static void split(float x, elem (&p)[NS]) {
+        p[0] = bf(x);
+        p[1] = bf(x - fl(p[0]));
+    }
+    // the constant operand's parts, each rounded from the exact remainder
+    __device__ static void split_exact(double v, elem (&p)[NS]) {
+        p[0] = __bfloat16_as_ushort(__double2bfloat16(v));
+        p[1] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0])));
+    }
+};
+template<>
+struct op_traits<PREC_BF16X6> : op_traits<PREC_BF16> {
+    static constexpr int NS = 3;
+    __device__ static void split(float x, elem (&p)[NS]) {
+        p[0]          = bf(x);
+        const float r = x - fl(p[0]);    // exact
+        p[1]          = bf(r);
+        p[2]          = bf(r - fl(p[1]));
+    }
+    __device__ static void split_exact(double v, elem (&p)[NS]) {
+        p[0] = __bfloat16_as_ushort(__double2bfloat16(v));
+        p[1] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0])));
+        p[2] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0]) - (double)fl(p[1])));
     }
 };
 template<>
 struct op_traits<PREC_TF32> {
     using elem                      = uint32_t;
+    static constexpr int NS         = 2;
     static constexpr int K_PER_MMA  = 8;
     static constexpr int PER_CHUNK  = 4;
     static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
@@ -112,10 +136,30 @@ struct op_traits<PREC_TF32> {
         asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
         return r;
     }
-    __device__ static void split(float x, elem& hi, elem& lo) {
-        hi = to_tf32(x);
-        lo = to_tf32(x - __uint_as_float(hi));
+    __device__ static void split(float x, elem (&p)[NS]) {
+        p[0] = to_tf32(x);
+        p[1] = to_tf32(x - __uint_as_float(p[0]));
     }
+    __device__ static void split_exact(double v, elem (&p)[NS]) {
+        p[0] = to_tf32((float)v);
+        p[1] = to_tf32((float)(v - (double)__uint_as_float(p[0])));
+    }
+};
+
+// Products of the split operands, smallest first: (part of X, part of A).
+template<int NS>
+struct split_products;
+template<>
+struct split_products<2> {
+    static constexpr int NP = 3;
+    __host__ __device__ static constexpr int x(int p) { return p == 0 ? 1 : 0; }
+    __host__ __device__ static constexpr int a(int p) { return p == 1 ? 1 : 0; }
+};
+template<>
+struct split_products<3> {
+    static constexpr int NP = 6;
+    __host__ __device__ static constexpr int x(int p) { return p == 0 ? 2 : (p == 1 || p == 3) ? 1 : 0; }
+    __host__ __device__ static constexpr int a(int p) { return p == 2 ? 2 : (p == 1 || p == 4) ? 1 : 0; }
 };
 
 // Byte offset of element (row, k) of a rows x 32 K-major operand stored as
@@ -163,9 +207,10 @@ struct tc_cfg {
     static constexpr int R0B   = LOGN % 4;                    // remainder stage (CUDA cores) first
     static constexpr int NTC   = LOGN / 4;                    // radix-16 tensor-core stages
     static constexpr int OPB   = (int)sizeof(typename op_traits<PREC>::elem);
+    static constexpr int NS    = op_traits<PREC>::NS;
     static constexpr int ABYTE = 128 * 32 * OPB;
     static constexpr int BBYTE = 32 * 32 * OPB;
-    static constexpr int SMEM  = 2 * T * N * 8 + 2 * ABYTE + 2 * BBYTE;
+    static constexpr int SMEM  = 2 * T * N * 8 + NS * ABYTE + NS * BBYTE;
 };
 
 template<int LOGN, int PREC, int MODE>
@@ -180,10 +225,14 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     extern __shared__ __align__(128) unsigned char smem[];
     cpx<float>* work0 = reinterpret_cast<cpx<float>*>(smem);
     cpx<float>* work1 = work0 + T * N;
-    unsigned char* opA_hi = reinterpret_cast<unsigned char*>(work1 + T * N);
-    unsigned char* opA_lo = opA_hi + C::ABYTE;
-    unsigned char* opB_hi = opA_lo + C::ABYTE;
-    unsigned char* opB_lo = opB_hi + C::BBYTE;
+    constexpr int  NS = C::NS;    // parts of each split operand
+    unsigned char* opA[NS];       // the twiddled inputs X, part by part
+    unsigned char* opB[NS];       // the DFT matrix A
+    static_for<NS>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        opA[i]          = reinterpret_cast<unsigned char*>(work1 + T * N) + i * C::ABYTE;
+        opB[i]          = reinterpret_cast<unsigned char*>(work1 + T * N) + NS * C::ABYTE + i * C::BBYTE;
+    });
     __shared__ uint64_t mbar;
     __shared__ uint32_t tslot;
     bool                aborted = false;
@@ -210,17 +259,12 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         double v;
         if (n < 16) v = k < 16 ? c : s;
         else v = k < 16 ? -s : c;
-        E hi, lo;
-        O::split((float)v, hi, lo);
-        // exact lo from the double value
-        if constexpr (PREC == PREC_BF16) {
-            const __nv_bfloat16 h = __ushort_as_bfloat16(hi);
-            lo = __bfloat16_as_ushort(__double2bfloat16(v - (double)__bfloat162float(h)));
-        } else {
-            lo = O::to_tf32((float)(v - (double)__uint_as_float(hi)));
-        }
-        *reinterpret_cast<E*>(opB_hi + op_off<PREC, 32>(n, k)) = hi;
-        *reinterpret_cast<E*>(opB_lo + op_off<PREC, 32>(n, k)) = lo;
+        E part[NS];
+        O::split_exact(v, part);
+        static_for<NS>([&](auto ic) {
+            constexpr int i                                       = decltype(ic)::value;
+            *reinterpret_cast<E*>(opB[i] + op_off<PREC, 32>(n, k)) = part[i];
+        });
     }
     const bool conj_in  = MODE != 2 && a.conj;
     const bool conj_out = MODE != 1 && a.conj;
@@ -334,17 +378,21 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             // core-matrix row per store
             static_for<32 / O::PER_CHUNK>([&](auto cc) {
                 constexpr int c = decltype(cc)::value;
-                E             h[O::PER_CHUNK], l[O::PER_CHUNK];
+                E             part[NS][O::PER_CHUNK];
                 static_for<O::PER_CHUNK>([&](auto qc) {
-                    constexpr int kk = c * O::PER_CHUNK + decltype(qc)::value;
+                    constexpr int q  = decltype(qc)::value;
+                    constexpr int kk = c * O::PER_CHUNK + q;
                     const float   xv = kk < 16 ? x[kk & 15].re : x[kk & 15].im;
-                    O::split(xv, h[decltype(qc)::value], l[decltype(qc)::value]);
+                    E             e[NS];
+                    O::split(xv, e);
+                    static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
                 });
-                uint4 hv, lv;
-                memcpy(&hv, h, 16);
-                memcpy(&lv, l, 16);
-                *reinterpret_cast<uint4*>(opA_hi + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = hv;
-                *reinterpret_cast<uint4*>(opA_lo + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = lv;
+                static_for<NS>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    uint4         pv;
+                    memcpy(&pv, part[i], 16);
+                    *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = pv;
+                });
             });
             fence_proxy_async_smem();
             tc_fence_before();
@@ -354,16 +402,18 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
                 constexpr uint32_t LBO_A = (128 / 8) * 128, LBO_B = (32 / 8) * 128, SBO = 128;
                 constexpr int      KS    = 32 / O::K_PER_MMA;               // MMAs per product
                 constexpr int      CH    = O::K_PER_MMA / O::PER_CHUNK;     // chunks per MMA (2)
+                using SP                 = split_products<NS>;
                 uint32_t           acc   = 0;
-                const unsigned char* A[3] = {opA_lo, opA_hi, opA_hi};
-                const unsigned char* B[3] = {opB_hi, opB_lo, opB_hi};
-                for (int p = 0; p < 3; ++p) {
+                static_for<SP::NP>([&](auto pc) {
+                    constexpr int        p  = decltype(pc)::value;
+                    const unsigned char* xa = opA[SP::x(p)];
+                    const unsigned char* ab = opB[SP::a(p)];
                     for (int ks = 0; ks < KS; ++ks) {
-                        umma<PREC>(taddr, sdesc(A[p] + ks * CH * LBO_A, LBO_A, SBO), sdesc(B[p] + ks * CH * LBO_B, LBO_B, SBO),
+                        umma<PREC>(taddr, sdesc(xa + ks * CH * LBO_A, LBO_A, SBO), sdesc(ab + ks * CH * LBO_B, LBO_B, SBO),
                                    O::IDESC, acc);
                         acc = 1;
                     }
-                }
+                });
                 umma_commit(&mbar);
             }
             const bool ok = mbar_wait_bounded(&mbar, phase);
@@ -510,7 +560,7 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
         if (!two && (plan->log_n < 8 || plan->log_n > 12)) {
             return pcx_fail(PCX_ERR_UNSUPPORTED, "tensor-core form built for 2^8 <= N <= 2^16");
         }
-        if (precision != 0 && precision != 1) return pcx_fail(PCX_ERR_INVALID, "precision: 0 bf16x3, 1 tf32x3");
+        if (precision < 0 || precision > 2) return pcx_fail(PCX_ERR_INVALID, "precision: 0 bf16x3, 1 tf32x3, 2 bf16x6");
         if ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) % 16 != 0) {
             return pcx_fail(PCX_ERR_INVALID, "data pointers must be 16-byte aligned");
         }
@@ -548,11 +598,13 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
                 r.scale    = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
                 r.twN      = plan->twN2;
                 r.lg_other = plan->log_n1;
-                cudaError_t e1 = precision == 0 ? dispatch_tc_pass<tc::PREC_BF16, 1>(plan->log_n1, c, st)
-                                                : dispatch_tc_pass<tc::PREC_TF32, 1>(plan->log_n1, c, st);
+                cudaError_t e1 = precision == 0   ? dispatch_tc_pass<tc::PREC_BF16, 1>(plan->log_n1, c, st)
+                                 : precision == 1 ? dispatch_tc_pass<tc::PREC_TF32, 1>(plan->log_n1, c, st)
+                                                  : dispatch_tc_pass<tc::PREC_BF16X6, 1>(plan->log_n1, c, st);
                 PCX_CUDA_TRY(e1);
-                cudaError_t e2 = precision == 0 ? dispatch_tc_pass<tc::PREC_BF16, 2>(plan->log_n2, r, st)
-                                                : dispatch_tc_pass<tc::PREC_TF32, 2>(plan->log_n2, r, st);
+                cudaError_t e2 = precision == 0   ? dispatch_tc_pass<tc::PREC_BF16, 2>(plan->log_n2, r, st)
+                                 : precision == 1 ? dispatch_tc_pass<tc::PREC_TF32, 2>(plan->log_n2, r, st)
+                                                  : dispatch_tc_pass<tc::PREC_BF16X6, 2>(plan->log_n2, r, st);
                 PCX_CUDA_TRY(e2);
             }
             return PCX_OK;
@@ -566,8 +618,9 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
         a.scale = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
         a.twN   = plan->twL;
         a.error = plan->err;
-        cudaError_t  e  = precision == 0 ? dispatch_tc<tc::PREC_BF16>(plan->log_n, a, st)
-                                         : dispatch_tc<tc::PREC_TF32>(plan->log_n, a, st);
+        cudaError_t  e  = precision == 0   ? dispatch_tc<tc::PREC_BF16>(plan->log_n, a, st)
+                          : precision == 1 ? dispatch_tc<tc::PREC_TF32>(plan->log_n, a, st)
+                                           : dispatch_tc<tc::PREC_BF16X6>(plan->log_n, a, st);
         PCX_CUDA_TRY(e);
         return PCX_OK;
     });

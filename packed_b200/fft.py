@@ -339,8 +339,10 @@ class fft_unit:
 
     def exec_tensor_core(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
                          batch: int = 1, precision: str = "bf16", stream=None) -> None:
-        """Tensor-core form (pcx_tc_fft_exec): split-bf16 or split-tf32 DFT-matrix stages."""
-        prec = {"bf16": 0, "tf32": 1}[precision]
+        """Tensor-core form (pcx_tc_fft_exec): DFT-matrix stages with split operands, "bf16"
+        (two parts, three products), "tf32" (two parts, three products) or "bf16x6" (three
+        bf16 parts, six products)."""
+        prec = {"bf16": 0, "tf32": 1, "bf16x6": 2}[precision]
         _lib.check(_lib.lib().pcx_tc_fft_exec(self._plan, _ptr(dst), _ptr(src), direction, int(normalize), batch,
                                               prec, _stream_ptr(stream)))
 
