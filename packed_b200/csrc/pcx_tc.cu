@@ -210,7 +210,11 @@ struct tc_cfg {
     static constexpr int NS    = op_traits<PREC>::NS;
     static constexpr int ABYTE = 128 * 32 * OPB;
     static constexpr int BBYTE = 32 * 32 * OPB;
-    static constexpr int SMEM  = 2 * T * N * 8 + NS * ABYTE + NS * BBYTE;
+    // padded work layout (one pad element per 8): faster wherever it keeps
+    // three CTAs per SM or there is no remainder stage (measured per form)
+    static constexpr bool PAD  = PREC != PREC_TF32 || LOGN % 4 == 0;
+    static constexpr int  WORK = T * N + (PAD ? T * N / 8 : 0);    // complex per work buffer
+    static constexpr int  SMEM = 2 * WORK * 8 + NS * ABYTE + NS * BBYTE;
 };
 
 template<int LOGN, int PREC, int MODE>
@@ -223,15 +227,19 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     constexpr int T   = C::T;
     constexpr int NB  = T * N / 16;    // radix-16 butterflies per stage in this CTA
     extern __shared__ __align__(128) unsigned char smem[];
+    // work buffers: element i at wp(i) = i + i/8 (a pad after every 8 elements
+    // keeps the strided Stockham stores and the per-pack row accesses on
+    // distinct banks), or at i
+    auto        wp    = [](int i) { return C::PAD ? i + (i >> 3) : i; };
     cpx<float>* work0 = reinterpret_cast<cpx<float>*>(smem);
-    cpx<float>* work1 = work0 + T * N;
+    cpx<float>* work1 = work0 + C::WORK;
     constexpr int  NS = C::NS;    // parts of each split operand
     unsigned char* opA[NS];       // the twiddled inputs X, part by part
     unsigned char* opB[NS];       // the DFT matrix A
     static_for<NS>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        opA[i]          = reinterpret_cast<unsigned char*>(work1 + T * N) + i * C::ABYTE;
-        opB[i]          = reinterpret_cast<unsigned char*>(work1 + T * N) + NS * C::ABYTE + i * C::BBYTE;
+        opA[i]          = reinterpret_cast<unsigned char*>(work1 + C::WORK) + i * C::ABYTE;
+        opB[i]          = reinterpret_cast<unsigned char*>(work1 + C::WORK) + NS * C::ABYTE + i * C::BBYTE;
     });
     __shared__ uint64_t mbar;
     __shared__ uint32_t tslot;
@@ -281,15 +289,15 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             const int     i  = q % N, jg = q / N;
             const float4* s  = reinterpret_cast<const float4*>(base + 2 * (i * cols + c0 + 8 * jg));
             const float4  r0 = __ldg(s), r1 = __ldg(s + 1), i0 = __ldg(s + 2), i1 = __ldg(s + 3);
-            cpx<float>*   w  = work0 + (8 * jg) * N + i;
-            w[0 * N]         = {r0.x, cj * i0.x};
-            w[1 * N]         = {r0.y, cj * i0.y};
-            w[2 * N]         = {r0.z, cj * i0.z};
-            w[3 * N]         = {r0.w, cj * i0.w};
-            w[4 * N]         = {r1.x, cj * i1.x};
-            w[5 * N]         = {r1.y, cj * i1.y};
-            w[6 * N]         = {r1.z, cj * i1.z};
-            w[7 * N]         = {r1.w, cj * i1.w};
+            const int     b0 = (8 * jg) * N + i;
+            work0[wp(b0 + 0 * N)] = {r0.x, cj * i0.x};
+            work0[wp(b0 + 1 * N)] = {r0.y, cj * i0.y};
+            work0[wp(b0 + 2 * N)] = {r0.z, cj * i0.z};
+            work0[wp(b0 + 3 * N)] = {r0.w, cj * i0.w};
+            work0[wp(b0 + 4 * N)] = {r1.x, cj * i1.x};
+            work0[wp(b0 + 5 * N)] = {r1.y, cj * i1.y};
+            work0[wp(b0 + 6 * N)] = {r1.z, cj * i1.z};
+            work0[wp(b0 + 7 * N)] = {r1.w, cj * i1.w};
         }
     } else
     // rows in natural order (conjugated for the inverse); missing rows are zero
@@ -305,7 +313,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             i1              = __ldg(s + 3);
         }
         const float      cj = conj_in ? -1.f : 1.f;
-        cpx<float>*      w  = work0 + r * N + pk8 * 8;
+        cpx<float>*      w  = work0 + wp(r * N + pk8 * 8);    // 8 elements, no pad inside
         w[0] = {r0.x, cj * i0.x};
         w[1] = {r0.y, cj * i0.y};
         w[2] = {r0.z, cj * i0.z};
@@ -331,12 +339,12 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             cpx<float> x[R];
             static_for<R>([&](auto jc) {
                 constexpr int j = decltype(jc)::value;
-                x[j]            = in[tr * N + bl + j * (N / R)];
+                x[j]            = in[wp(tr * N + bl + j * (N / R))];
             });
             dft<R, 1, 0>(x);
             static_for<R>([&](auto jc) {
                 constexpr int j              = decltype(jc)::value;
-                out[tr * N + bl * R + j]     = x[j];
+                out[wp(tr * N + bl * R + j)] = x[j];
             });
         }
         ns = R;
@@ -368,7 +376,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             }
             static_for<16>([&](auto jc) {
                 constexpr int j = decltype(jc)::value;
-                cpx<float>    v = in[tr * N + bl + j * (N / 16)];
+                cpx<float>    v = in[wp(tr * N + bl + j * (N / 16))];
                 if constexpr (j > 0) {
                     if (ns > 1) v = cmul(v, stw_factor<4, j>(f));
                 }
@@ -434,7 +442,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             const int base = tr * N + (bl / ns) * ns * 16 + k;
             static_for<16>([&](auto jc) {
                 constexpr int j        = decltype(jc)::value;
-                out[base + j * ns]     = {__uint_as_float(r[j]), __uint_as_float(r[j + 16])};
+                out[wp(base + j * ns)] = {__uint_as_float(r[j]), __uint_as_float(r[j + 16])};
             });
             tc_fence_before();
             __syncthreads();    // operands and accumulator free for the next block
@@ -464,7 +472,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
                 const uint32_t ex = (uint32_t)(c0 + 8 * jg + e) * (uint32_t)k;    // < M
                 const cpx<float> t =
                     cmul(ldg_cpx(th + (ex >> lgo)), ldg_cpx(tl + (ex & (uint32_t)(cols - 1))));
-                const cpx<float> o = cmul(in[(8 * jg + e) * N + k], t);
+                const cpx<float> o = cmul(in[wp((8 * jg + e) * N + k)], t);
                 re[e]              = o.re;
                 im[e]              = o.im;
             });
@@ -482,18 +490,18 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         float*          base = a.dst + tr * (2 * N * R);
         for (int q = tid; q < T * N / 8; q += NT) {
             const int         k = q % N, jg = q / N;
-            const cpx<float>* w = in + (8 * jg) * N + k;
+            auto              w = [&](int e) { return in[wp((8 * jg + e) * N + k)]; };
             float4*           d = reinterpret_cast<float4*>(base + 2 * (k * R + j0 + 8 * jg));
-            d[0] = make_float4(w[0 * N].re * sc, w[1 * N].re * sc, w[2 * N].re * sc, w[3 * N].re * sc);
-            d[1] = make_float4(w[4 * N].re * sc, w[5 * N].re * sc, w[6 * N].re * sc, w[7 * N].re * sc);
-            d[2] = make_float4(w[0 * N].im * sim, w[1 * N].im * sim, w[2 * N].im * sim, w[3 * N].im * sim);
-            d[3] = make_float4(w[4 * N].im * sim, w[5 * N].im * sim, w[6 * N].im * sim, w[7 * N].im * sim);
+            d[0] = make_float4(w(0).re * sc, w(1).re * sc, w(2).re * sc, w(3).re * sc);
+            d[1] = make_float4(w(4).re * sc, w(5).re * sc, w(6).re * sc, w(7).re * sc);
+            d[2] = make_float4(w(0).im * sim, w(1).im * sim, w(2).im * sim, w(3).im * sim);
+            d[3] = make_float4(w(4).im * sim, w(5).im * sim, w(6).im * sim, w(7).im * sim);
         }
     } else if (!aborted) {
         const float sc = a.scale, sim = conj_out ? -a.scale : a.scale;
         for (int q = tid; q < rows * N / 8; q += NT) {
             const int         r = q / (N / 8), pk8 = q % (N / 8);
-            const cpx<float>* w = in + r * N + pk8 * 8;
+            const cpx<float>* w = in + wp(r * N + pk8 * 8);    // 8 elements, no pad inside
             float4*           d = reinterpret_cast<float4*>(a.dst + (row0 + r) * (2 * N) + pk8 * 16);
             d[0] = make_float4(w[0].re * sc, w[1].re * sc, w[2].re * sc, w[3].re * sc);
             d[1] = make_float4(w[4].re * sc, w[5].re * sc, w[6].re * sc, w[7].re * sc);
