@@ -356,24 +356,31 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
 
     uint32_t phase    = 0;
     int      tw_shift = LOGN - 4 - __ffs(ns) + 1;    // log2(N / (16 ns))
+    // twiddle j of a butterfly at position k is W_{16 ns}^(jk): one or two of
+    // the six factors W^(qk), q = 1,2,3,4,8,12, read from the W_N table
+    // (W_{16 ns}^e = W_N^(e * N / (16 ns))); each block's factors are
+    // requested while the previous block's products run
+    auto load_f = [&](cpx<float>(&g)[6], int nsx, int shx, int mbx) {
+        const int kx = ((mbx + tid) % (N / 16)) & (nsx - 1);
+        if (nsx > 1) {
+            g[0] = ldg_cpx(twN + ((kx) << shx));
+            g[1] = ldg_cpx(twN + ((2 * kx) << shx));
+            g[2] = ldg_cpx(twN + ((3 * kx) << shx));
+            g[3] = ldg_cpx(twN + ((4 * kx) << shx));
+            g[4] = ldg_cpx(twN + ((8 * kx) << shx));
+            g[5] = ldg_cpx(twN + ((12 * kx) << shx));
+        }
+    };
+    cpx<float> fn[6] = {};
+    load_f(fn, ns, tw_shift, 0);
     for (int st = 0; st < C::NTC; ++st) {
         for (int mb = 0; mb < NB; mb += 128) {
             const int  b  = mb + tid;
             const int  tr = b / (N / 16), bl = b % (N / 16);
             const int  k  = bl & (ns - 1);
             cpx<float> x[16];
-            // twiddle j of the butterfly is W_{16 ns}^(jk): one or two of the six
-            // factors W^(qk), q = 1,2,3,4,8,12, read from the W_N table
             cpx<float> f[6];
-            if (ns > 1) {
-                const int sh = tw_shift;    // W_{16 ns}^e = W_N^(e * N / (16 ns))
-                f[0]         = ldg_cpx(twN + ((k) << sh));
-                f[1]         = ldg_cpx(twN + ((2 * k) << sh));
-                f[2]         = ldg_cpx(twN + ((3 * k) << sh));
-                f[3]         = ldg_cpx(twN + ((4 * k) << sh));
-                f[4]         = ldg_cpx(twN + ((8 * k) << sh));
-                f[5]         = ldg_cpx(twN + ((12 * k) << sh));
-            }
+            static_for<6>([&](auto qc) { f[decltype(qc)::value] = fn[decltype(qc)::value]; });
             static_for<16>([&](auto jc) {
                 constexpr int j = decltype(jc)::value;
                 cpx<float>    v = in[wp(tr * N + bl + j * (N / 16))];
@@ -423,6 +430,11 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
                     }
                 });
                 umma_commit(&mbar);
+            }
+            if (mb + 128 < NB) {
+                load_f(fn, ns, tw_shift, mb + 128);
+            } else if (st + 1 < C::NTC) {
+                load_f(fn, ns * 16, tw_shift - 4, 0);
             }
             const bool ok = mbar_wait_bounded(&mbar, phase);
             if (__syncthreads_or(!ok)) {
