@@ -129,6 +129,11 @@ __device__ __forceinline__ bool compute_any_failed(bool bad) {
 }
 
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// counter += 1 with release semantics at GPU scope: this thread's earlier
+// writes, and those it has observed, are visible to whoever acquires the count
+__device__ __forceinline__ void red_release_add(int* p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ fs_item fs_decode(long long j, long long batch, int lag, int TC, int TR) {
     const long long A = (long long)lag * TC;
@@ -198,53 +203,71 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
 
     if (tid >= NT) {
         // ======================= copy warp
-        const int lane     = tid - NT;
-        long long pending  = -1;    // item whose completion is not yet published
-        int       pend_s   = 0;
-        uint32_t  pend_par = 0;
-        bool      fail     = false;
-        int       ncol[2]  = {0, 0};    // column items seen per stage (slotok / written phases)
-        int       pcol     = 0;         // written phase of the pending column item
+        const int      lane     = tid - NT;
+        const uint64_t pol      = l2_evict_first_policy();    // column tiles are read once
+        long long      pending  = -1;    // item whose completion is not yet published
+        int            pend_s   = 0;
+        uint32_t       pend_par = 0;
+        long long      rowdef   = -1;    // row item published once its stage was read
+        int            rd_s     = 0;
+        uint32_t       rd_par   = 0;
+        bool           fail     = false;
+        int            ncol[2]  = {0, 0};    // column items seen per stage (slotok / written phases)
+        int            pcol     = 0;         // written phase of the pending column item
         // bounded mbarrier wait by lane 0, the answer shared by the warp
         auto wwait = [&](uint64_t* bar, uint32_t parity) -> bool {
             int ok = 1;
             if (lane == 0) ok = mbar_wait_bounded(bar, parity) ? 1 : 0;
             return __shfl_sync(0xffffffffu, ok, 0) != 0;
         };
-        // publish the completion of `pending`
-        auto complete = [&]() {
+        // row item `jr` is done once its rows are in shared memory: drop their
+        // L2 lines unwritten and count it
+        auto publish_row = [&](long long jr) {
+            const fs_item it = fs_decode(jr, a.batch, a.lag, TC, TR);
+            const char*   g  = reinterpret_cast<const char*>(scr + (it.r % a.nslot) * (long long)(N1 * N2) +
+                                                          (long long)it.tile * CR * N2);
+            for (int q = lane; q < CR * RROW / 128; q += 32) l2_discard(g + (size_t)q * 128);
+            __syncwarp();
+            if (lane == 0) red_release_add(a.row_done + it.r, 1);
+        };
+        // the deferred row item, after waiting for its rows to land
+        auto flush_rowdef = [&]() {
+            if (rowdef < 0) return;
+            if (!wwait(&full[rd_s], rd_par)) fail = true;
+            if (!fail) publish_row(rowdef);
+            rowdef = -1;
+        };
+        // publish the completion of `pending`; a row item may instead be
+        // deferred until the compute warps have read its stage (so its copy
+        // has landed without waiting for it here)
+        auto complete = [&](bool defer_row) {
             if (pending < 0) return;
             const fs_item it = fs_decode(pending, a.batch, a.lag, TC, TR);
             if (!it.row) {
                 if (!wwait(&written[pend_s], (uint32_t)(pcol & 1))) fail = true;
                 if (lane == 0 && !fail) {
                     fence_proxy_async_global();    // the slot is read back by TMA copies
-                    __threadfence();
-                    atomicAdd(a.col_done + it.r, 1);
+                    red_release_add(a.col_done + it.r, 1);
                 }
+            } else if (defer_row) {
+                rowdef = pending;
+                rd_s   = pend_s;
+                rd_par = pend_par;
             } else {
                 if (!wwait(&full[pend_s], pend_par)) fail = true;
-                if (!fail) {
-                    // the rows are in shared memory: drop their L2 lines unwritten
-                    const char* g = reinterpret_cast<const char*>(scr + (it.r % a.nslot) * (long long)(N1 * N2) +
-                                                                  (long long)it.tile * CR * N2);
-                    for (int q = lane; q < CR * RROW / 128; q += 32) l2_discard(g + (size_t)q * 128);
-                }
-                __syncwarp();
-                if (lane == 0 && !fail) {
-                    __threadfence();
-                    atomicAdd(a.row_done + it.r, 1);
-                }
+                if (!fail) publish_row(pending);
             }
             pending = -1;
         };
-        // wait for *ctr >= target, publishing the pending completion first
+        // wait for *ctr >= target, publishing every pending completion first
         auto need = [&](const int* ctr, int target) -> bool {
             int v = 0;
             if (lane == 0) v = ld_acquire(ctr);
             v = __shfl_sync(0xffffffffu, v, 0);
             if (v >= target) return true;
-            complete();
+            flush_rowdef();
+            complete(false);
+            if (fail) return false;
             int ok = 1;
             if (lane == 0) ok = fs_wait(ctr, target) ? 1 : 0;
             return __shfl_sync(0xffffffffu, ok, 0) != 0;
@@ -257,11 +280,16 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                 fail = true;
                 break;
             }
+            // the stage's previous item (k-2) has been read: a deferred row
+            // item from it is done
+            if (rowdef >= 0) {
+                publish_row(rowdef);
+                rowdef = -1;
+            }
             const fs_item  it  = fs_decode(j, a.batch, a.lag, TC, TR);
             unsigned char* buf = ring + s * F::STAGE;
             if (!it.row) {
                 if (lane == 0) {
-                    const uint64_t pol = l2_evict_first_policy();
                     mbar_arrive_expect_tx(&full[s], F::COLB);
 #pragma unroll
                     for (int y = 0; y < N1; y += F::BOXY) {
@@ -282,7 +310,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                     fence_acq_rel_gpu();
                     mbar_arrive(&slotok[s]);
                 }
-                complete();
+                complete(true);
                 pending  = j;
                 pend_s   = s;
                 pend_par = par;
@@ -292,38 +320,34 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                     fail = true;
                     break;
                 }
+                // one bulk copy per row, issued by as many lanes
                 if (lane == 0) {
                     fence_proxy_async_global();    // column-pass writes -> TMA reads
-                    const cpx<T>* g = scr + (it.r % a.nslot) * (long long)(N1 * N2) + (long long)it.tile * CR * N2;
                     mbar_arrive_expect_tx(&full[s], CR * RROW);
-                    for (int q = 0; q < CR; ++q) {
-                        bulk_g2s(reinterpret_cast<cpx<T>*>(buf) + q * RSI, g + (long long)q * N2, RROW, &full[s]);
-                    }
                 }
                 __syncwarp();
-                complete();
+                const cpx<T>* g = scr + (it.r % a.nslot) * (long long)(N1 * N2) + (long long)it.tile * CR * N2;
+                for (int q = lane; q < CR; q += 32) {
+                    bulk_g2s(reinterpret_cast<cpx<T>*>(buf) + q * RSI, g + (long long)q * N2, RROW, &full[s]);
+                }
+                __syncwarp();
+                complete(true);
                 pending  = j;
                 pend_s   = s;
                 pend_par = par;
             }
         }
-        if (fail) {
-            // no copy may still be landing when the block exits
-            if (lane == 0) {
-                atomicExch(a.error, 1);
-                if (pending >= 0) mbar_wait_bounded(&full[pend_s], pend_par, 100000000ull);
-            }
-            __syncwarp();
-            return;
+        if (!fail) {
+            flush_rowdef();
+            complete(false);
         }
-        const int      last_s   = pend_s;
-        const uint32_t last_par = pend_par;
-        const bool     had      = pending >= 0;
-        complete();
         if (fail && lane == 0) {
+            // no copy may still be landing when the block exits
             atomicExch(a.error, 1);
-            if (had) mbar_wait_bounded(&full[last_s], last_par, 100000000ull);
+            if (pending >= 0) mbar_wait_bounded(&full[pend_s], pend_par, 100000000ull);
+            if (rowdef >= 0) mbar_wait_bounded(&full[rd_s], rd_par, 100000000ull);
         }
+        __syncwarp();
         return;
     }
 
