@@ -121,27 +121,36 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
         ch = item / a.nblk;
         b0 = (item - ch * a.nblk) * a.step - a.in_shift;
     };
-    // thread 0: claim the next item and start the copies of its rows that lie
-    // inside [0, len); the threads fill the others
+    // warp 0: thread 0 claims the next item; the warp's lanes start the
+    // copies of its rows that lie inside [0, len), a row each in turn; the
+    // threads fill the others
     auto claim_and_copy = [&]() {
-        const long long item = (long long)atomicAdd(a.counter, 1u);
-        s_item               = item;
+        if (tid == 0) {
+            const long long item = (long long)atomicAdd(a.counter, 1u);
+            s_item               = item;
+            if (item < a.total) {
+                long long ch, b0;
+                item_pos(item, ch, b0);
+                long long r_lo = b0 >= 0 ? 0 : (-b0 + N2 - 1) / N2;
+                long long r_hi = b0 + (long long)N1 * N2 <= a.len ? N1 : (a.len - b0) / N2;
+                r_lo           = r_lo > N1 ? N1 : r_lo;
+                r_hi           = r_hi < r_lo ? r_lo : (r_hi > N1 ? N1 : r_hi);
+                s_rlo          = (int)r_lo;
+                s_rhi          = (int)r_hi;
+                mbar_arrive_expect_tx(&full, (uint32_t)(r_hi - r_lo) * (N2 * 8));
+            }
+        }
+        __syncwarp();
+        const long long item = s_item;
         if (item >= a.total) return;
         long long ch, b0;
         item_pos(item, ch, b0);
-        long long r_lo = b0 >= 0 ? 0 : (-b0 + N2 - 1) / N2;
-        long long r_hi = b0 + (long long)N1 * N2 <= a.len ? N1 : (a.len - b0) / N2;
-        r_lo           = r_lo > N1 ? N1 : r_lo;
-        r_hi           = r_hi < r_lo ? r_lo : (r_hi > N1 ? N1 : r_hi);
-        s_rlo          = (int)r_lo;
-        s_rhi          = (int)r_hi;
-        mbar_arrive_expect_tx(&full, (uint32_t)(r_hi - r_lo) * (N2 * 8));
         const float* base = src + ch * a.src_stride + 2 * b0;    // packed: 2 reals per sample
-        for (long long r = r_lo; r < r_hi; ++r) bulk_g2s(win + r * RS, base + 2 * r * N2, N2 * 8, &full);
+        for (int r = s_rlo + tid; r < s_rhi; r += 32) bulk_g2s(win + r * RS, base + 2LL * r * N2, N2 * 8, &full);
     };
 
     __syncthreads();
-    if (tid == 0) claim_and_copy();
+    if (tid < 32) claim_and_copy();
     uint32_t phase = 0;
     for (;;) {
         __syncthreads();
@@ -298,7 +307,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                     // the window is read: start the next block's copies
                     fence_proxy_async_smem();
                     __syncthreads();
-                    if (tid == 0) claim_and_copy();
+                    if (tid < 32) claim_and_copy();
                 }
                 stage_compute_tab<P1, 0>(v, t, tw1);
                 run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
