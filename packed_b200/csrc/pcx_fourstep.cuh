@@ -128,7 +128,6 @@ __device__ __forceinline__ bool compute_any_failed(bool bad) {
     return r != 0;
 }
 
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 // counter += 1 with release semantics at GPU scope: this thread's earlier
 // writes, and those it has observed, are visible to whoever acquires the count
 __device__ __forceinline__ void red_release_add(int* p, int v) {
@@ -306,10 +305,10 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                     break;
                 }
                 __syncwarp();
-                if (lane == 0) {
-                    fence_acq_rel_gpu();
-                    mbar_arrive(&slotok[s]);
-                }
+                // the acquire of the slot's counter (or a first use of the
+                // slot) orders the compute warps' writes after the earlier
+                // row tiles' reads, through this arrive and their wait
+                if (lane == 0) mbar_arrive(&slotok[s]);
                 complete(true);
                 pending  = j;
                 pend_s   = s;
