@@ -225,6 +225,16 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
         }
         __syncthreads();
 
+        // in place: thread 0 reads the load flags of the first previous windows
+        // now, so that step 3 rarely has to wait for them
+        unsigned pflag[4] = {0u, 0u, 0u, 0u};
+        if (a.inplace && tid == 0) {
+            const long long blk = item % a.nblk;
+            static_for<4>([&](auto dc) {
+                constexpr int d = decltype(dc)::value + 1;
+                if (d <= a.hwait && d <= blk) pflag[d - 1] = ld_acquire(a.flags + (item - d));
+            });
+        }
         // ---------------- step 2: rows; spectrum times conj(K) or K; inverse rows
         {
             // the U groups of a half-warp take rows S apart, so their window
@@ -270,6 +280,13 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 const long long blk  = item % a.nblk;
                 for (int d = 1; d <= a.hwait && d <= blk && !s_abort; ++d) {
                     const unsigned* f = a.flags + (item - d);
+                    if (d <= 4) {
+                        unsigned pv = 0u;
+                        static_for<4>([&](auto ic) {
+                            if (decltype(ic)::value == d - 1) pv = pflag[decltype(ic)::value];
+                        });
+                        if (pv == a.epoch) continue;
+                    }
                     if (ld_acquire(f) == a.epoch) continue;
                     const unsigned long long t0 = globaltimer_ns();
                     while (ld_acquire(f) != a.epoch) {
