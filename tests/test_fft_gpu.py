@@ -7,7 +7,7 @@ import torch
 
 import oracle as O
 from packed_b200 import fft_order, fft_unit, real_size, vector
-from tests._util import TOL, golden, normal_cx, rel_l2, uniform_cx
+from tests._util import TOL, golden, normal_cx, rel_l2
 
 pytestmark = pytest.mark.gpu
 
