@@ -73,6 +73,17 @@ size_t pcx_plan_size(pcx_plan plan);
  * PCX_OK.  Synchronises with the device.
  */
 int pcx_plan_status(pcx_plan plan);
+
+/*
+ * Self-test of the bounded device waits (no reference counterpart).  One
+ * GPU thread waits on an mbarrier phase that never completes (for at most
+ * mbar_limit_ns) and on a device counter that never reaches its target (the
+ * four-step kernel's cross-block wait, about one second), with the same
+ * bounded waits the kernels use.  *mbar_satisfied / *counter_satisfied
+ * receive 1 if a wait saw its condition, 0 if it gave up; both must be 0,
+ * and the context stays usable.  Synchronises with the device.
+ */
+int pcx_selftest_waits(unsigned long long mbar_limit_ns, int* mbar_satisfied, int* counter_satisfied);
 /* Bytes of scratch an exec of this plan uses for `batch` rows (0 for n <= 4096). */
 size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
 

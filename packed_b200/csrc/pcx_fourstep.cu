@@ -59,3 +59,44 @@ cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& 
     return f64 ? pcxg::dispatch_fs<double>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm)
                : pcxg::dispatch_fs<float>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm);
 }
+
+namespace {
+// One thread runs the kernels' bounded waits on conditions that never come
+// true (phase 0 of an mbarrier nobody arrives on, a counter nobody
+// increments) and records whether each returned `true`; both must give up.
+__global__ void k_wait_probe(const int* ctr, int* out, unsigned long long mbar_limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        pcxg::mbar_init(&bar, 1);
+        pcxg::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = pcxg::mbar_wait_bounded(&bar, 0u, mbar_limit_ns) ? 1 : 0;
+        out[1] = pcxg::fs_wait(ctr, 1) ? 1 : 0;
+        out[2] = 1;    // the kernel got past both waits
+    }
+}
+}    // namespace
+
+extern "C" int pcx_selftest_waits(unsigned long long mbar_limit_ns, int* mbar_satisfied, int* counter_satisfied) {
+    return pcx_guard([&]() -> int {
+        if (!mbar_satisfied || !counter_satisfied) return pcx_fail(PCX_ERR_INVALID, "null result pointer");
+        int* d = nullptr;
+        PCX_CUDA_TRY(cudaMalloc(&d, 4 * sizeof(int)));
+        int         h[4] = {-1, -1, -1, 0};
+        cudaError_t e    = cudaMemset(d, 0, 4 * sizeof(int));
+        if (e == cudaSuccess) {
+            k_wait_probe<<<1, 32>>>(d + 3, d, mbar_limit_ns);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(h, d, 3 * sizeof(int), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        PCX_CUDA_TRY(e);
+        if (h[2] != 1) return pcx_fail(PCX_ERR_CUDA, "wait probe did not finish");
+        *mbar_satisfied    = h[0];
+        *counter_satisfied = h[1];
+        return PCX_OK;
+    });
+}
