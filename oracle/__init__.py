@@ -80,9 +80,11 @@ def ref() -> ctypes.CDLL:
         _ref.ref_fxcorr_fixed_f32.argtypes = [_fp, _c_size, _c_size, _fp, _c_size]
         _ref.ref_fft_batch_f32.argtypes = [ctypes.c_int, _c_size, _c_size, _fp, ctypes.c_int, ctypes.c_int]
         _ref.ref_fxcorr_fixed_batch_f32.argtypes = [_fp, _c_size, _c_size, _fp, _c_size, _c_size, ctypes.c_int]
+        _ref.ref_fft_raw_packs_f32.argtypes = [ctypes.c_int, _c_size, _c_size, _fp, _fp, ctypes.c_int,
+                                               ctypes.c_int]
         _ref.ref_last_error.restype = ctypes.c_char_p
         for name in ("ref_fft_f32", "ref_fft_oop_f32", "ref_fxcorr_f32", "ref_fxcorr_fixed_f32",
-                     "ref_fft_batch_f32", "ref_fxcorr_fixed_batch_f32"):
+                     "ref_fft_batch_f32", "ref_fxcorr_fixed_batch_f32", "ref_fft_raw_packs_f32"):
             getattr(_ref, name).restype = ctypes.c_int
     return _ref
 
@@ -209,6 +211,18 @@ def ref_fft_oop(src: np.ndarray, n: int, src_len: int, order: int, direction: in
     s = np.ascontiguousarray(src, dtype=np.float32)
     rc = ref().ref_fft_oop_f32(order, n, sub_size, dst.ctypes.data_as(_fp), s.ctypes.data_as(_fp), src_len,
                                direction, int(normalize))
+    if rc:
+        raise ValueError(ref().ref_last_error().decode())
+    return dst
+
+
+def ref_fft_raw_packs(src: np.ndarray, n: int, pack_dst: int, pack_src: int, order: int = 0,
+                      sub_size: int = 2048) -> np.ndarray:
+    """Forward transform of one row through the reference's fft_raw<PD, PS>(dest, source)."""
+    s = np.ascontiguousarray(src, dtype=np.float32)
+    dst = np.zeros(real_size(n, pack_dst), dtype=np.float32)
+    rc = ref().ref_fft_raw_packs_f32(order, n, sub_size, dst.ctypes.data_as(_fp), s.ctypes.data_as(_fp), pack_dst,
+                                     pack_src)
     if rc:
         raise ValueError(ref().ref_last_error().decode())
     return dst

@@ -182,6 +182,38 @@ int ref_fft_oop_f32(int order, std::size_t n, std::size_t sub_size, float* dst, 
     });
 }
 
+// Forward out-of-place transform at pack widths pd / ps through
+// fft_unit<float, Order>::fft_raw<PD, PS>(dest, source) (fft.hpp:645-670),
+// for PD, PS in {1, 2, 4, 8}: the reference's pack conversions in its
+// loads and stores (its AVX2 registers hold packs of at most 8 floats, so
+// wider packs do not compile there, avx2_common.hpp:444).
+int ref_fft_raw_packs_f32(int order, std::size_t n, std::size_t sub_size, float* dst, const float* src, int pd,
+                          int ps) {
+    return guarded([&] {
+        auto run = [&]<pcxo::fft_order O>() {
+            auto unit = pcxo::fft_unit<float, O>(n, sub_size);
+            auto with = [&]<std::size_t PD>() {
+                switch (ps) {
+                case 1: unit.template fft_raw<PD, 1>(dst, src); return 0;
+                case 2: unit.template fft_raw<PD, 2>(dst, src); return 0;
+                case 4: unit.template fft_raw<PD, 4>(dst, src); return 0;
+                case 8: unit.template fft_raw<PD, 8>(dst, src); return 0;
+                default: g_err = "unsupported source pack"; return 1;
+                }
+            };
+            switch (pd) {
+            case 1: return with.template operator()<1>();
+            case 2: return with.template operator()<2>();
+            case 4: return with.template operator()<4>();
+            case 8: return with.template operator()<8>();
+            default: g_err = "unsupported destination pack"; return 1;
+            }
+        };
+        return order == 0 ? run.template operator()<pcxo::fft_order::normal>()
+                          : run.template operator()<pcxo::fft_order::bit_reversed>();
+    });
+}
+
 // The reference's fxcorr_unit<float> exactly as shipped (fxcorr.hpp:62-136),
 // in place on `data` (s elements).  Correct only for single-block inputs.
 int ref_fxcorr_f32(const float* g, std::size_t k, std::size_t n_fft, float* data, std::size_t s) {

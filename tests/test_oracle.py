@@ -134,3 +134,18 @@ def test_pack_layout_roundtrip():
             a = O.pack(z, p)
             assert a.shape[-1] == O.real_size(n, p)
             np.testing.assert_allclose(O.unpack(a, n, p), z.astype(np.complex64))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("n", [64, 1024, 16384])
+def test_oracle_pack_conversions_match_reference(n):
+    """The reference's own fft_raw<PD, PS> (its pack conversions in the FFT's
+    loads and stores) against the oracle, natural and bit-reversed order."""
+    rng = np.random.default_rng(n + 3)
+    z = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    for order in (0, 1):
+        for ps, pd in ((1, 8), (8, 1), (2, 4), (4, 2), (1, 1), (2, 8)):
+            x = O.pack(z, ps)
+            got = O.ref_fft_raw_packs(x, n, pd, ps, order=order)
+            want = O.fft_packed(x, n, order=order, pack_src=ps, pack_dst=pd)
+            assert rel_l2(O.unpack(got, n, pd), O.unpack(want, n, pd)) < REF_TOL, (order, ps, pd)
