@@ -211,6 +211,28 @@ public:
         exec_batch(dest, source, batch, PackSize, PCX_INVERSE, Normalized, dest_stride, src_stride);
     }
 
+    // ---- tensor-core form (no reference counterpart, pcx_tc_fft_exec):
+    // `batch` contiguous device rows of size() complex64 elements at pack 8,
+    // natural order, 2^8 <= size() <= 2^16.  `precision` picks how each
+    // DFT-matrix operand is split: bf16x6 (three bfloat16 parts, six
+    // products) and tf32x3 stay within FP32-level error, bf16x3 does not.
+    enum class tc_precision : int { bf16x3 = 0, tf32x3 = 1, bf16x6 = 2 };
+    void fft_batch_tensor_core(T* dest, const T* source, uZ batch, tc_precision precision = tc_precision::bf16x6)
+        requires std::same_as<T, float>
+    {
+        detail_::check(pcx_tc_fft_exec(m_plan.get(), dest, source, PCX_FORWARD, 1, batch, static_cast<int>(precision),
+                                       m_stream));
+        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+    }
+    template<bool Normalized = true>
+    void ifft_batch_tensor_core(T* dest, const T* source, uZ batch, tc_precision precision = tc_precision::bf16x6)
+        requires std::same_as<T, float>
+    {
+        detail_::check(pcx_tc_fft_exec(m_plan.get(), dest, source, PCX_INVERSE, Normalized ? 1 : 0, batch,
+                                       static_cast<int>(precision), m_stream));
+        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+    }
+
     // Handle of the underlying C-ABI plan.
     [[nodiscard]] auto plan() const -> pcx_plan { return m_plan.get(); }
 

@@ -35,6 +35,16 @@ static double rel_err(const V& got, const std::vector<cd>& want) {
     return std::sqrt(num / den);
 }
 
+// The tensor-core calls of fft_unit<float> (a thin layer over
+// pcx_tc_fft_exec, whose results the Python GPU tests check per size and
+// precision): compiled here, not called.
+[[maybe_unused]] static void tensor_core_api(pcxo::fft_unit<float>& unit, float* dst, const float* src) {
+    using prec = pcxo::fft_unit<float>::tc_precision;
+    unit.fft_batch_tensor_core(dst, src, 2);
+    unit.fft_batch_tensor_core(dst, src, 2, prec::tf32x3);
+    unit.ifft_batch_tensor_core<false>(dst, src, 2, prec::bf16x3);
+}
+
 static int fails = 0;
 static void expect(bool ok, const char* what, double v = 0) {
     std::printf("%-44s %s %.3e\n", what, ok ? "ok  " : "FAIL", v);
