@@ -188,11 +188,22 @@ class C2Sweep:
     def run_part(self, key):
         lg = int(key).bit_length() - 1
         b = self.points >> lg
-        self.units[lg].exec(self.y, self.x, batch=b, direction=0)
-        self.units[lg].exec(self.x, self.y, batch=b, direction=1)
+        self.units[lg].exec(self.y, self.x, batch=b, direction=0, check=False)
+        self.units[lg].exec(self.x, self.y, batch=b, direction=1, check=False)
 
     def part_bytes(self, key):
         return self.points * B_PT * 2
+
+    def part_work(self, key):
+        """(transforms, 5 N log2 N flops) of one part: forward + inverse over the buffer."""
+        lg = int(key).bit_length() - 1
+        rows = self.points >> lg
+        return 2 * rows, 2 * rows * 5 * (1 << lg) * lg
+
+    def check_status(self):
+        """Raise if a kernel gave up a bounded wait during the run (rows unwritten)."""
+        for u in self.units.values():
+            u.status()
 
     e2e_chunks = 8
 
@@ -213,8 +224,8 @@ class C2Sweep:
         def compute(buf, n, lg, st):    # forward into scratch, inverse back: the exec calls themselves
             rows = n >> (lg + 1)
             u = self.units[lg]
-            u.exec(scratch[:n], buf, batch=rows, direction=0, stream=st)
-            u.exec(buf, scratch[:n], batch=rows, direction=1, stream=st)
+            u.exec(scratch[:n], buf, batch=rows, direction=0, stream=st, check=False)
+            u.exec(buf, scratch[:n], batch=rows, direction=1, stream=st, check=False)
 
         ms = pipelined_e2e(torch, host_in, host_out, chunks, scratch.numel(), compute)
         nb = 2 * self.points * 4 * len(self.log_ns)
@@ -262,8 +273,11 @@ class C2Sweep:
             tot_t += time.perf_counter() - t0
             tot_b += reps * rows * n * B_PT * 2
         return {"value": tot_b / tot_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-                "sample": f"reference fft_unit<float> (oracle/_ref) normal order fwd+inv on {threads} threads, "
-                          f"per N in 2^6..2^20 a batch of max({threads}, 2^22/N) rows repeated for ~{per:.1f} s"}
+                "sample": f"reference fft_unit<float> (oracle/_ref) normal order fwd+inv on {threads} threads; "
+                          f"per N in 2^{self.log_ns[0]}..2^{self.log_ns[-1]} a sample of max({threads}, 2^22/N) rows "
+                          f"(2^22 points = 32 MiB of complex64, of the 2^{self.points.bit_length() - 1}-point "
+                          f"workload) repeated for ~{per:.1f} s; GB/s in the bench's unit (16 B per point per "
+                          f"direction)"}
 
 
 class C1(C2Sweep):
@@ -306,6 +320,9 @@ class C1(C2Sweep):
     def parts(self):
         return ["1024", "direct:1024"]
 
+    def part_work(self, key):
+        return C2Sweep.part_work(self, "1024")
+
     def run_part(self, key):
         if key == "1024":
             self.graph.replay()
@@ -327,8 +344,8 @@ class C1(C2Sweep):
 
         def step():
             buf.copy_(host_in, non_blocking=True)
-            u.exec(tmp, buf, batch=64, direction=0)
-            u.exec(buf, tmp, batch=64, direction=1)
+            u.exec(tmp, buf, batch=64, direction=0, check=False)
+            u.exec(buf, tmp, batch=64, direction=1, check=False)
             host_out.copy_(buf, non_blocking=True)
 
         with torch.cuda.stream(s):
@@ -383,7 +400,17 @@ class C3Fxcorr:
         return ["fxcorr"]
 
     def run_part(self, key):
-        self.unit.exec(self.x, self.x, self.length, channels=self.channels)
+        self.unit.exec(self.x, self.x, self.length, channels=self.channels, check=False)
+
+    def check_status(self):
+        self.unit.status()
+
+    def part_work(self, key):
+        """Two N_fft-point transforms per overlap-save block (forward, inverse)."""
+        step = self.n_fft - self.k + 1
+        blocks = self.channels * -(-self.length // step)
+        lg = self.n_fft.bit_length() - 1
+        return 2 * blocks, 2 * blocks * 5 * self.n_fft * lg
 
     def part_bytes(self, key):
         return self.bytes_per_step()
@@ -397,7 +424,7 @@ class C3Fxcorr:
         chunks = [(c0 * per, min(group, self.channels - c0) * per, None) for c0 in range(0, self.channels, group)]
 
         def compute(buf, n, _, st):    # the correlator call itself, in place
-            self.unit.exec(buf, buf, self.length, channels=n // per, stream=st)
+            self.unit.exec(buf, buf, self.length, channels=n // per, stream=st, check=False)
 
         ms = pipelined_e2e(torch, host_in, host_out, chunks, group * per, compute)
         nb = self.x.numel() * 4
@@ -513,9 +540,9 @@ class C4TensorCore:
         m, lg = self._split(key)
         u = self.units[lg]
         if m == "plain":
-            u.exec(self.y[lg], self.x[lg], batch=self.batch)
+            u.exec(self.y[lg], self.x[lg], batch=self.batch, check=False)
         else:
-            u.exec_tensor_core(self.y[lg], self.x[lg], batch=self.batch, precision=m[3:])
+            u.exec_tensor_core(self.y[lg], self.x[lg], batch=self.batch, precision=m[3:], check=False)
 
     def run_part(self, key):
         g = self.graphs[key]
@@ -527,6 +554,14 @@ class C4TensorCore:
     def part_bytes(self, key):
         _, lg = self._split(key)
         return (self.batch << lg) * B_PT
+
+    def check_status(self):
+        for u in self.units.values():
+            u.status()
+
+    def part_work(self, key):
+        _, lg = self._split(key)
+        return self.batch, self.batch * 5 * (1 << lg) * lg
 
     def bytes_per_step(self):
         return sum(self.part_bytes(p) for p in self.parts())
@@ -617,6 +652,12 @@ class C5Ragged:
             self.xunits.append(fxcorr_unit(taps, nf))
         self.batch = ragged_batch(ffts, self.xcs)
         self.fft_points = sum(cnt << lg for lg, (cnt, _, _, _) in self.groups.items())
+        self.fft_flops = sum(cnt * 5 * (lg << lg) for lg, (cnt, _, _, _) in self.groups.items())
+        self.xc_ffts, self.xc_flops = 0, 0
+        for (_, _, s, taps, nf) in self.xcs:
+            blocks = -(-s // (nf - taps.size() + 1))
+            self.xc_ffts += 2 * blocks
+            self.xc_flops += 2 * blocks * 5 * nf * (nf.bit_length() - 1)
 
     def parts(self):
         return ["ragged_graph", "plain_per_size"]
@@ -626,12 +667,23 @@ class C5Ragged:
             self.batch()
         else:
             for lg, (cnt, src, dst, u) in self.groups.items():
-                u.exec(dst, src, batch=cnt)
+                u.exec(dst, src, batch=cnt, check=False)
             for (y, x, s, _, _), u in zip(self.xcs, self.xunits):
-                u.exec(y, x, s)
+                u.exec(y, x, s, check=False)
 
     def part_bytes(self, key):
         return (self.fft_points + self.xc_points) * B_PT
+
+    def part_work(self, key):
+        t = sum(cnt for cnt, _, _, _ in self.groups.values()) + self.xc_ffts
+        return t, self.fft_flops + self.xc_flops
+
+    def check_status(self):
+        self.batch.status()
+        for _, _, _, u in self.groups.values():
+            u.status()
+        for u in self.xunits:
+            u.status()
 
     def bytes_per_step(self):
         return self.part_bytes("ragged_graph")
@@ -698,6 +750,7 @@ def run(args, wl, rank, world):
                 ev[s][p][1].record(stream)
         t1.record(stream)
         barrier()
+    wl.check_status()    # outside the timed region: a bounded wait that gave up fails the run
     ms = t0.elapsed_time(t1)
     for s in range(args.steps):
         for p in wl.parts():
@@ -786,6 +839,21 @@ def main() -> None:
     top = max(mean, key=mean.get)
     ach = wl.part_bytes(top) / (mean[top] / 1e3) / 1e9
     per_part = {p: round(wl.part_bytes(p) / (mean[p] / 1e3) / 1e9, 1) for p in wl.parts()}
+    # throughput in the other units: transforms/s and 5 N log2 N GFLOP/s, whole
+    # job (all ranks), over the same device time as `value`
+    if wl.name in ("c1", "c4", "c5"):
+        if wl.name == "c5":
+            counted = ["ragged_graph"]
+        elif wl.name == "c1":
+            counted = ["1024"]
+        else:
+            counted = [min((f"{m}:{1 << lg}" for m in wl.forms_of(lg)), key=lambda q: means[q]) for lg in wl.log_ns]
+    else:
+        counted = wl.parts()
+    work = [wl.part_work(p) for p in counted]
+    n_tf, n_fl = sum(w[0] for w in work), sum(w[1] for w in work)
+    per_part_tps = {p: round(wl.part_work(p)[0] / (mean[p] / 1e3), 1) for p in wl.parts()}
+    per_part_gflops = {p: round(wl.part_work(p)[1] / (mean[p] / 1e3) / 1e9, 1) for p in wl.parts()}
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
@@ -795,7 +863,11 @@ def main() -> None:
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
         "pct_hbm": 100.0 * value / world / pk["hbm_gbs"],
+        "transforms_per_s": n_tf * world / (ms_step / 1e3),
+        "gflops_5nlogn": n_fl * world / (ms_step / 1e3) / 1e9,
         "per_part_gbs": per_part,
+        "per_part_transforms_per_s": per_part_tps,
+        "per_part_gflops_5nlogn": per_part_gflops,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": traffic, "peak_src": pk["src"],
                      "kernel": f"{wl.name}:{top}", "algorithmic_bytes": wl.part_bytes(top)},

@@ -84,6 +84,16 @@ int pcx_plan_status(pcx_plan plan);
  * and the context stays usable.  Synchronises with the device.
  */
 int pcx_selftest_waits(unsigned long long mbar_limit_ns, int* mbar_satisfied, int* counter_satisfied);
+/*
+ * Self-test of the give-up path of one plan (no reference counterpart).
+ * Enqueues on `stream` one GPU thread that waits, for at most limit_ns
+ * (<= 2 s), on an mbarrier phase that never completes and, when the wait
+ * gives up, sets the plan's error flag exactly as a transform kernel does
+ * when its input copy never lands.  The next pcx_plan_status after the
+ * stream has drained returns PCX_ERR_TIMEOUT (and clears the flag), which
+ * the C++ fft_unit turns into an exception.  No fault, no hang.
+ */
+int pcx_selftest_plan_wait(pcx_plan plan, unsigned long long limit_ns, void* stream);
 /* Bytes of scratch an exec of this plan uses for `batch` rows (0 for n <= 4096). */
 size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
 
@@ -194,9 +204,12 @@ int pcx_fft_exec_ws(pcx_plan plan, void* dst, const void* src, size_t src_len, i
  * scratch, processing the batch in chunks that fit it; sizes whose single
  * transform does not fit (n * element bytes > 8 MiB: only fp64 at n = 2^20)
  * are rejected with
- * PCX_ERR_UNSUPPORTED.  The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls whose GPU work overlaps race.
+ * PCX_ERR_UNSUPPORTED.  The first call on each device is its set-up: it
+ * looks up the array's device address (cudaGetSymbolAddress), which also
+ * makes the CUDA runtime load the module that holds the array (under lazy
+ * module loading, the default, the 8 MiB are committed then, by the
+ * loader); make that call during initialisation, before any stream capture.
+ * All calls share the array: calls whose GPU work overlaps race.
  * The plan itself must already exist (pcx_plan_create allocates).
  */
 int pcx_fft_exec_noalloc(pcx_plan plan, void* dst, const void* src, size_t src_len, int pack_dst, int pack_src,
@@ -233,9 +246,10 @@ int pcx_fxcorr_exec(pcx_fxcorr h, void* dst, const void* src, size_t len, int pa
                     size_t dst_stride, size_t src_stride, void* stream);
 
 /*
- * PCX_ERR_TIMEOUT if an in-place correlation since the last call had a block
- * give up waiting for its predecessor's read (bounded device wait; the
- * affected outputs are not written), else PCX_OK.  Synchronises the device.
+ * PCX_ERR_TIMEOUT if a correlation or adjoint of this handle since the last
+ * call had a block give up a bounded device wait (for its input copy, or, in
+ * place, for its predecessor's read; the affected outputs are not written),
+ * else PCX_OK.  Synchronises the device.
  */
 int pcx_fxcorr_status(pcx_fxcorr h);
 

@@ -222,7 +222,7 @@ public:
     {
         detail_::check(pcx_tc_fft_exec(m_plan.get(), dest, source, PCX_FORWARD, 1, batch, static_cast<int>(precision),
                                        m_stream));
-        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        sync();
     }
     template<bool Normalized = true>
     void ifft_batch_tensor_core(T* dest, const T* source, uZ batch, tc_precision precision = tc_precision::bf16x6)
@@ -230,7 +230,21 @@ public:
     {
         detail_::check(pcx_tc_fft_exec(m_plan.get(), dest, source, PCX_INVERSE, Normalized ? 1 : 0, batch,
                                        static_cast<int>(precision), m_stream));
-        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        sync();
+    }
+
+    // ---- adjoint (no reference counterpart; pcx_fft_vjp).  Given g_out, the
+    // cotangent of the output of fft_batch (inverse = false) or ifft_batch
+    // (inverse = true, scaled as Normalized says), writes g_in, the cotangent
+    // of that call's input: the forward DFT's adjoint is the unnormalised
+    // inverse, the inverse's is the forward scaled as the inverse was.
+    // `batch` device rows at pack PackSize, row stride in reals (0: packed).
+    template<bool Normalized = true, uZ PackSize = default_pack_size<T>>
+    void vjp(T* g_in, const T* g_out, uZ batch = 1, bool inverse = false, uZ stride = 0) {
+        const uZ row = detail_::real_size(m_size, PackSize);
+        detail_::check(pcx_fft_vjp(m_plan.get(), g_in, g_out, (int)PackSize, inverse ? PCX_INVERSE : PCX_FORWARD,
+                                   Normalized ? 1 : 0, batch, stride ? stride : row, m_stream));
+        sync();
     }
 
     // Handle of the underlying C-ABI plan.
@@ -265,7 +279,7 @@ private:
             detail_::device_view<T> v(dest, std::max(rd, rs), true);
             detail_::check(pcx_fft_exec(m_plan.get(), v.get(), v.get(), src_len, (int)pd, (int)ps, dir, norm, 1, rd, rs,
                                         m_stream));
-            detail_::check_cuda(cudaStreamSynchronize(m_stream));
+            sync();
             v.commit();
             return;
         }
@@ -273,7 +287,7 @@ private:
         detail_::device_view<T> s(const_cast<T*>(source), rs, true);
         detail_::check(
             pcx_fft_exec(m_plan.get(), d.get(), s.get(), src_len, (int)pd, (int)ps, dir, norm, 1, rd, rs, m_stream));
-        detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        sync();
         d.commit();
     }
 
@@ -283,7 +297,14 @@ private:
         ss           = ss ? ss : row;
         detail_::check(pcx_fft_exec(m_plan.get(), dest, source, m_size, (int)p, (int)p, dir, norm, batch, ds, ss,
                                     m_stream));
+        sync();
+    }
+
+    // Wait for the stream, then turn a bounded device wait that gave up
+    // (rows left unwritten, pcx_plan_status) into an exception.
+    void sync() {
         detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        detail_::check(pcx_plan_status(m_plan.get()));
     }
 
     struct plan_deleter {
@@ -383,6 +404,7 @@ public:
         detail_::check(pcx_fft_par_exec(m_plan.get(), dptr.data(), sptr.data(), m_size, len, (int)dt::pack_size,
                                         (int)st::pack_size, PCX_FORWARD, 0, m_stream));
         detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        detail_::check(pcx_plan_status(m_plan.get()));
         for (uZ i = 0; i < nstaged_dest; ++i) staged[i]->commit();
     }
 

@@ -93,6 +93,7 @@ public:
         detail_::device_view<T> s(const_cast<T*>(st::re_data(source)), row, true);
         detail_::check(pcx_fxcorr_exec(m_h.get(), d.get(), s.get(), n, (int)st::pack_size, 1, row, row, m_stream));
         detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        detail_::check(pcx_fxcorr_status(m_h.get()));
         d.commit();
     }
 
@@ -103,7 +104,7 @@ public:
         detail_::check(pcx_fxcorr_exec(m_h.get(), dest, source, len, (int)PackSize, channels,
                                        dest_stride ? dest_stride : row, src_stride ? src_stride : row, m_stream));
         detail_::check_cuda(cudaStreamSynchronize(m_stream));
-        if (dest == source) detail_::check(pcx_fxcorr_status(m_h.get()));
+        detail_::check(pcx_fxcorr_status(m_h.get()));
     }
 
     // Adjoint: gx = d loss/dx (convolution of gy with g); gg (optional) = d loss/dg.
@@ -112,6 +113,7 @@ public:
         const uZ row = detail_::real_size(len, PackSize);
         detail_::check(pcx_fxcorr_vjp(m_h.get(), gx, gg, gy, x, len, (int)PackSize, channels, row, m_stream));
         detail_::check_cuda(cudaStreamSynchronize(m_stream));
+        detail_::check(pcx_fxcorr_status(m_h.get()));
     }
 
 private:

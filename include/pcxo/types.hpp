@@ -149,10 +149,27 @@ bool operator==(const device_allocator<T>&, const device_allocator<U>&) noexcept
     return true;
 }
 
-// The reference's default allocator name (allocators.hpp:11-48).  On this
-// build it hands out managed memory so existing code runs on the GPU unchanged.
+// The reference's default allocator name (allocators.hpp:11-48).  It hands
+// out managed memory so existing code runs on the GPU unchanged; CUDA aligns
+// every managed allocation to at least 256 bytes, so any Alignment up to 256
+// (the reference's default is 64) is met, and larger ones are rejected at
+// compile time.
 template<typename T, std::align_val_t Alignment = std::align_val_t{64}>
-using aligned_allocator = managed_allocator<T>;
+class aligned_allocator : public managed_allocator<T> {
+    static_assert(static_cast<std::size_t>(Alignment) <= 256 &&
+                      (static_cast<std::size_t>(Alignment) & (static_cast<std::size_t>(Alignment) - 1)) == 0,
+                  "aligned_allocator: managed memory is aligned to 256 bytes; Alignment must be a power of two <= 256");
+
+public:
+    aligned_allocator() noexcept = default;
+    template<typename U>
+    aligned_allocator(const aligned_allocator<U, Alignment>&) noexcept {}
+
+    template<typename U>
+    struct rebind {
+        using other = aligned_allocator<U, Alignment>;
+    };
+};
 
 /**
  * Customisation point (types.hpp:113-148): real_type, pack_size,

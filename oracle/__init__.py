@@ -36,9 +36,16 @@ _lib = None
 _ref = None
 
 
+# Reference checkout the shim is compiled from: PCX_REFERENCE, else
+# /root/reference.  Where neither exists the prebuilt _ref library is used.
+REFERENCE_DIR = os.environ.get("PCX_REFERENCE", "/root/reference")
+
+
 def build() -> None:
     """Compile liboracle.so (and the reference shim when the sources exist)."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    ref = Path(REFERENCE_DIR)
+    args = [f"REF={ref}"] if ref.is_dir() else []
+    subprocess.run(["make", "-s", "-C", str(HERE), *args], check=True)
 
 
 def lib() -> ctypes.CDLL:

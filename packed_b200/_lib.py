@@ -32,6 +32,7 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_plan_size": (_sz, [_vp]),
     "pcx_plan_status": (_i, [_vp]),
     "pcx_selftest_waits": (_i, [ctypes.c_ulonglong, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "pcx_selftest_plan_wait": (_i, [_vp, ctypes.c_ulonglong, _vp]),
     "pcx_plan_workspace_size": (_sz, [_vp, _sz]),
     "pcx_plan_tune": (_i, [_vp, _sz, _vp, ctypes.POINTER(_i)]),
     "pcx_plan_form": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_sz)]),

@@ -10,13 +10,19 @@
 // holds until the process exits.
 //
 // The array's name in host code is a host-side stand-in, not a device
-// address, so its device address is looked up with cudaGetSymbolAddress once
-// per device (with that device current) on the first call on that device and
-// passed to the kernels.  That first call should therefore come before any
-// stream capture.  Calls share the array and it keeps the last call's
-// contents; the four-step passes write every scratch element before reading
-// it, so nothing needs clearing.  Calls whose GPU work overlaps (different
-// streams, other threads) race on the array.
+// address, so its device address is looked up with cudaGetSymbolAddress, with
+// the device current, on the first call on that device (set-up) and passed to
+// the kernels.  That lookup also makes the CUDA runtime load the array's
+// module (with lazy module loading, the default, the 8 MiB are committed
+// then, by the loader), so the first call on each device belongs in the
+// caller's initialisation and should come before any stream capture.  The
+// address is cached per device together with the context it was looked up
+// in, and looked up again when the device's context has changed (after a
+// reset the module is loaded anew and may sit elsewhere).  Calls share the
+// array and it keeps the last call's contents; the four-step passes write
+// every scratch element before reading it, so nothing needs clearing.  Calls
+// whose GPU work overlaps (different streams, other threads) race on the
+// array.
 #include "pcx_host.hpp"
 
 #include <mutex>
@@ -27,24 +33,53 @@ namespace {
 __device__ __align__(256) unsigned char g_noalloc_scratch[PCX_NOALLOC_SCRATCH_BYTES];
 
 constexpr int MAX_DEVICES = 64;
-void*         g_scratch_ptr[MAX_DEVICES];
+struct scratch_entry {
+    void* ctx;    // CUcontext current when the address was looked up
+    void* ptr;
+};
+scratch_entry g_scratch[MAX_DEVICES];
 std::mutex    g_scratch_mutex;
 
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// cuCtxGetCurrent through the runtime's driver entry point (no -lcuda).
+using ctx_get_fn = int (*)(void**);
+ctx_get_fn ctx_get() {
+    static ctx_get_fn f = []() -> ctx_get_fn {
+        void*                           p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            return nullptr;
+        }
+        return reinterpret_cast<ctx_get_fn>(p);
+    }();
+    return f;
+}
+void* current_ctx() {
+    void* c = nullptr;
+    if (ctx_get_fn f = ctx_get()) {
+        if (f(&c) != 0) c = nullptr;
+    }
+    return c;
+}
+
+// Device address of g_noalloc_scratch on the current device.
 int scratch_address(void** out) {
     int dev = 0;
     PCX_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= MAX_DEVICES) return pcx_fail(PCX_ERR_UNSUPPORTED, "device index out of range");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void*       p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            return pcx_fail(PCX_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    scratch_entry&              e   = g_scratch[dev];
+    void*                       ctx = current_ctx();
+    if (!e.ptr || !ctx || e.ctx != ctx) {
+        void*       p  = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (rc != cudaSuccess || !p) {
+            return pcx_fail(PCX_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(rc));
         }
-        g_scratch_ptr[dev] = p;
+        e.ptr = p;
+        e.ctx = current_ctx();    // the lookup has made the primary context current
     }
-    *out = g_scratch_ptr[dev];
+    *out = e.ptr;
     return PCX_OK;
 }
 

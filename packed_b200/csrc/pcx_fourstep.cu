@@ -79,6 +79,31 @@ __global__ void k_wait_probe(const int* ctr, int* out, unsigned long long mbar_l
 }
 }    // namespace
 
+namespace {
+// One thread waits, bounded by limit_ns, on phase 0 of an mbarrier nobody
+// arrives on and, when the wait gives up, records it in the plan's error flag
+// exactly as the transform kernels do when their input copy never lands.
+__global__ void k_plan_wait_probe(int* err, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        pcxg::mbar_init(&bar, 1);
+        pcxg::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !pcxg::mbar_wait_bounded(&bar, 0u, limit_ns)) atomicExch(err, 1);
+}
+}    // namespace
+
+extern "C" int pcx_selftest_plan_wait(pcx_plan plan, unsigned long long limit_ns, void* stream) {
+    return pcx_guard([&]() -> int {
+        if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
+        if (limit_ns > 2000000000ull) return pcx_fail(PCX_ERR_INVALID, "wait limit above 2 s");
+        k_plan_wait_probe<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(plan->err, limit_ns);
+        PCX_CUDA_TRY(cudaGetLastError());
+        return PCX_OK;
+    });
+}
+
 extern "C" int pcx_selftest_waits(unsigned long long mbar_limit_ns, int* mbar_satisfied, int* counter_satisfied) {
     return pcx_guard([&]() -> int {
         if (!mbar_satisfied || !counter_satisfied) return pcx_fail(PCX_ERR_INVALID, "null result pointer");

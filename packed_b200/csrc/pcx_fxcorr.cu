@@ -355,7 +355,7 @@ extern "C" int pcx_fxcorr_status(pcx_fxcorr h) {
         PCX_CUDA_TRY(cudaMemcpy(&err, h->ctl + 1, sizeof(unsigned), cudaMemcpyDeviceToHost));
         if (err) {
             PCX_CUDA_TRY(cudaMemset(h->ctl + 1, 0, sizeof(unsigned)));
-            return pcx_fail(PCX_ERR_TIMEOUT, "an in-place correlation block gave up waiting for its predecessor");
+            return pcx_fail(PCX_ERR_TIMEOUT, "a correlation block gave up a bounded wait (for its input copy or, in place, for its predecessor)");
         }
         return PCX_OK;
     });

@@ -261,8 +261,13 @@ class fft_unit:
     def exec(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
              batch: int = 1, pack_dst: int | None = None, pack_src: int | None = None, src_len: int = 0,
              dst_stride: int | None = None, src_stride: int | None = None, stream=None,
-             workspace: torch.Tensor | None = None) -> None:
-        """Batched transform of `batch` rows of packed reals (pcx_fft_exec)."""
+             workspace: torch.Tensor | None = None, check: bool = True) -> None:
+        """Batched transform of `batch` rows of packed reals (pcx_fft_exec).
+
+        With ``check`` (the default) the call waits for the stream and raises
+        TimeoutError if a kernel gave up a bounded wait and left rows
+        unwritten; ``check=False`` returns as soon as the work is queued, and
+        the caller reads the flag later with :meth:`status`."""
         pd = pack_dst or default_pack_size(self._dtype)
         ps = pack_src or pd
         if dst.dtype != self._dtype or src.dtype != self._dtype:
@@ -278,6 +283,12 @@ class fft_unit:
                                    batch, ds, ss, _ptr(workspace), workspace.numel() * workspace.element_size(),
                                    _stream_ptr(stream))
         _lib.check(rc)
+        if check:
+            self._wait_and_check(stream)
+
+    def _wait_and_check(self, stream) -> None:
+        (stream if stream is not None else torch.cuda.current_stream()).synchronize()
+        self.status()
 
     def fft_raw(self, dest: torch.Tensor, source: torch.Tensor | None = None, source_size: int | None = None,
                 pack_dest: int = 1, pack_src: int = 1) -> None:
@@ -338,13 +349,15 @@ class fft_unit:
                              f"to destination pack size (which is {dest.pack_size})")
 
     def exec_tensor_core(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,
-                         batch: int = 1, precision: str = "bf16", stream=None) -> None:
+                         batch: int = 1, precision: str = "bf16", stream=None, check: bool = True) -> None:
         """Tensor-core form (pcx_tc_fft_exec): DFT-matrix stages with split operands, "bf16"
         (two parts, three products), "tf32" (two parts, three products) or "bf16x6" (three
-        bf16 parts, six products)."""
+        bf16 parts, six products).  ``check`` as in :meth:`exec`."""
         prec = {"bf16": 0, "tf32": 1, "bf16x6": 2}[precision]
         _lib.check(_lib.lib().pcx_tc_fft_exec(self._plan, _ptr(dst), _ptr(src), direction, int(normalize), batch,
                                               prec, _stream_ptr(stream)))
+        if check:
+            self._wait_and_check(stream)
 
     # ------------------------------------------------------------- adjoint
     def vjp(self, g_out: torch.Tensor, *, direction: int = 0, normalize: bool = True, batch: int = 1,
@@ -427,19 +440,25 @@ class fxcorr_unit:
         return (self._n - (self._k - 1)) // p * p
 
     def status(self) -> None:
-        """Raise TimeoutError if an in-place block gave up waiting (pcx_fxcorr_status)."""
+        """Raise TimeoutError if a block gave up a bounded wait (pcx_fxcorr_status)."""
         _lib.check(_lib.lib().pcx_fxcorr_status(self._h))
 
     def kernel_size(self) -> int:
         return self._k
 
     def exec(self, dst: torch.Tensor, src: torch.Tensor, length: int, *, channels: int = 1, pack: int | None = None,
-             dst_stride: int | None = None, src_stride: int | None = None, stream=None) -> None:
+             dst_stride: int | None = None, src_stride: int | None = None, stream=None,
+             check: bool = True) -> None:
+        """Correlate `channels` rows (pcx_fxcorr_exec).  With ``check`` (the default) the call
+        waits for the stream and raises TimeoutError if a block gave up a bounded wait."""
         p = pack or default_pack_size(self._dtype)
         rs = real_size(length, p)
         _lib.check(_lib.lib().pcx_fxcorr_exec(self._h, _ptr(dst), _ptr(src), length, p, channels,
                                               dst_stride if dst_stride is not None else rs,
                                               src_stride if src_stride is not None else rs, _stream_ptr(stream)))
+        if check:
+            (stream if stream is not None else torch.cuda.current_stream()).synchronize()
+            self.status()
 
     def __call__(self, dest: vector, source: vector | None = None) -> None:
         if source is None:

@@ -35,16 +35,6 @@ static double rel_err(const V& got, const std::vector<cd>& want) {
     return std::sqrt(num / den);
 }
 
-// The tensor-core calls of fft_unit<float> (a thin layer over
-// pcx_tc_fft_exec, whose results the Python GPU tests check per size and
-// precision): compiled here, not called.
-[[maybe_unused]] static void tensor_core_api(pcxo::fft_unit<float>& unit, float* dst, const float* src) {
-    using prec = pcxo::fft_unit<float>::tc_precision;
-    unit.fft_batch_tensor_core(dst, src, 2);
-    unit.fft_batch_tensor_core(dst, src, 2, prec::tf32x3);
-    unit.ifft_batch_tensor_core<false>(dst, src, 2, prec::bf16x3);
-}
-
 static int fails = 0;
 static void expect(bool ok, const char* what, double v = 0) {
     std::printf("%-44s %s %.3e\n", what, ok ? "ok  " : "FAIL", v);
@@ -229,6 +219,135 @@ int main() {
         std::vector<cd> sq(n);
         for (std::size_t i = 0; i < n; ++i) sq[i] = za[i] * za[i];
         expect(rel_err(a, sq) < 2e-6, "expr a = a * a (in place)", rel_err(a, sq));
+    }
+    {    // tensor-core form (pcx_tc_fft_exec): forward in each precision, inverse round trip
+        const std::size_t n = 4096, batch = 4;
+        pcxo::fft_unit<float> unit(n);
+        std::vector<cd>       x(n * batch);
+        for (auto& v: x) v = cd(u(rng), u(rng));
+        std::vector<float> h(2 * n * batch);
+        for (std::size_t b = 0; b < batch; ++b) {
+            for (std::size_t i = 0; i < n; ++i) {
+                h[2 * n * b + pcxo::pidx<8>(i)]     = float(x[b * n + i].real());
+                h[2 * n * b + pcxo::pidx<8>(i) + 8] = float(x[b * n + i].imag());
+                x[b * n + i] = cd(h[2 * n * b + pcxo::pidx<8>(i)], h[2 * n * b + pcxo::pidx<8>(i) + 8]);
+            }
+        }
+        float *d_x = nullptr, *d_y = nullptr;
+        pcxo::detail_::check_cuda(cudaMalloc(&d_x, h.size() * sizeof(float)));
+        pcxo::detail_::check_cuda(cudaMalloc(&d_y, h.size() * sizeof(float)));
+        pcxo::detail_::check_cuda(cudaMemcpy(d_x, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+        using prec = pcxo::fft_unit<float>::tc_precision;
+        auto rel = [&](const float* dev, bool spectrum) {
+            std::vector<float> o(h.size());
+            pcxo::detail_::check_cuda(cudaMemcpy(o.data(), dev, o.size() * sizeof(float), cudaMemcpyDeviceToHost));
+            double worst = 0;
+            for (std::size_t b = 0; b < batch; ++b) {
+                std::vector<cd> in(x.begin() + b * n, x.begin() + (b + 1) * n), got(n);
+                for (std::size_t i = 0; i < n; ++i) {
+                    got[i] = cd(o[2 * n * b + pcxo::pidx<8>(i)], o[2 * n * b + pcxo::pidx<8>(i) + 8]);
+                }
+                worst = std::max(worst, rel_err(got, spectrum ? dft(in, -1) : in));
+            }
+            return worst;
+        };
+        unit.fft_batch_tensor_core(d_y, d_x, batch);
+        const double e6 = rel(d_y, true);
+        expect(e6 < 2e-6, "fft_batch_tensor_core bf16x6", e6);
+        unit.fft_batch_tensor_core(d_y, d_x, batch, prec::tf32x3);
+        const double et = rel(d_y, true);
+        expect(et < 2e-6, "fft_batch_tensor_core tf32x3", et);
+        unit.ifft_batch_tensor_core(d_x, d_y, batch, prec::tf32x3);
+        const double er = rel(d_x, false);
+        expect(er < 2e-6, "ifft_batch_tensor_core round trip", er);
+        cudaFree(d_x);
+        cudaFree(d_y);
+    }
+    {    // adjoints (no reference counterpart): fft_unit::vjp is the unnormalised inverse
+        const std::size_t n = 1024, batch = 3;
+        std::vector<cd>   gy(n * batch);
+        for (auto& v: gy) v = cd(u(rng), u(rng));
+        pcxo::fft_unit<double> unit(n);
+        const std::size_t      row = 2 * n;    // pack 4, no padding
+        double*                d_gy = nullptr;
+        double*                d_gx = nullptr;
+        pcxo::detail_::check_cuda(cudaMalloc(&d_gy, batch * row * sizeof(double)));
+        pcxo::detail_::check_cuda(cudaMalloc(&d_gx, batch * row * sizeof(double)));
+        std::vector<double> h(batch * row);
+        for (std::size_t b = 0; b < batch; ++b) {
+            for (std::size_t i = 0; i < n; ++i) {
+                h[b * row + pcxo::pidx<4>(i)]     = gy[b * n + i].real();
+                h[b * row + pcxo::pidx<4>(i) + 4] = gy[b * n + i].imag();
+            }
+        }
+        pcxo::detail_::check_cuda(cudaMemcpy(d_gy, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        double worst = 0;
+        for (int inverse = 0; inverse < 2; ++inverse) {
+            unit.vjp<true, 4>(d_gx, d_gy, batch, inverse != 0);
+            pcxo::detail_::check_cuda(cudaMemcpy(h.data(), d_gx, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (std::size_t b = 0; b < batch; ++b) {
+                std::vector<cd> in(gy.begin() + b * n, gy.begin() + (b + 1) * n), got(n);
+                // adjoint of the forward: F^H g; of the normalised inverse: F g / n
+                auto want = dft(in, inverse ? -1 : +1);
+                if (inverse) {
+                    for (auto& v: want) v /= double(n);
+                }
+                for (std::size_t i = 0; i < n; ++i) {
+                    got[i] = cd(h[b * row + pcxo::pidx<4>(i)], h[b * row + pcxo::pidx<4>(i) + 4]);
+                }
+                worst = std::max(worst, rel_err(got, want));
+            }
+        }
+        expect(worst < 1e-13, "fft_unit<double>::vjp (forward, inverse)", worst);
+        cudaFree(d_gy);
+        cudaFree(d_gx);
+    }
+    {    // fxcorr_unit::vjp: gx = convolution of gy with g, gg = correlation of gy with x
+        const std::size_t k = 100, s = 3000, nf = 512;
+        std::vector<cd>   gd(k), xd(s), gyd(s);
+        for (auto& v: gd) v = cd(u(rng), u(rng));
+        for (auto& v: xd) v = cd(u(rng), u(rng));
+        for (auto& v: gyd) v = cd(u(rng), u(rng));
+        pcxo::vector<float> g(k);
+        for (std::size_t i = 0; i < k; ++i) g[i] = std::complex<float>(gd[i]);
+        pcxo::fxcorr_unit<float> xc(g, nf);
+        pcxo::vector<float>      x(s), gyv(s), gx(s), gg(k);
+        for (std::size_t i = 0; i < s; ++i) {
+            x[i]   = std::complex<float>(xd[i]);
+            gyv[i] = std::complex<float>(gyd[i]);
+            xd[i]  = cd(std::complex<float>(x[i]));
+            gyd[i] = cd(std::complex<float>(gyv[i]));
+        }
+        for (std::size_t i = 0; i < k; ++i) gd[i] = cd(std::complex<float>(g[i]));
+        xc.vjp(gx.data(), gg.data(), gyv.data(), x.data(), s);
+        std::vector<cd> gx_want(s, 0.0), gg_want(k, 0.0);
+        for (std::size_t m = 0; m < s; ++m) {
+            for (std::size_t j = 0; j < k && m + j < s; ++j) {
+                gx_want[m + j] += gd[j] * gyd[m];
+                gg_want[j] += xd[m + j] * std::conj(gyd[m]);
+            }
+        }
+        expect(rel_err(gx, gx_want) < 2e-6, "fxcorr_unit::vjp gx (convolution)", rel_err(gx, gx_want));
+        expect(rel_err(gg, gg_want) < 2e-6, "fxcorr_unit::vjp gg (correlation)", rel_err(gg, gg_want));
+    }
+    {    // a bounded device wait that gives up becomes an exception through the drop-in
+        pcxo::fft_unit<float> unit(1024);
+        pcxo::vector<float>   v(1024);
+        pcxo::detail_::check(pcx_selftest_plan_wait(unit.plan(), 1000000ull, nullptr));
+        bool thrown = false;
+        try {
+            unit(v);
+        } catch (const std::runtime_error& e) {
+            thrown = std::string(e.what()).find("gave up") != std::string::npos;
+        }
+        expect(thrown, "given-up device wait -> std::runtime_error");
+        bool again = true;
+        try {
+            unit(v);    // the flag was read and cleared: the next call runs normally
+        } catch (const std::exception&) {
+            again = false;
+        }
+        expect(again, "next call after a give-up succeeds");
     }
     {    // exceptions keep the reference's types and messages
         bool thrown = false;

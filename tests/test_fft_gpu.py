@@ -223,6 +223,37 @@ def test_vjp_adjoint_identity(log_n):
             assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
+@pytest.mark.parametrize("log_n", [10, 16])
+def test_vjp_vs_central_fd(log_n):
+    """pcx_fft_vjp (FP64 plan) against FP64 central finite differences of
+    L = sum w |Y|^2, Y = the plan's forward, normalised inverse or unnormalised
+    inverse of x, w ~ U[0,1): 32 coordinates, real and imaginary directions,
+    |fd - grad| <= 1e-6 * max(1, |fd|).  Y is linear in x, so the perturbed
+    outputs are Y +- h*dY with dY the transform of the unit step, and the
+    difference is summed term by term.  L is quadratic, so the central
+    difference has no truncation error at any step; h = 1e-3 keeps its
+    rounding noise near 1e-9 (at h = 1e-6 forming Y +- h*dY from |Y| ~ sqrt(n)
+    leaves up to ~2e-6 on coordinates whose gradient is small)."""
+    n, batch, h = 1 << log_n, 2, 1e-3
+    rng = np.random.default_rng(log_n + 100)
+    z = normal_cx(rng, batch, n)
+    w = rng.uniform(0, 1, (batch, n))
+    unit = fft_unit(n, dtype=F64)
+    k = np.arange(n)
+    for direction, norm in ((0, True), (1, True), (1, False)):
+        scale = 1.0 / n if (direction == 1 and norm) else 1.0
+        Y = (np.fft.fft(z, axis=-1) if direction == 0 else np.fft.ifft(z, axis=-1) * n) * scale
+        gy = to_dev(O.pack(2 * w * Y, 4, np.float64), F64)    # dL/dRe Y + i dL/dIm Y
+        gx = O.unpack(unit.vjp(gy, direction=direction, normalize=norm, batch=batch).cpu().numpy(), n, 4)
+        sign = -1.0 if direction == 0 else 1.0
+        for b, i in zip(rng.integers(0, batch, 32), rng.integers(0, n, 32)):
+            col = np.exp(sign * 2j * np.pi * ((i * k) % n) / n) * scale    # transform of e_i
+            for u, an in ((1.0, gx[b, i].real), (1j, gx[b, i].imag)):
+                dy = u * col
+                fd = float(np.sum(w[b] * (np.abs(Y[b] + h * dy) ** 2 - np.abs(Y[b] - h * dy) ** 2)) / (2 * h))
+                assert abs(fd - an) <= 1e-6 * max(1.0, abs(fd)), (direction, norm, fd, an)
+
+
 @pytest.mark.slow
 @pytest.mark.parametrize("log_n", [6, 10, 12, 13, 16, 18, 20])
 def test_full_size_roundtrip_and_parseval(log_n):

@@ -117,10 +117,9 @@ def test_c3_full_size_sampled():
         zc = O.unpack(xo[c].cpu().numpy(), s, 8)
         yc = O.unpack(y[c].cpu().numpy(), s, 8)
         idx = np.concatenate([rng.integers(0, s, 60), [0, 12287, 12288, s - 1]])
-        for i in idx:
-            seg = zc[i:i + k]
-            want = np.sum(seg * np.conj(gd[: len(seg)]))
-            assert abs(yc[i] - want) <= 2e-5 * (np.sqrt(k) / 64 * 1.5 + abs(want))
+        want = np.array([np.sum(zc[i:i + k] * np.conj(gd[: len(zc[i:i + k])])) for i in idx])
+        # the sampled outputs, as a vector, meet the FP32 bar
+        assert rel_l2(yc[idx], want) < TOL[np.float32]
 
 
 def test_vjp_against_oracle():
@@ -140,55 +139,100 @@ def test_vjp_against_oracle():
     assert rel_l2(gg, gg_want) < TOL[np.float32]
 
 
-def test_autograd_c3_gradients_vs_fd():
-    # loss = sum w |y|^2, w ~ U[0,1) seed 6; C3 kernel shape (K=4096, N=16384)
-    # on 1 channel of 2^16; gradients at 64 random coordinates vs FP64 central
-    # finite differences (h = 1e-6) of the FP64 direct loss.
-    rng = np.random.default_rng(2)
-    s, k, n = 1 << 16, 4096, 16384
-    z = normal_cx(rng, s)
-    g = normal_cx(rng, k, sigma=1 / 64)
+def _c3_like_problem(dtype, s=1 << 16, k=4096):
+    """One channel with C3's kernel shape and distributions: signal N(0,1)
+    (seed 2), kernel N(0,1/4096) (seed 3), loss weight U[0,1) (seed 6)."""
+    z = normal_cx(np.random.default_rng(2), s)
+    g = normal_cx(np.random.default_rng(3), k, sigma=1 / 64)
     w = np.random.default_rng(6).uniform(0, 1, s)
-    x = dev(O.pack(z, 8)).requires_grad_(True)
-    gt = dev(O.pack(g, 8)).requires_grad_(True)
+    if dtype == F32:    # the FP64 side sees exactly the FP32 inputs
+        z, g = z.astype(np.complex64).astype(complex), g.astype(np.complex64).astype(complex)
+    return z, g, w
+
+
+def _autograd_grads(z, g, w, n, dtype):
+    """d(sum w |y|^2)/dx and /dg through FxcorrFunction (pcx_fxcorr_vjp)."""
+    s, k = z.size, g.size
+    p = 8 if dtype == F32 else 4
+    npd = np.float32 if dtype == F32 else np.float64
+    x = dev(O.pack(z, p, npd), dtype).requires_grad_(True)
+    gt = dev(O.pack(g, p, npd), dtype).requires_grad_(True)
     y = FxcorrFunction.apply(x, gt, n, s, k, 1)
-    wt = dev(O.pack(w.astype(complex), 8))
+    wt = dev(O.pack(w.astype(complex), p, npd), dtype)
     wr = wt.clone()
-    wr.view(-1, 2, 8)[:, 1, :] = wt.view(-1, 2, 8)[:, 0, :]    # weight both re and im
-    loss = (wr * y * y).sum()
-    loss.backward()
-    gx = O.unpack(x.grad.cpu().numpy(), s, 8)
-    gg = O.unpack(gt.grad.cpu().numpy(), k, 8)
-    yd = O.xcorr_ols(z, g, n)
+    wr.view(-1, 2, p)[:, 1, :] = wt.view(-1, 2, p)[:, 0, :]    # weight both re and im
+    (wr * y * y).sum().backward()
+    return O.unpack(x.grad.cpu().numpy(), s, p), O.unpack(gt.grad.cpu().numpy(), k, p)
 
-    def local_loss_x(zz, i):
-        lo, hi = max(0, i - k + 1), i + 1
-        seg = zz[lo: min(s, hi + k - 1)]
-        yy = np.array([np.sum(seg[m - lo: m - lo + k] * np.conj(g[: len(seg[m - lo: m - lo + k])]))
-                       for m in range(lo, hi)])
-        return float(np.sum(w[lo:hi] * np.abs(yy) ** 2))
 
-    h = 1e-6
-    for i in rng.integers(0, s, 32):
-        for unit_dir, part in ((1.0, "re"), (1j, "im")):
-            zp, zm = z.copy(), z.copy()
-            zp[i] += h * unit_dir
-            zm[i] -= h * unit_dir
-            fd = (local_loss_x(zp, i) - local_loss_x(zm, i)) / (2 * h)
-            an = gx[i].real if part == "re" else gx[i].imag
-            assert abs(fd - an) <= 1e-6 * max(1.0, abs(fd)) + 2e-5 * abs(fd)
-    # kernel coordinates: FD of the full FP64 loss (overlap-save in FP64)
-    for j in rng.integers(0, k, 32):
-        for unit_dir, part in ((1.0, "re"), (1j, "im")):
-            gp, gm = g.copy(), g.copy()
-            gp[j] += h * unit_dir
-            gm[j] -= h * unit_dir
-            lp = float(np.sum(w * np.abs(O.xcorr_ols(z, gp, n)) ** 2))
-            lm = float(np.sum(w * np.abs(O.xcorr_ols(z, gm, n)) ** 2))
-            fd = (lp - lm) / (2 * h)
-            an = gg[j].real if part == "re" else gg[j].imag
-            assert abs(fd - an) <= 1e-6 * max(1.0, abs(fd)) + 2e-5 * abs(fd)
-    assert np.isfinite(yd).all()
+def _central_fd(z, g, w, n, coords_x, coords_g, h=1e-6):
+    """FP64 central finite differences (step h) of L = sum w |y|^2, y the
+    correlation of z with g, at the given signal and kernel coordinates, in
+    the real and the imaginary direction.  y is linear in z and in conj(g), so
+    the perturbed outputs are formed exactly as y +- h*dy (dy the outputs'
+    change per unit step, from the definition y[m] = sum_j z[m+j] conj(g[j])),
+    and L(+h) - L(-h) is summed term by term over the affected outputs: the
+    difference quotient then carries ~1e-9 of rounding noise instead of the
+    ~1e-6 that subtracting two separately summed losses of ~3e4 would."""
+    s, k = z.size, g.size
+    y = O.xcorr_ols(z, g, n)
+
+    def fd(lo, dy):
+        yy, ww = y[lo:lo + dy.size], w[lo:lo + dy.size]
+        return float(np.sum(ww * (np.abs(yy + h * dy) ** 2 - np.abs(yy - h * dy) ** 2)) / (2 * h))
+
+    out_x, out_g = [], []
+    for i in coords_x:
+        lo = max(0, i - k + 1)
+        m = np.arange(lo, i + 1)
+        for u in (1.0, 1j):
+            out_x.append(fd(lo, u * np.conj(g[i - m])))
+    for j in coords_g:
+        m = np.arange(0, s - j)
+        for u in (1.0, 1j):
+            out_g.append(fd(0, z[m + j] * np.conj(u)))
+    return np.array(out_x), np.array(out_g)
+
+
+def _parts(v, coords):
+    return np.array([c for i in coords for c in (v[i].real, v[i].imag)])
+
+
+def test_adjoint_fp64_vs_central_fd():
+    """FP64 correlator (K = 4096, N_fft = 8192: the largest FP64 correlator
+    size) against FP64 central finite differences at 64 signal and 64 kernel
+    coordinates: |fd - grad| <= 1e-6 * max(1, |fd|), nothing added."""
+    n = 8192
+    z, g, w = _c3_like_problem(F64)
+    gx, gg = _autograd_grads(z, g, w, n, F64)
+    rng = np.random.default_rng(64)
+    cx, cg = rng.integers(0, z.size, 64), rng.integers(0, g.size, 64)
+    fdx, fdg = _central_fd(z, g, w, n, cx, cg)
+    for fd, an in ((fdx, _parts(gx, cx)), (fdg, _parts(gg, cg))):
+        assert np.all(np.abs(fd - an) <= 1e-6 * np.maximum(1.0, np.abs(fd))), np.max(np.abs(fd - an))
+    # and the whole gradients against the FP64 reference gradient (direct sums)
+    yd = O.xcorr_direct(z, g)
+    gxw, ggw = O.xcorr_vjp_direct(z, g, 2 * w * yd)
+    assert rel_l2(gx, gxw) < 1e-12 and rel_l2(gg, ggw) < 1e-12
+
+
+def test_adjoint_fp32_c3_vs_central_fd():
+    """FP32 correlator at C3's shape (K = 4096, N_fft = 16384) against the same
+    FP64 central differences.  An FP32 gradient carries the FP32 parity error
+    (relative L2 <= 2e-6 of the gradient vector), so each coordinate is held to
+    |fd - grad| <= 2e-5 * rms(grad): ten times the vector bar, per coordinate."""
+    n = 16384
+    z, g, w = _c3_like_problem(F32)
+    gx, gg = _autograd_grads(z, g, w, n, F32)
+    rng = np.random.default_rng(64)
+    cx, cg = rng.integers(0, z.size, 64), rng.integers(0, g.size, 64)
+    fdx, fdg = _central_fd(z, g, w, n, cx, cg)
+    for fd, full, an in ((fdx, gx, _parts(gx, cx)), (fdg, gg, _parts(gg, cg))):
+        rms = np.sqrt(np.mean(np.abs(full) ** 2))
+        assert np.all(np.abs(fd - an) <= 2e-5 * rms), np.max(np.abs(fd - an)) / rms
+    yd = O.xcorr_direct(z, g)
+    gxw, ggw = O.xcorr_vjp_direct(z, g, 2 * w * yd)
+    assert rel_l2(gx, gxw) < TOL[np.float32] and rel_l2(gg, ggw) < TOL[np.float32]
 
 
 def test_errors():

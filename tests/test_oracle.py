@@ -68,6 +68,21 @@ def test_unordered_permutation_is_the_references():
         assert rel_l2(ref[pos], nat) < REF_TOL
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref (the reference compiled here) not built")
+@pytest.mark.parametrize("sub", [64, 128, 512, 4096])
+@pytest.mark.parametrize("order", [1, 2])
+def test_order_permutation_does_not_depend_on_sub_size(order, sub):
+    # The reference's unordered (and bit_reversed) output order, run through
+    # the reference itself at several sub_size values: position p holds
+    # frequency bitrev(sigma(p)) (bitrev(p)) whatever the sub_size, which is
+    # what order_pos implements and the GPU kernels use.
+    rng = np.random.default_rng(sub + order)
+    for n in (64, 256, 1024, 4096, 16384, 32768):
+        z = normal_cx(rng, n)
+        got = O.unpack(O.ref_fft(O.pack(z, 8), n, order, 0, True, sub), n, 8)
+        assert rel_l2(got[O.order_pos(n, order)], np.fft.fft(z)) < REF_TOL
+
+
 @pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 128])
 def test_oracle_fft_matches_direct_dft(n):
     rng = np.random.default_rng(n)
