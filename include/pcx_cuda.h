@@ -105,18 +105,66 @@ size_t pcx_plan_workspace_size(pcx_plan plan, size_t batch);
 
 /*
  * Autotuner (no reference counterpart: the reference picks its radix
- * schedule at compile time).  Times the forms this plan supports, and their
- * tile-schedule / chunk-size variants, on `batch` rows of scratch data
- * (forward, natural order, default pack; at most 512 MB per buffer) on
- * `stream`, and makes the fastest the plan's form for later execs that use
- * the plan's own scratch (pcx_fft_exec).  Allocates and frees its buffers;
- * synchronises.  *form_out (if not NULL) receives the PCX_FORM_* chosen.
- * A plan for n <= 4096 has one form: PCX_FORM_DEFAULT, nothing is timed.
+ * schedule at compile time, fft.hpp:546-575, 1856-1958).  Times the forms
+ * this plan supports on `batch` rows of scratch data (forward, natural order,
+ * default pack; at most 512 MB per buffer) on `stream`: the one-pass form
+ * (FP32 n = 8192), every built-in variant of the one-launch four-step for this
+ * size (split N1 x N2, i.e. the radix schedule of both passes; tile shape as
+ * blocks per SM; ring stages) at three dependency distances, and the chunked
+ * four-step at two scratch sizes; it makes the fastest the plan's form for
+ * later execs that use the plan's own scratch (pcx_fft_exec).  Allocates and
+ * frees its buffers; synchronises.  *form_out (if not NULL) receives the
+ * PCX_FORM_* chosen; pcx_plan_tuning gives the details.  With PCX_TUNE_CACHE
+ * set, a cached result for this GPU, size, type and batch is applied without
+ * timing (see the tuning cache below).  PCX_TUNE_VERBOSE=1 prints each
+ * candidate's time to stderr.  A plan for n <= 4096 has one form:
+ * PCX_FORM_DEFAULT, nothing is timed.
  */
 int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* form_out);
 /* The plan's current form (PCX_FORM_*), the one-launch four-step's dependency
  * distance in rounds of tiles, and the chunked form's scratch bytes per buffer. */
 int pcx_plan_form(pcx_plan plan, int* form, int* rounds, size_t* chunk_bytes);
+
+/*
+ * What pcx_plan_tune chose (no reference counterpart; the reference's knobs
+ * SubSize / NodeSizeRec / Strategy, fft.hpp:546-575, and its cost model
+ * get_subtform_idx_strategic_, fft.hpp:1856-1958, fix its schedule at compile
+ * time).  For the one-launch four-step: the split N = 2^log_n1 * 2^log_n2
+ * (the radix schedule of the two sub-transforms follows from it), the tile
+ * shape as resident blocks per SM (64 KB / blocks_per_sm per tile), the ring
+ * stages and the dependency distance in rounds of tiles.
+ */
+typedef struct {
+    int    form;          /* PCX_FORM_* */
+    int    rounds;        /* one-launch four-step: tile distance in rounds of tiles */
+    size_t chunk_bytes;   /* chunked four-step: scratch bytes per buffer */
+    int    log_n1;        /* one-launch four-step: split */
+    int    log_n2;
+    int    blocks_per_sm; /* one-launch four-step: resident blocks per SM (tile shape) */
+    int    stages;        /* one-launch four-step: ring stages */
+    double ms;            /* device time of one timed transform batch when tuned (0: not timed) */
+} pcx_tune_result;
+int pcx_plan_tuning(pcx_plan plan, pcx_tune_result* out);
+/* Make `r` the plan's form without timing (a result from pcx_plan_tuning or
+ * the cache); PCX_ERR_UNSUPPORTED if it names a variant not built for the
+ * plan's size.  r->ms is ignored. */
+int pcx_plan_set_tuning(pcx_plan plan, const pcx_tune_result* r);
+
+/*
+ * Tuning cache (no reference counterpart): results of pcx_plan_tune keyed by
+ * GPU name, size, element type and batch (rounded down to a power of two),
+ * kept in memory and saved to / merged from a JSON file.  When the
+ * environment variable PCX_TUNE_CACHE names a file, pcx_plan_tune loads it
+ * once, uses a matching entry instead of timing, and saves new results to it.
+ * Host code only: none of these calls touches the GPU.
+ */
+int    pcx_tune_cache_load(const char* path);
+int    pcx_tune_cache_save(const char* path);
+int    pcx_tune_cache_put(const char* gpu, size_t n, int dtype, size_t batch, const pcx_tune_result* r);
+/* PCX_ERR_INVALID when there is no entry. */
+int    pcx_tune_cache_get(const char* gpu, size_t n, int dtype, size_t batch, pcx_tune_result* r);
+int    pcx_tune_cache_clear(void);
+size_t pcx_tune_cache_size(void);
 
 /*
  * Batched transform of `batch` rows.  Replaces

@@ -36,6 +36,14 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_plan_workspace_size": (_sz, [_vp, _sz]),
     "pcx_plan_tune": (_i, [_vp, _sz, _vp, ctypes.POINTER(_i)]),
     "pcx_plan_form": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_sz)]),
+    "pcx_plan_tuning": (_i, [_vp, _vp]),
+    "pcx_plan_set_tuning": (_i, [_vp, _vp]),
+    "pcx_tune_cache_load": (_i, [ctypes.c_char_p]),
+    "pcx_tune_cache_save": (_i, [ctypes.c_char_p]),
+    "pcx_tune_cache_put": (_i, [ctypes.c_char_p, _sz, _i, _sz, _vp]),
+    "pcx_tune_cache_get": (_i, [ctypes.c_char_p, _sz, _i, _sz, _vp]),
+    "pcx_tune_cache_clear": (_i, []),
+    "pcx_tune_cache_size": (_sz, []),
     "pcx_fft_par_exec": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _sz, _sz, _i, _i, _i, _i, _vp]),
     "pcx_vec_eval": (_i, [_i, _vp, _i, _sz, _vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i), _i, _vp]),
     "pcx_fft_exec": (_i, [_vp, _vp, _vp, _sz, _i, _i, _i, _i, _sz, _sz, _sz, _vp]),
@@ -56,6 +64,12 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_ragged_items": (_sz, [_vp]),
     "pcx_ragged_destroy": (_i, [_vp]),
 }
+
+class TuneResult(ctypes.Structure):
+    """pcx_tune_result (include/pcx_cuda.h)."""
+    _fields_ = [("form", _i), ("rounds", _i), ("chunk_bytes", _sz), ("log_n1", _i), ("log_n2", _i),
+                ("blocks_per_sm", _i), ("stages", _i), ("ms", ctypes.c_double)]
+
 
 _lib: ctypes.CDLL | None = None
 

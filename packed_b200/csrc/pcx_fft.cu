@@ -7,8 +7,10 @@
 #include "pcx_host.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include <string>
 
@@ -168,6 +170,61 @@ size_t pcx_plan_s::chunk_rows(size_t batch) const {
     return std::min(c, std::max<size_t>(batch, 1));
 }
 
+// Make `v` the plan's one-launch four-step variant: its split's tables (W_N
+// tables, W_{16 N2}, full stage tables), generated again only when the split
+// changes, and its tile counts and resident blocks per SM.
+static int fs_select(pcx_plan_s* p, const fs_variant& v) {
+    const bool f64 = p->dtype == PCX_F64;
+    if (v.l1 + v.l2 != p->log_n) return pcx_fail(PCX_ERR_INVALID, "four-step variant of another size");
+    int tc = 0, tr = 0, per_sm = 0;
+    const cudaError_t ea = pcx_fourstep(f64, v, fs_args{}, 0, p->sms, true, &tc, &tr, &per_sm);
+    if (ea != cudaSuccess) {
+        cudaGetLastError();
+        return pcx_fail(ea == cudaErrorNotSupported ? PCX_ERR_UNSUPPORTED : PCX_ERR_CUDA,
+                        std::string("four-step variant: ") + cudaGetErrorString(ea));
+    }
+    if (p->fs_tab_l1 != v.l1 || !p->fs_mem) {
+        const size_t eb = p->elem_bytes();
+        const int    n1 = 1 << v.l1, n2 = 1 << v.l2;
+        int          f1 = 0, f2 = 0;
+        PCX_CUDA_TRY(pcx_fourstep_tables(v.l1, nullptr, f64, 0, &f1));
+        PCX_CUDA_TRY(pcx_fourstep_tables(v.l2, nullptr, f64, 0, &f2));
+        if (p->fs_mem) cudaFree(p->fs_mem);
+        p->fs_mem    = nullptr;
+        p->fs_tab_l1 = 0;
+        const size_t ent = (size_t)n1 + 2 * (size_t)n2 + f1 + f2;
+        PCX_CUDA_TRY(cudaMalloc(&p->fs_mem, ent * eb));
+        char* b    = static_cast<char*>(p->fs_mem);
+        p->fs_thi  = b;
+        p->fs_tlo  = b + (size_t)n1 * eb;
+        p->fs_tb   = b + ((size_t)n1 + n2) * eb;
+        p->fs_st1  = b + ((size_t)n1 + 2 * n2) * eb;
+        p->fs_st2  = b + ((size_t)n1 + 2 * n2 + f1) * eb;
+        PCX_CUDA_TRY(pcx_gen_twiddles(p->fs_thi, n1, p->log_n, n2, f64, 0));
+        PCX_CUDA_TRY(pcx_gen_twiddles(p->fs_tlo, n2, p->log_n, 1, f64, 0));
+        PCX_CUDA_TRY(pcx_gen_twiddles(p->fs_tb, n2, v.l2 + 4, 1, f64, 0));
+        PCX_CUDA_TRY(pcx_fourstep_tables(v.l1, p->fs_st1, f64, 0, &f1));
+        PCX_CUDA_TRY(pcx_fourstep_tables(v.l2, p->fs_st2, f64, 0, &f2));
+        p->fs_tab_l1 = v.l1;
+    }
+    p->fs_var    = v;
+    p->fs_tc     = tc;
+    p->fs_tr     = tr;
+    p->fs_per_sm = per_sm;
+    return PCX_OK;
+}
+
+// The built-in variants of the one-launch four-step for this plan's size.
+static std::vector<fs_variant> fs_candidates(const pcx_plan_s* p) {
+    std::vector<fs_variant> out;
+    if (p->dtype == PCX_F64) {
+        for (const auto& v: kFsVariantsF64) if (v.l1 + v.l2 == p->log_n) out.push_back(v);
+    } else {
+        for (const auto& v: kFsVariantsF32) if (v.l1 + v.l2 == p->log_n) out.push_back(v);
+    }
+    return out;
+}
+
 static int plan_init_tables(pcx_plan_s* p) {
     const int  log_n = p->log_n;
     const bool f64   = p->dtype == PCX_F64;
@@ -249,11 +306,21 @@ static int plan_init_tables(pcx_plan_s* p) {
             }
             PCX_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
             // one launch for all chunks of a batch
-            if (pcx_fourstep(f64, p->log_n1, p->log_n2, fs_args{}, 0, p->sms, true, &p->fs_tc, &p->fs_tr,
-                             &p->fs_per_sm) != cudaSuccess) {
-                cudaGetLastError();
+            // one launch for a whole batch: the size's first built-in variant
+            p->fs_tc = p->fs_tr = 0;
+            for (const fs_variant& v: fs_candidates(p)) {
+                if (fs_select(p, v) == PCX_OK) break;
                 p->fs_tc = p->fs_tr = 0;
             }
+            // full stage tables of the two sub-transforms (the TMA-fed passes)
+            int f1 = 0, f2 = 0;
+            PCX_CUDA_TRY(pcx_fourstep_tables(p->log_n1, nullptr, f64, 0, &f1));
+            PCX_CUDA_TRY(pcx_fourstep_tables(p->log_n2, nullptr, f64, 0, &f2));
+            PCX_CUDA_TRY(cudaMalloc(&p->fst, ((size_t)f1 + f2) * eb));
+            p->fst1 = p->fst;
+            p->fst2 = static_cast<char*>(p->fst) + (size_t)f1 * eb;
+            PCX_CUDA_TRY(pcx_fourstep_tables(p->log_n1, p->fst1, f64, 0, &f1));
+            PCX_CUDA_TRY(pcx_fourstep_tables(p->log_n2, p->fst2, f64, 0, &f2));
             // N = 8192 in FP32 also has a one-pass form (64 KB rows in shared memory)
             v3_args z3{};
             if (pcx_v3_single(f64, log_n, z3, 0, p->sms, true) == cudaSuccess) {
@@ -320,6 +387,10 @@ void pcx_plan_s::release() {
     if (tw) cudaFree(tw);
     if (stw) cudaFree(stw);
     if (stw_one) cudaFree(stw_one);
+    if (fst) cudaFree(fst);
+    if (fs_mem) cudaFree(fs_mem);
+    fs_mem    = nullptr;
+    fs_tab_l1 = 0;
     if (fs_ctr) cudaFree(fs_ctr);
     if (par_buf) cudaFree(par_buf);
     par_buf   = nullptr;
@@ -336,6 +407,9 @@ void pcx_plan_s::release() {
     tw      = nullptr;
     stw     = nullptr;
     stw_one  = nullptr;
+    fst      = nullptr;
+    fst1     = nullptr;
+    fst2     = nullptr;
     fs_ctr   = nullptr;
     fs_ctr_n = 0;
     scratch  = nullptr;
@@ -366,25 +440,82 @@ extern "C" int pcx_plan_status(pcx_plan plan) {
     });
 }
 
+namespace {
+// Name of the current device, the tuning cache's GPU key.
+std::string gpu_name() {
+    int            dev = 0;
+    cudaDeviceProp pr{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    return pr.name;
+}
+
+// The plan's current choice as a cache / report record.
+pcx_tune_result plan_choice(const pcx_plan_s* p, double ms) {
+    pcx_tune_result r{};
+    r.form          = p->form;
+    r.rounds        = p->fs_rounds;
+    r.chunk_bytes   = p->chunk_bytes;
+    r.log_n1        = p->fs_var.l1;
+    r.log_n2        = p->fs_var.l2;
+    r.blocks_per_sm = p->fs_var.minb;
+    r.stages        = p->fs_var.st;
+    r.ms            = ms;
+    return r;
+}
+
+// Apply a tuning record to the plan; false if it names a variant not built here.
+bool apply_choice(pcx_plan_s* p, const pcx_tune_result& r) {
+    if (r.form == PCX_FORM_FUSED || (r.form == PCX_FORM_DEFAULT && r.log_n1 > 0)) {
+        const fs_variant v{r.log_n1, r.log_n2, r.blocks_per_sm, r.stages};
+        if (fs_select(p, v) != PCX_OK) return false;
+    }
+    if (r.form == PCX_FORM_ONEPASS && !p->stw_one) return false;
+    p->form        = r.form;
+    p->fs_rounds   = r.rounds > 0 ? r.rounds : 3;
+    p->chunk_bytes = r.chunk_bytes;
+    return true;
+}
+
+std::once_flag g_cache_once;
+}    // namespace
+
 extern "C" int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* form_out) {
     return pcx_guard([&]() -> int {
         if (!plan) return pcx_fail(PCX_ERR_INVALID, "plan is null");
         pcx_plan_s* p = plan;
         if (form_out) *form_out = p->form;
         if (!p->two_pass || batch == 0) return PCX_OK;
+        const size_t eb    = p->elem_bytes();
+        const size_t rows  = std::max<size_t>(1, std::min(batch, ((size_t)512 << 20) / (p->n * eb)));
+        const char*  cpath = std::getenv("PCX_TUNE_CACHE");
+        const bool   verbose = std::getenv("PCX_TUNE_VERBOSE") != nullptr;
+        const std::string gpu = gpu_name();
+        if (cpath && *cpath) {
+            // a missing or unreadable file just means nothing is cached yet
+            std::call_once(g_cache_once, [&]() { (void)pcx_tune_cache_load(cpath); });
+            pcx_tune_result hit{};
+            if (pcx_tune_cache_get(gpu.c_str(), p->n, p->dtype, rows, &hit) == PCX_OK && apply_choice(p, hit)) {
+                if (form_out) *form_out = p->form;
+                return PCX_OK;
+            }
+        }
         struct cand {
-            int    form;
-            int    rounds;
-            size_t chunk;
+            int        form;
+            int        rounds;
+            size_t     chunk;
+            fs_variant v;
         };
         std::vector<cand> cands;
-        if (p->stw_one) cands.push_back({PCX_FORM_ONEPASS, 3, 0});
+        if (p->stw_one) cands.push_back({PCX_FORM_ONEPASS, 3, 0, {}});
         if (p->fs_tc > 0) {
-            for (int r: {2, 3, 6}) cands.push_back({PCX_FORM_FUSED, r, 0});
+            for (const fs_variant& v: fs_candidates(p)) {
+                for (int r: {2, 3, 6}) cands.push_back({PCX_FORM_FUSED, r, 0, v});
+            }
         }
-        for (size_t mb: {24, 48}) cands.push_back({PCX_FORM_CHUNKED, 3, mb << 20});
-        const size_t eb   = p->elem_bytes();
-        const size_t rows = std::max<size_t>(1, std::min(batch, ((size_t)512 << 20) / (p->n * eb)));
+        for (size_t mb: {24, 48}) cands.push_back({PCX_FORM_CHUNKED, 3, mb << 20, {}});
         const size_t bytes = rows * p->n * eb;
         cudaStream_t st    = static_cast<cudaStream_t>(stream);
         void *       x = nullptr, *y = nullptr;
@@ -395,8 +526,14 @@ extern "C" int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* for
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
         };
-        const int   keep_form = p->form, keep_rounds = p->fs_rounds;
-        const size_t keep_chunk = p->chunk_bytes;
+        const pcx_tune_result keep = plan_choice(p, 0.0);
+        const fs_variant      keep_var = p->fs_var;
+        auto restore = [&]() {
+            if (keep_var.l1 > 0) fs_select(p, keep_var);
+            p->form        = keep.form;
+            p->fs_rounds   = keep.rounds;
+            p->chunk_bytes = keep.chunk_bytes;
+        };
         cudaError_t e = cudaMalloc(&x, bytes);
         if (e == cudaSuccess) e = cudaMalloc(&y, bytes);
         if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, bytes, st);
@@ -406,44 +543,86 @@ extern "C" int pcx_plan_tune(pcx_plan plan, size_t batch, void* stream, int* for
             cleanup();
             return pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e));
         }
-        const size_t row = 2 * p->n;
+        const size_t row    = 2 * p->n;
+        const int    pk     = p->dtype == PCX_F64 ? 4 : 8;
         float        best_ms = 0.f;
-        cand         best    = {keep_form, keep_rounds, keep_chunk};
+        cand         best{keep.form, keep.rounds, keep.chunk_bytes, keep_var};
         for (const cand& c: cands) {
+            if (c.form == PCX_FORM_FUSED && !(c.v == p->fs_var) && fs_select(p, c.v) != PCX_OK) continue;
             p->form        = c.form;
             p->fs_rounds   = c.rounds;
             p->chunk_bytes = c.chunk;
             int rc = PCX_OK;
             for (int w = 0; w < 2 && rc == PCX_OK; ++w) {
-                rc = pcx_fft_run(p, y, x, p->n, p->dtype == PCX_F64 ? 4 : 8, p->dtype == PCX_F64 ? 4 : 8,
-                                 PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
+                rc = pcx_fft_run(p, y, x, p->n, pk, pk, PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
             }
             if (rc == PCX_OK) e = cudaEventRecord(e0, st);
             for (int it = 0; it < 3 && rc == PCX_OK && e == cudaSuccess; ++it) {
-                rc = pcx_fft_run(p, y, x, p->n, p->dtype == PCX_F64 ? 4 : 8, p->dtype == PCX_F64 ? 4 : 8,
-                                 PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
+                rc = pcx_fft_run(p, y, x, p->n, pk, pk, PCX_FORWARD, 0, rows, row, row, nullptr, 0, st, 1.0);
             }
             if (rc == PCX_OK && e == cudaSuccess) e = cudaEventRecord(e1, st);
             if (rc == PCX_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
             float ms = 0.f;
             if (rc == PCX_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
             if (rc != PCX_OK || e != cudaSuccess) {
-                p->form        = keep_form;
-                p->fs_rounds   = keep_rounds;
-                p->chunk_bytes = keep_chunk;
+                restore();
                 cleanup();
                 return rc != PCX_OK ? rc : pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e));
+            }
+            ms /= 3.f;
+            if (verbose) {
+                std::fprintf(stderr, "pcx_plan_tune n=%zu rows=%zu form=%d split=%dx%d blocks/SM=%d stages=%d rounds=%d "
+                             "chunk=%zuMB: %.4f ms\n", p->n, rows, c.form, 1 << c.v.l1, 1 << c.v.l2, c.v.minb, c.v.st,
+                             c.rounds, c.chunk >> 20, ms);
             }
             if (best_ms == 0.f || ms < best_ms) {
                 best_ms = ms;
                 best    = c;
             }
         }
+        if (best.form == PCX_FORM_FUSED || (best.form == PCX_FORM_DEFAULT && best.v.l1 > 0)) {
+            if (int rc = fs_select(p, best.v)) {
+                restore();
+                cleanup();
+                return rc;
+            }
+        } else if (keep_var.l1 > 0 && !(p->fs_var == keep_var)) {
+            fs_select(p, keep_var);
+        }
         p->form        = best.form;
         p->fs_rounds   = best.rounds;
         p->chunk_bytes = best.chunk;
         cleanup();
+        if (cpath && *cpath) {
+            const pcx_tune_result r = plan_choice(p, best_ms);
+            pcx_tune_cache_put(gpu.c_str(), p->n, p->dtype, rows, &r);
+            pcx_tune_cache_save(cpath);
+        }
         if (form_out) *form_out = p->form;
+        return PCX_OK;
+    });
+}
+
+extern "C" int pcx_plan_set_tuning(pcx_plan plan, const pcx_tune_result* r) {
+    return pcx_guard([&]() -> int {
+        if (!plan || !r) return pcx_fail(PCX_ERR_INVALID, "null argument");
+        if (!plan->two_pass) {
+            if (r->form != PCX_FORM_DEFAULT) return pcx_fail(PCX_ERR_UNSUPPORTED, "sizes up to 4096 have one form");
+            return PCX_OK;
+        }
+        if (r->form < PCX_FORM_DEFAULT || r->form > PCX_FORM_CHUNKED) return pcx_fail(PCX_ERR_INVALID, "unknown form");
+        if (!apply_choice(plan, *r)) {
+            return pcx_fail(PCX_ERR_UNSUPPORTED, "this form or four-step variant is not built for the plan's size");
+        }
+        return PCX_OK;
+    });
+}
+
+extern "C" int pcx_plan_tuning(pcx_plan plan, pcx_tune_result* out) {
+    return pcx_guard([&]() -> int {
+        if (!plan || !out) return pcx_fail(PCX_ERR_INVALID, "null argument");
+        *out = plan_choice(plan, 0.0);
+        if (out->chunk_bytes == 0) out->chunk_bytes = (size_t)24 << 20;
         return PCX_OK;
     });
 }
@@ -725,7 +904,11 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         const long long ctas   = (long long)p->sms * std::max(1, p->fs_per_sm);
         long long       lag    = (rounds * ctas + per_t - 1) / per_t;
         lag                    = std::max<long long>(1, std::min<long long>(lag, (long long)batch));
-        const long long nslot  = std::min<long long>((long long)batch, 2 * lag + 2);
+        // slots in use at once: lag transforms between a column tile and its
+        // row tiles, on both sides; rounded up to a power of two so that the
+        // kernel finds a transform's slot with a mask
+        long long nslot = 1;
+        while (nslot < std::min<long long>((long long)batch, 2 * lag + 2)) nslot *= 2;
         std::lock_guard<std::mutex> g(p->mu);
         const size_t need = (size_t)nslot * per;
         if (p->scratch_bytes < need) {
@@ -752,18 +935,18 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
         a.conj_in    = io.conj_in;
         a.conj_out   = io.conj_out;
         a.scale      = io.scale;
-        a.stw1       = p->stw1;
-        a.stw2       = p->stw2;
-        a.tw_hi      = p->tw_hi;
-        a.tw_lo      = p->tw_lo;
-        a.tw_b       = p->tw_b;
+        a.stw1       = p->fs_st1;
+        a.stw2       = p->fs_st2;
+        a.tw_hi      = p->fs_thi;
+        a.tw_lo      = p->fs_tlo;
+        a.tw_b       = p->fs_tb;
         a.scratch    = p->scratch;
         a.nslot      = (int)nslot;
         a.lag        = (int)lag;
         a.col_done   = p->fs_ctr;
         a.row_done   = p->fs_ctr + batch;
         a.error      = p->err;
-        PCX_CUDA_TRY(pcx_fourstep(f64, p->log_n1, p->log_n2, a, st, p->sms, false, nullptr, nullptr, nullptr));
+        PCX_CUDA_TRY(pcx_fourstep(f64, p->fs_var, a, st, p->sms, false, nullptr, nullptr, nullptr));
         return PCX_OK;
     }
 
@@ -802,7 +985,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
                 c.batch      = rows;
                 c.conj_out   = 0;
                 c.scale      = 1.0;
-                c.stw        = p->stw1;
+                c.stw        = p->fst1;
                 c.tw_hi      = p->tw_hi;
                 c.tw_lo      = p->tw_lo;
                 c.tw_b       = p->tw_b;
@@ -860,7 +1043,7 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
                 r.dst_stride = (long long)dstride;
                 r.batch      = rows;
                 r.conj_in    = 0;
-                r.stw        = p->stw2;
+                r.stw        = p->fst2;
                 cudaError_t e = pcx_v3_row(f64, p->log_n1, p->log_n2, r, p->err, st2, p->sms, false);
                 if (e != cudaErrorNotSupported) {
                     PCX_CUDA_TRY(e);

@@ -655,6 +655,121 @@ __global__ void __launch_bounds__(NT, single3_minb(NT)) k_single3(v3_args a) {
 
 namespace pcxg {
 
+// Copy a table of BYTES bytes into shared memory (16-byte units; the caller syncs).
+template<int BYTES, class T>
+__device__ __forceinline__ void copy_table_to_smem(cpx<T>* dst, const void* src, int tid, int nt) {
+    static_assert(BYTES % 16 == 0, "table in 16-byte units");
+    const uint4* sp = reinterpret_cast<const uint4*>(src);
+    uint4*       dp = reinterpret_cast<uint4*>(dst);
+    for (int i = tid; i < BYTES / 16; i += nt) dp[i] = __ldg(sp + i);
+}
+
+// ---- full stage tables of the sub-transforms -------------------------------
+// For stage S >= 1 of splan P (Ns = 2^nsbits(S) butterfly positions, radix R)
+// position k keeps all R entries W^(j*k), j = 0..R-1, W = W_{Ns*R} (entry 0 is
+// 1), generated in FP64 and rounded once.  A butterfly then multiplies each
+// input by its table entry, where the factor tables of pcx_fft_v2.cuh form
+// nine of the fifteen radix-16 twiddles as products of two entries (36 more
+// FP32 instructions per butterfly).  For the sub-transforms of the four-step
+// (64..1024 points) a full table is 1-10 KB.
+template<class P>
+__host__ __device__ constexpr int fs_full_tw_offset(int S) {
+    int off = 0;
+    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) << P::rbits(s);
+    return off;
+}
+template<class P>
+__host__ __device__ constexpr int fs_full_tw_size() {
+    return fs_full_tw_offset<P>(P::NST);
+}
+
+template<class T>
+__global__ void k_full_twiddles(cpx<T>* out, int ns, int rb, int log_nsr) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (ns << rb)) return;
+    const long long e = (long long)(q >> rb) * (q & ((1 << rb) - 1));
+    double          sn, cs;
+    sincospi(2.0 * (double)e / (double)(1LL << log_nsr), &sn, &cs);
+    out[q] = {T(cs), T(-sn)};
+}
+
+// Butterflies of stage S >= 1 with the full table (tab: this sub-transform's).
+template<class P, int S, bool SH, class T, int E>
+__device__ __forceinline__ void stage_apply_full(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ tab) {
+    constexpr int RB  = P::rbits(S);
+    constexpr int R   = 1 << RB;
+    constexpr int NSB = P::nsbits(S);
+    constexpr int G   = E / R;
+    static_for<G>([&](auto gc) {
+        constexpr int g  = decltype(gc)::value;
+        const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
+        const cpx<T>* tw = tab + fs_full_tw_offset<P>(S) + (k << RB);
+        cpx<T>        a[R];
+        static_for<R / 2>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            cpx<T>        w0, w1;
+            ld2<SH>(tw + 2 * q, w0, w1);
+            a[2 * q]     = q == 0 ? v[g] : cmul(v[g + 2 * q * G], w0);
+            a[2 * q + 1] = cmul(v[g + (2 * q + 1) * G], w1);
+        });
+        dft<R, 1, 0>(a);
+        static_for<R>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            v[g + j * G]    = a[j];
+        });
+    });
+}
+
+// Barrier 1 over the NT compute threads that also ORs `bad` across them.
+template<int NT>
+__device__ __forceinline__ bool bar1_any(bool bad) {
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+                 "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((uint32_t)bad), "n"(NT)
+                 : "memory");
+    return r != 0;
+}
+
+// Stages 1..NST-1 through the exchange buffer with the full tables; the
+// barriers are xch_sync<BARN>.  With a named barrier (BARN > 0: the NT = BARN
+// compute threads of a block that also has a copy warp) the first exchange's
+// opening barrier doubles as the give-up vote: it returns true, before
+// anything is written, when any of those threads passes `bad`, so all of them
+// leave at the same point without a barrier of its own.  With BARN <= 0 `bad`
+// is ignored and the result is false.
+template<class P, class X, bool SH, int BARN, class T, int E>
+__device__ __forceinline__ bool run_stages_full(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
+                                                const cpx<T>* __restrict__ tab, bool bad = false) {
+    bool abort = false;
+    static_for<P::NST - 1>([&](auto sc) {
+        constexpr int S = decltype(sc)::value;
+        constexpr int G = E / (1 << P::rbits(S));
+        if (abort) return;
+        if constexpr (S == 0 && BARN > 0) {
+            if (bar1_any<BARN>(bad)) {
+                abort = true;
+                return;
+            }
+        } else {
+            xch_sync<BARN>();
+        }
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int g = i % G, j = i / G;
+            xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
+        });
+        xch_sync<BARN>();
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = xch[X::idx(m, t + i * P::TT)];
+        });
+        stage_apply_full<P, S + 1, SH>(v, t, tab);
+    });
+    return abort;
+}
+
 // ===========================================================================
 // TMA-fed four-step passes.  Same arithmetic as k_col2 / k_row2; the input
 // tiles arrive in shared memory through a two-stage bulk-copy ring
@@ -705,15 +820,19 @@ template<class T, int LOGN1, int C>
 __host__ __device__ constexpr int col3_base_smem() {
     return 2 * (1 << LOGN1) * 2 * C * (int)sizeof(T) + xch_interleaved<(1 << LOGN1), C>::size * (int)sizeof(cpx<T>);
 }
+// Full stage table bytes of an L = 2^LOGL point sub-transform.
+template<class T, int LOGL>
+__host__ __device__ constexpr int full_tw_bytes() {
+    return fs_full_tw_size<splan<LOGL>>() * (int)sizeof(cpx<T>);
+}
 template<class T, int LOGN1, int C>
 __host__ __device__ constexpr bool col3_tws() {
-    return stw_fits(col3_base_smem<T, LOGN1, C>(), stage_tw_smem_bytes<splan<LOGN1>, T>(), 1);
+    return stw_fits(col3_base_smem<T, LOGN1, C>(), full_tw_bytes<T, LOGN1>(), 1);
 }
 template<class T, int LOGN1, int C>
 __host__ __device__ constexpr int col3_smem() {
-    return col3_tws<T, LOGN1, C>()
-               ? smem_align16(col3_base_smem<T, LOGN1, C>()) + stage_tw_smem_bytes<splan<LOGN1>, T>()
-               : col3_base_smem<T, LOGN1, C>();
+    return col3_tws<T, LOGN1, C>() ? smem_align16(col3_base_smem<T, LOGN1, C>()) + full_tw_bytes<T, LOGN1>()
+                                   : col3_base_smem<T, LOGN1, C>();
 }
 
 template<class T, int LOGN1, int LOGN2, int LP, int C, int NT>
@@ -747,7 +866,7 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
     const int           t   = tid / C;
     const long long     tiles = a.batch * TPR;
 
-    if constexpr (SH) stage_tw_to_smem<P, T>(tws, a.stw, tid, NT);
+    if constexpr (SH) copy_table_to_smem<full_tw_bytes<T, LOGN1>()>(tws, a.stw, tid, NT);
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -802,7 +921,7 @@ __global__ void __launch_bounds__(NT, 1) k_col3(const __grid_constant__ CUtensor
         const cpx<T>   tl = ldg_cpx(tlo + (e0 & (N2 - 1)));
         const cpx<T>   tu = ldg_cpx(tb + n2);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X, SH>(v, xch, c, t, stw);
+        run_stages_full<P, X, SH, 0>(v, xch, c, t, stw);
         cpx<T>* dst = reinterpret_cast<cpx<T>*>(a.dst) + row * (a.dst_stride / 2) + (long long)t * N2 + n2;
         apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<T> o) {
             constexpr int i             = decltype(ic)::value;
@@ -820,13 +939,12 @@ __host__ __device__ constexpr int row3_base_smem() {
 }
 template<class T, int LOGN2, int CR, int G8>
 __host__ __device__ constexpr bool row3_tws() {
-    return stw_fits(row3_base_smem<T, LOGN2, CR, G8>(), stage_tw_smem_bytes<splan<LOGN2>, T>(), 1);
+    return stw_fits(row3_base_smem<T, LOGN2, CR, G8>(), full_tw_bytes<T, LOGN2>(), 1);
 }
 template<class T, int LOGN2, int CR, int G8>
 __host__ __device__ constexpr int row3_smem() {
-    return row3_tws<T, LOGN2, CR, G8>()
-               ? smem_align16(row3_base_smem<T, LOGN2, CR, G8>()) + stage_tw_smem_bytes<splan<LOGN2>, T>()
-               : row3_base_smem<T, LOGN2, CR, G8>();
+    return row3_tws<T, LOGN2, CR, G8>() ? smem_align16(row3_base_smem<T, LOGN2, CR, G8>()) + full_tw_bytes<T, LOGN2>()
+                                        : row3_base_smem<T, LOGN2, CR, G8>();
 }
 
 template<class T, int LOGN1, int LOGN2, int LP, int CR, int G8, int NT>
@@ -859,7 +977,7 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
     const long long     tiles = a.batch * TPR;
     const cpx<T>*       src = reinterpret_cast<const cpx<T>*>(a.src);
 
-    if constexpr (SH) stage_tw_to_smem<P, T>(tws, a.stw, tid, NT);
+    if constexpr (SH) copy_table_to_smem<full_tw_bytes<T, LOGN2>()>(tws, a.stw, tid, NT);
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -913,7 +1031,7 @@ __global__ void __launch_bounds__(NT, 1) k_row3(v3_pass_args pa) {
         __syncthreads();    // stage s consumed: refill it with the tile after next
         if (tid == 0 && tile + 2 * (long long)gridDim.x < tiles) issue(tile + 2 * (long long)gridDim.x, s);
         stage_compute_tab<P, 0>(v, t, stw);
-        run_stages_tab<P, X, SH>(v, xch, m, t, stw);
+        run_stages_full<P, X, SH, 0>(v, xch, m, t, stw);
         T*      dst = reinterpret_cast<T*>(a.dst) + row * a.dst_stride + pk<LP>(t * N1 + k1);
         const T sc  = T(a.scale);
         const T sim = a.conj_out ? -sc : sc;

@@ -1,63 +1,22 @@
-// Instantiations and launch of the one-launch four-step kernel (k_fourstep).
+// Dispatch of the one-launch four-step kernel (k_fourstep) over its variants,
+// its stage tables, and the self-tests of its bounded waits.
 #include "pcx_fourstep.cuh"
-#include "pcx_v2_launch.cuh"
+#include "pcx_host.hpp"
 
-namespace pcxg {
+// The variant translation units (pcx_fs_part*.cu).
+cudaError_t pcx_fs_part0(bool, const pcxg::fs_variant&, const pcxg::fs_args&, cudaStream_t, int, bool, int*, int*, int*);
+cudaError_t pcx_fs_part1(bool, const pcxg::fs_variant&, const pcxg::fs_args&, cudaStream_t, int, bool, int*, int*, int*);
+cudaError_t pcx_fs_part2(bool, const pcxg::fs_variant&, const pcxg::fs_args&, cudaStream_t, int, bool, int*, int*, int*);
+cudaError_t pcx_fs_part3(bool, const pcxg::fs_variant&, const pcxg::fs_args&, cudaStream_t, int, bool, int*, int*, int*);
+cudaError_t pcx_fs_part4(bool, const pcxg::fs_variant&, const pcxg::fs_args&, cudaStream_t, int, bool, int*, int*, int*);
 
-template<class T, int LOGN1, int LOGN2>
-static cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc, int* tr,
-                             int* per_sm) {
-    using F = fs_cfg<T, LOGN1, LOGN2>;
-    static_assert(F::SMEM <= 232448, "shared memory per block");
-    static_assert(F::MINB * (F::SMEM + 1024 + 256) <= 233472, "blocks per SM fit the shared memory");
-    static_assert(F::STAGE % 128 == 0, "TMA destinations stay 128-byte aligned");
-    auto kern = k_fourstep<T, LOGN1, LOGN2>;
-    if (tc) *tc = F::TC;
-    if (tr) *tr = F::TR;
-    if (attr_only) {
-        cudaError_t e = set_smem(kern, F::SMEM);
-        if (e == cudaSuccess && per_sm) e = occupancy_cached(reinterpret_cast<const void*>(kern), F::NT + 32, F::SMEM, per_sm);
-        return e;
-    }
-    const long long items = a.batch * (F::TC + F::TR);
-    if (items == 0) return cudaSuccess;
-    // 3-D view of the source: [transform][n1][2*N2 reals], box = 64 bytes x min(N1, 256) rows
-    CUtensorMap      map;
-    const cuuint64_t dims[3]    = {(cuuint64_t)2 << LOGN2, (cuuint64_t)1 << LOGN1, (cuuint64_t)a.batch};
-    const long long  ss         = a.batch > 1 ? a.src_stride : (2LL << (LOGN1 + LOGN2));    // unused when 1 row
-    const cuuint64_t strides[2] = {((cuuint64_t)2 << LOGN2) * sizeof(T), (cuuint64_t)ss * sizeof(T)};
-    const cuuint32_t box[3]     = {(cuuint32_t)(2 * F::C), (cuuint32_t)F::BOXY, 1};
-    const cuuint32_t estr[3]    = {1, 1, 1};
-    cudaError_t      e = encode_tensor_map(&map, sizeof(T) == 8, 3, const_cast<void*>(a.src), dims, strides, box, estr);
-    if (e != cudaSuccess) return e;
-    unsigned grid = 0;
-    e             = persistent_grid(kern, F::NT + 32, F::SMEM, items, sms, &grid);
-    if (e != cudaSuccess) return e;
-    kern<<<grid, F::NT + 32, F::SMEM, st>>>(map, a);
-    return cudaGetLastError();
-}
-
-template<class T>
-static cudaError_t dispatch_fs(int l1, int l2, const fs_args& a, cudaStream_t st, int sms, bool attr_only, int* tc,
-                               int* tr, int* per_sm) {
-    switch (l1 * 32 + l2) {
-    case 7 * 32 + 7: return launch_fs<T, 7, 7>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 8 * 32 + 7: return launch_fs<T, 8, 7>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 8 * 32 + 8: return launch_fs<T, 8, 8>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 9 * 32 + 8: return launch_fs<T, 9, 8>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 9 * 32 + 9: return launch_fs<T, 9, 9>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 10 * 32 + 9: return launch_fs<T, 10, 9>(a, st, sms, attr_only, tc, tr, per_sm);
-    case 10 * 32 + 10: return launch_fs<T, 10, 10>(a, st, sms, attr_only, tc, tr, per_sm);
-    default: return cudaErrorNotSupported;
-    }
-}
-
-}    // namespace pcxg
-
-cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
+cudaError_t pcx_fourstep(bool f64, const pcxg::fs_variant& v, const pcxg::fs_args& a, cudaStream_t st, int sms,
                          bool attr_only, int* col_tiles, int* row_tiles, int* blocks_per_sm) {
-    return f64 ? pcxg::dispatch_fs<double>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm)
-               : pcxg::dispatch_fs<float>(log_n1, log_n2, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm);
+    for (auto part: {pcx_fs_part0, pcx_fs_part1, pcx_fs_part2, pcx_fs_part3, pcx_fs_part4}) {
+        const cudaError_t e = part(f64, v, a, st, sms, attr_only, col_tiles, row_tiles, blocks_per_sm);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return cudaErrorNotSupported;
 }
 
 namespace {
@@ -78,6 +37,39 @@ __global__ void k_wait_probe(const int* ctr, int* out, unsigned long long mbar_l
     }
 }
 }    // namespace
+
+namespace {
+template<int LOGL, class T>
+cudaError_t gen_full_tables(void* out, cudaStream_t st) {
+    using P = pcxg::splan<LOGL>;
+    for (int s = 1; s < P::NST; ++s) {
+        const int n = (1 << P::nsbits(s)) << P::rbits(s);
+        auto*     o = static_cast<pcxg::cpx<T>*>(out) + pcxg::fs_full_tw_offset<P>(s);
+        pcxg::k_full_twiddles<T><<<(n + 255) / 256, 256, 0, st>>>(o, 1 << P::nsbits(s), P::rbits(s),
+                                                                 P::nsbits(s) + P::rbits(s));
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+template<int LOGL>
+cudaError_t full_tables(void* out, bool f64, cudaStream_t st, int* entries) {
+    *entries = pcxg::fs_full_tw_size<pcxg::splan<LOGL>>();
+    if (!out) return cudaSuccess;
+    return f64 ? gen_full_tables<LOGL, double>(out, st) : gen_full_tables<LOGL, float>(out, st);
+}
+}    // namespace
+
+cudaError_t pcx_fourstep_tables(int log_l, void* out, bool f64, cudaStream_t st, int* entries) {
+    switch (log_l) {
+    case 6: return full_tables<6>(out, f64, st, entries);
+    case 7: return full_tables<7>(out, f64, st, entries);
+    case 8: return full_tables<8>(out, f64, st, entries);
+    case 9: return full_tables<9>(out, f64, st, entries);
+    case 10: return full_tables<10>(out, f64, st, entries);
+    default: return cudaErrorNotSupported;
+    }
+}
 
 namespace {
 // One thread waits, bounded by limit_ns, on phase 0 of an mbarrier nobody

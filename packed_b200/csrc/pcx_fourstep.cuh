@@ -8,21 +8,29 @@
 //     col(0..lag-1), [col(r+lag), row(r)] for r = 0.., row(batch-lag..)
 // and CTA b takes items b, b + grid, b + 2*grid, ...  A row tile waits until
 // all column tiles of its transform are written (col_done[r] == TC); a column
-// tile of transform r writes slot r % nslot only after every row tile of
+// tile of transform r writes slot r & (nslot-1) only after every row tile of
 // transform r - nslot has read it (row_done[r - nslot] == TR).  Every
 // dependency points to an earlier item, so the smallest unfinished item can
 // always run.
 //
-// Each CTA has NT compute threads and one copy warp.  The copy warp owns
-// everything that waits on other CTAs: it checks dependencies, issues the TMA
-// copies into a two-stage ring, tells the compute warps when a column tile's
-// slot is free, and publishes completions (col_done after the compute warps
-// have written a column tile; row_done once a row tile's scratch rows have
-// landed in shared memory and their L2 lines are dropped without write-back).
-// Before it blocks on another CTA it first publishes its own pending
-// completion, so it never waits while holding one.  The compute warps only
-// wait on mbarriers of their own CTA and synchronise among themselves on a
-// named barrier, so no dependency latency sits on their critical path.
+// Each CTA has NT compute threads and two helper warps, so that no wait sits
+// on the compute warps' path except their own tile landing:
+//  * the producer warp walks the CTA's items, waits for a ring stage to be
+//    free and for the item's dependency on other CTAs, and issues the TMA
+//    copies into the ST-stage ring (for a column tile it also tells the
+//    compute warps when the slot may be written);
+//  * the publisher warp walks the same items and publishes each completion as
+//    soon as it happens (col_done once the compute warps wrote a column tile;
+//    row_done once a row tile's scratch rows have landed in shared memory and
+//    their L2 lines are dropped unwritten).  It never waits on another CTA, so
+//    the completions other CTAs wait for are never held up behind this CTA's
+//    own dependency waits.
+// A stage is refilled after the compute warps are done with it and the
+// publisher has passed its item (empty[s] counts both), so no barrier phase is
+// ever overtaken.  With three stages the exchanges of the sub-transforms run
+// in place in the item's own stage buffer (the tile is in registers by the
+// first exchange barrier), which keeps the ring within the shared memory of
+// two stages plus an exchange buffer while the producer runs two items ahead.
 //
 // Compared with one launch per pass per scratch chunk this removes the ramp
 // and tail of every short launch (the SMs were idle ~30% of each chunk).
@@ -41,27 +49,31 @@ struct fs_args {
     int         conj_in;
     int         conj_out;
     double      scale;
-    const void* stw1;     // stage tables of the N1 and N2 sub-transforms
+    const void* stw1;     // full stage tables of the N1 and N2 sub-transforms (fs_full_tw_*)
     const void* stw2;
     const void* tw_hi;    // W_N^(i*N2), i < N1
     const void* tw_lo;    // W_N^i, i < N2
     const void* tw_b;     // W_{16*N2}^m
     void*       scratch;  // nslot slots of N complex
-    int         nslot;
+    int         nslot;    // a power of two: transform r uses slot r & (nslot - 1)
     int         lag;      // transforms between a column pass and its row pass
     int*        col_done;
     int*        row_done;
     int*        error;
 };
 
-template<class T, int LOGN1, int LOGN2>
+// Variant of the one-launch four-step: split N = 2^LOGN1 * 2^LOGN2, MINB
+// resident blocks per SM (tiles of 64 KB / MINB: two blocks of 32 KB tiles
+// let one block issue while the other waits at a barrier, and need both
+// sub-transforms <= 512 points so that a tile still spans whole 32-byte
+// sectors of its rows), and ST ring stages (3: the exchanges run in place in
+// the item's stage; 2: a separate exchange buffer).  pcx_plan_tune times the
+// variants that are built for a size and keeps the fastest.
+template<class T, int LOGN1, int LOGN2, int MINB_ = (LOGN1 <= 9 ? 2 : 1), int ST_ = 3>
 struct fs_cfg {
     static constexpr int N1   = 1 << LOGN1;
     static constexpr int N2   = 1 << LOGN2;
-    // Two blocks per SM with 32 KB tiles while a column tile still spans
-    // whole 32-byte sectors of its rows (N1 <= 512): the two blocks' barrier
-    // phases run independently, so one issues while the other waits.
-    static constexpr int MINB = LOGN1 <= 9 ? 2 : 1;
+    static constexpr int MINB = MINB_;
     static constexpr int TILE = 65536 / MINB / (int)sizeof(cpx<T>);
     static constexpr int G8   = 64 / (2 * (int)sizeof(T));
     static constexpr int LP   = G8 == 8 ? 3 : 2;
@@ -76,13 +88,17 @@ struct fs_cfg {
     static constexpr int RSI  = N2 + 2;    // padded shared row of a row tile (complex)
     static constexpr int COLB = N1 * 2 * C * (int)sizeof(T);
     static constexpr int ROWB = CR * RSI * (int)sizeof(cpx<T>);
-    static constexpr int STAGE = ((COLB > ROWB ? COLB : ROWB) + 127) / 128 * 128;
     using X1                  = xch_interleaved<N1, C>;
     using X2                  = xch_grouped<N2, CR, G8>;
     static constexpr int XB   = smem_align16((X1::size > X2::size ? X1::size : X2::size) * (int)sizeof(cpx<T>));
-    static constexpr int BASE = 2 * STAGE + XB;
-    static constexpr int TB1  = stage_tw_smem_bytes<P1, T>();
-    static constexpr int TB2  = stage_tw_smem_bytes<P2, T>();
+    static constexpr int ST   = ST_;
+    static constexpr bool IP  = ST == 3;
+    static_assert(ST == 2 || ST == 3, "two or three ring stages");
+    static constexpr int TILEB = COLB > ROWB ? COLB : ROWB;
+    static constexpr int STAGE = ((IP ? (TILEB > XB ? TILEB : XB) : TILEB) + 127) / 128 * 128;
+    static constexpr int BASE = ST * STAGE + (IP ? 0 : XB);
+    static constexpr int TB1  = fs_full_tw_size<P1>() * (int)sizeof(cpx<T>);
+    static constexpr int TB2  = fs_full_tw_size<P2>() * (int)sizeof(cpx<T>);
     static constexpr bool SH  = stw_fits(BASE, TB1 + TB2, MINB);
     static constexpr int SMEM = SH ? BASE + TB1 + TB2 : BASE;
     static constexpr int BOXY = N1 < 256 ? N1 : 256;
@@ -115,19 +131,6 @@ struct fs_item {
     int       tile;
 };
 
-// OR of `bad` over the NT compute threads (named barrier 2), the same answer
-// in every one of them.
-template<int NT>
-__device__ __forceinline__ bool compute_any_failed(bool bad) {
-    uint32_t r;
-    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
-                 "bar.red.or.pred q, 2, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
-                 : "=r"(r)
-                 : "r"((uint32_t)bad), "n"(NT)
-                 : "memory");
-    return r != 0;
-}
-
 // counter += 1 with release semantics at GPU scope: this thread's earlier
 // writes, and those it has observed, are visible to whoever acquires the count
 __device__ __forceinline__ void red_release_add(int* p, int v) {
@@ -149,16 +152,18 @@ __device__ __forceinline__ fs_item fs_decode(long long j, long long batch, int l
     return {1, batch - lag + j / TR, (int)(j % TR)};
 }
 
-template<class T, int LOGN1, int LOGN2>
-__global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LOGN1, LOGN2>::MINB)
+template<class T, int LOGN1, int LOGN2, int MINB, int ST_>
+__global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, MINB)
     k_fourstep(const __grid_constant__ CUtensorMap tmap, fs_args a) {
-    using F            = fs_cfg<T, LOGN1, LOGN2>;
+    using F            = fs_cfg<T, LOGN1, LOGN2, MINB, ST_>;
     using P1           = typename F::P1;
     using P2           = typename F::P2;
     constexpr int N1   = F::N1;
     constexpr int N2   = F::N2;
-    constexpr int NT   = F::NT;    // compute threads; warp NT/32 copies
+    constexpr int NT   = F::NT;    // compute threads; then the producer warp, then the publisher warp
     constexpr int NW   = NT / 32;
+    constexpr int ST   = F::ST;
+    constexpr bool IP  = F::IP;
     constexpr int C    = F::C;
     constexpr int CR   = F::CR;
     constexpr int TC   = F::TC;
@@ -173,26 +178,26 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
     constexpr bool SH  = F::SH;
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char*      ring = smem;
-    cpx<T>*             xch  = reinterpret_cast<cpx<T>*>(smem + 2 * F::STAGE);
     cpx<T>*             tws1 = reinterpret_cast<cpx<T>*>(smem + F::BASE);
     cpx<T>*             tws2 = tws1 + F::TB1 / (int)sizeof(cpx<T>);
-    __shared__ uint64_t full[2];     // TMA bytes landed
-    __shared__ uint64_t empty[2];    // compute warps have read the stage
-    __shared__ uint64_t slotok[2];   // column tile: its scratch slot may be written
-    __shared__ uint64_t written[2];  // column tile: compute warps wrote the slot
+    __shared__ uint64_t full[ST];      // TMA bytes landed
+    __shared__ uint64_t empty[ST];     // compute warps done with the stage, publisher past its item
+    __shared__ uint64_t slotok[ST];    // column tile: its scratch slot may be written
+    __shared__ uint64_t written[ST];   // column tile: compute warps wrote the slot
     cpx<T>*             scr   = reinterpret_cast<cpx<T>*>(a.scratch);
     const int           tid   = threadIdx.x;
     const long long     items = a.batch * (TC + TR);
     const long long     G     = gridDim.x;
+    const long long     mask  = a.nslot - 1;
 
     if constexpr (SH) {
-        stage_tw_to_smem<P1, T>(tws1, a.stw1, tid, NT + 32);
-        stage_tw_to_smem<P2, T>(tws2, a.stw2, tid, NT + 32);
+        copy_table_to_smem<F::TB1>(tws1, a.stw1, tid, NT + 64);
+        copy_table_to_smem<F::TB2>(tws2, a.stw2, tid, NT + 64);
     }
     if (tid == 0) {
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < ST; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NW);
+            mbar_init(&empty[s], NW + 1);
             mbar_init(&slotok[s], 1);
             mbar_init(&written[s], NW);
         }
@@ -200,94 +205,79 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
     }
     __syncthreads();
 
-    if (tid >= NT) {
-        // ======================= copy warp
-        const int      lane     = tid - NT;
-        const uint64_t pol      = l2_evict_first_policy();    // column tiles are read once
-        long long      pending  = -1;    // item whose completion is not yet published
-        int            pend_s   = 0;
-        uint32_t       pend_par = 0;
-        long long      rowdef   = -1;    // row item published once its stage was read
-        int            rd_s     = 0;
-        uint32_t       rd_par   = 0;
-        bool           fail     = false;
-        int            ncol[2]  = {0, 0};    // column items seen per stage (slotok / written phases)
-        int            pcol     = 0;         // written phase of the pending column item
-        // bounded mbarrier wait by lane 0, the answer shared by the warp
-        auto wwait = [&](uint64_t* bar, uint32_t parity) -> bool {
-            int ok = 1;
-            if (lane == 0) ok = mbar_wait_bounded(bar, parity) ? 1 : 0;
-            return __shfl_sync(0xffffffffu, ok, 0) != 0;
-        };
-        // row item `jr` is done once its rows are in shared memory: drop their
-        // L2 lines unwritten and count it
-        auto publish_row = [&](long long jr) {
-            const fs_item it = fs_decode(jr, a.batch, a.lag, TC, TR);
-            const char*   g  = reinterpret_cast<const char*>(scr + (it.r % a.nslot) * (long long)(N1 * N2) +
-                                                          (long long)it.tile * CR * N2);
-            for (int q = lane; q < CR * RROW / 128; q += 32) l2_discard(g + (size_t)q * 128);
-            __syncwarp();
-            if (lane == 0) red_release_add(a.row_done + it.r, 1);
-        };
-        // the deferred row item, after waiting for its rows to land
-        auto flush_rowdef = [&]() {
-            if (rowdef < 0) return;
-            if (!wwait(&full[rd_s], rd_par)) fail = true;
-            if (!fail) publish_row(rowdef);
-            rowdef = -1;
-        };
-        // publish the completion of `pending`; a row item may instead be
-        // deferred until the compute warps have read its stage (so its copy
-        // has landed without waiting for it here)
-        auto complete = [&](bool defer_row) {
-            if (pending < 0) return;
-            const fs_item it = fs_decode(pending, a.batch, a.lag, TC, TR);
+    if (tid >= NT + 32) {
+        // ======================= publisher warp
+        const int lane    = tid - NT - 32;
+        int       ncol[ST] = {};
+        bool      fail    = false;
+        long long k       = 0;
+        for (long long j = blockIdx.x; j < items && !fail; j += G, ++k) {
+            const int      s   = (int)(k % ST);
+            const uint32_t par = (uint32_t)((k / ST) & 1);
+            const fs_item  it  = fs_decode(j, a.batch, a.lag, TC, TR);
+            int            ok  = 1;
             if (!it.row) {
-                if (!wwait(&written[pend_s], (uint32_t)(pcol & 1))) fail = true;
-                if (lane == 0 && !fail) {
-                    fence_proxy_async_global();    // the slot is read back by TMA copies
+                // the compute warps' stores of the tile are done: make them
+                // visible to other CTAs' TMA reads, then count the tile
+                if (lane == 0) ok = mbar_wait_bounded(&written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                ++ncol[s];
+                if (ok && lane == 0) {
+                    fence_proxy_async_global();
                     red_release_add(a.col_done + it.r, 1);
                 }
-            } else if (defer_row) {
-                rowdef = pending;
-                rd_s   = pend_s;
-                rd_par = pend_par;
             } else {
-                if (!wwait(&full[pend_s], pend_par)) fail = true;
-                if (!fail) publish_row(pending);
+                // the tile's scratch rows are in shared memory: drop their L2
+                // lines unwritten and count the tile
+                if (lane == 0) ok = mbar_wait_bounded(&full[s], par) ? 1 : 0;
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (ok) {
+                    const char* g = reinterpret_cast<const char*>(scr + (it.r & mask) * (long long)(N1 * N2) +
+                                                                  (long long)it.tile * CR * N2);
+                    for (int q = lane; q < CR * RROW / 128; q += 32) l2_discard(g + (size_t)q * 128);
+                    __syncwarp();
+                    if (lane == 0) red_release_add(a.row_done + it.r, 1);
+                }
             }
-            pending = -1;
-        };
-        // wait for *ctr >= target, publishing every pending completion first
+            if (!ok) {
+                fail = true;
+                if (lane == 0) atomicExch(a.error, 1);
+            } else if (lane == 0) {
+                mbar_arrive(&empty[s]);
+            }
+        }
+        __syncwarp();
+        return;
+    }
+
+    if (tid >= NT) {
+        // ======================= producer warp
+        const int      lane   = tid - NT;
+        const uint64_t pol    = l2_evict_first_policy();    // column tiles are read once
+        bool           fail   = false;
+        long long      issued = 0;    // items whose copies were issued
+        long long      k      = 0;
+        // bounded wait for *ctr >= target by lane 0, the answer shared by the warp
         auto need = [&](const int* ctr, int target) -> bool {
-            int v = 0;
-            if (lane == 0) v = ld_acquire(ctr);
-            v = __shfl_sync(0xffffffffu, v, 0);
-            if (v >= target) return true;
-            flush_rowdef();
-            complete(false);
-            if (fail) return false;
             int ok = 1;
             if (lane == 0) ok = fs_wait(ctr, target) ? 1 : 0;
             return __shfl_sync(0xffffffffu, ok, 0) != 0;
         };
-        long long k = 0;
         for (long long j = blockIdx.x; j < items && !fail; j += G, ++k) {
-            const int      s   = (int)(k & 1);
-            const uint32_t par = (uint32_t)((k >> 1) & 1);
-            if (k >= 2 && !wwait(&empty[s], par ^ 1u)) {
-                fail = true;
-                break;
-            }
-            // the stage's previous item (k-2) has been read: a deferred row
-            // item from it is done
-            if (rowdef >= 0) {
-                publish_row(rowdef);
-                rowdef = -1;
+            const int      s   = (int)(k % ST);
+            const uint32_t par = (uint32_t)((k / ST) & 1);
+            if (k >= ST) {
+                int ok = 1;
+                if (lane == 0) ok = mbar_wait_bounded(&empty[s], par ^ 1u) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    fail = true;
+                    break;
+                }
             }
             const fs_item  it  = fs_decode(j, a.batch, a.lag, TC, TR);
             unsigned char* buf = ring + s * F::STAGE;
             if (!it.row) {
+                // the source tile does not depend on anything: copy it first
                 if (lane == 0) {
                     mbar_arrive_expect_tx(&full[s], F::COLB);
 #pragma unroll
@@ -296,24 +286,15 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                                          &full[s], pol);
                     }
                 }
-                const bool ok = it.r < a.nslot || need(a.row_done + (it.r - a.nslot), TR);
-                if (!ok) {
-                    fail     = true;
-                    pending  = j;    // the copy is in flight: wait for it below
-                    pend_s   = s;
-                    pend_par = par;
-                    break;
-                }
-                __syncwarp();
+                issued = k + 1;
                 // the acquire of the slot's counter (or a first use of the
                 // slot) orders the compute warps' writes after the earlier
                 // row tiles' reads, through this arrive and their wait
+                if (!(it.r < a.nslot || need(a.row_done + (it.r - a.nslot), TR))) {
+                    fail = true;
+                    break;
+                }
                 if (lane == 0) mbar_arrive(&slotok[s]);
-                complete(true);
-                pending  = j;
-                pend_s   = s;
-                pend_par = par;
-                pcol     = ncol[s]++;
             } else {
                 if (!need(a.col_done + it.r, TC)) {
                     fail = true;
@@ -325,39 +306,48 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                     mbar_arrive_expect_tx(&full[s], CR * RROW);
                 }
                 __syncwarp();
-                const cpx<T>* g = scr + (it.r % a.nslot) * (long long)(N1 * N2) + (long long)it.tile * CR * N2;
+                const cpx<T>* g = scr + (it.r & mask) * (long long)(N1 * N2) + (long long)it.tile * CR * N2;
                 for (int q = lane; q < CR; q += 32) {
                     bulk_g2s(reinterpret_cast<cpx<T>*>(buf) + q * RSI, g + (long long)q * N2, RROW, &full[s]);
                 }
-                __syncwarp();
-                complete(true);
-                pending  = j;
-                pend_s   = s;
-                pend_par = par;
+                issued = k + 1;
             }
-        }
-        if (!fail) {
-            flush_rowdef();
-            complete(false);
+            __syncwarp();
         }
         if (fail && lane == 0) {
-            // no copy may still be landing when the block exits
+            // no copy may still be landing when the block exits: wait
+            // (bounded) for the last ST issued items' copies
             atomicExch(a.error, 1);
-            if (pending >= 0) mbar_wait_bounded(&full[pend_s], pend_par, 100000000ull);
-            if (rowdef >= 0) mbar_wait_bounded(&full[rd_s], rd_par, 100000000ull);
+            for (long long q = issued - 1; q >= 0 && q >= issued - ST; --q) {
+                mbar_wait_bounded(&full[(int)(q % ST)], (uint32_t)((q / ST) & 1), 100000000ull);
+            }
         }
         __syncwarp();
         return;
     }
 
     // ======================= compute warps
-    const int lane    = tid % 32;
-    int       ncol[2] = {0, 0};
-    long long k       = 0;
+    // A bounded wait that gives up (tile copy or slot hand-off) is recorded
+    // in `bad`; the work of that item goes on with whatever the stage holds,
+    // nothing is stored, and at the next exchange barrier, which doubles as
+    // a vote, every compute thread leaves together (run_stages_full).
+    const int lane     = tid % 32;
+    int       ncol[ST] = {};
+    bool      bad      = false;
+    long long k        = 0;
+    cpx<T>*   xsep     = reinterpret_cast<cpx<T>*>(smem + ST * F::STAGE);    // exchange buffer when !IP
     for (long long j = blockIdx.x; j < items; j += G, ++k) {
-        const int      s   = (int)(k & 1);
-        const uint32_t par = (uint32_t)((k >> 1) & 1);
+        const int      s   = (int)(k % ST);
+        const uint32_t par = (uint32_t)((k / ST) & 1);
         const fs_item it = fs_decode(j, a.batch, a.lag, TC, TR);
+        cpx<T>*        xch = IP ? reinterpret_cast<cpx<T>*>(ring + s * F::STAGE) : xsep;
+        // the stage is no longer read: it may be refilled (the publisher adds
+        // its own arrival once it has passed the item)
+        auto release_stage = [&]() {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        };
         // column tile: the four-step twiddle inputs are requested before the
         // tile's data is waited for, and used after the stages
         cpx<T> th{}, tl{}, tu{};
@@ -368,10 +358,9 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
             tl                = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_lo) + (e0 & (N2 - 1)));
             tu                = ldg_cpx(reinterpret_cast<const cpx<T>*>(a.tw_b) + n2);
         }
-        // all compute warps leave together when any of them gave up
-        if (compute_any_failed<NT>(!mbar_wait_bounded(&full[s], par))) {
-            if (tid == 0) atomicExch(a.error, 1);
-            return;
+        if (!mbar_wait_bounded(&full[s], par)) {
+            bad = true;
+            atomicExch(a.error, 1);
         }
         if (!it.row) {
             // ---------------- column tile: N1-point DFTs down C columns
@@ -388,25 +377,26 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                 cpx<T>        x = lds_swapped<T, SW>(in, (t + i * TT) * SEG + pk<LP>(c), PK);
                 v[i]            = {x.re, a.conj_in ? -x.im : x.im};
             });
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
+            if constexpr (!IP) release_stage();
             stage_compute_tab<P1, 0>(v, t, stw1);
-            run_stages_tab<P1, typename F::X1, SH, NT>(v, xch, c, t, stw1);
-            const bool sok = mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1));
-            ++ncol[s];
-            if (compute_any_failed<NT>(!sok)) {
-                // the copy warp gave up on this slot: nothing is written
-                if (tid == 0) atomicExch(a.error, 1);
-                return;
+            if (run_stages_full<P1, typename F::X1, SH, NT>(v, xch, c, t, stw1, bad)) return;
+            if constexpr (IP) release_stage();
+            if (!mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1))) {
+                // the producer gave up on this slot: nothing is written, and
+                // the compute warps leave at the next item's vote
+                bad = true;
+                atomicExch(a.error, 1);
             }
-            cpx<T>* dst = scr + (it.r % a.nslot) * (long long)(N1 * N2) + (long long)t * N2 + n2;
-            apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<T> o) {
-                constexpr int i             = decltype(ic)::value;
-                dst[(long long)i * TT * N2] = o;
-            });
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&written[s]);
+            ++ncol[s];
+            if (!bad) {
+                cpx<T>* dst = scr + (it.r & mask) * (long long)(N1 * N2) + (long long)t * N2 + n2;
+                apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<T> o) {
+                    constexpr int i             = decltype(ic)::value;
+                    dst[(long long)i * TT * N2] = o;
+                });
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&written[s]);
+            }
         } else {
             // ---------------- row tile: N2-point DFTs along CR rows
             constexpr int E    = P2::E;
@@ -423,11 +413,10 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2>::NT + 32, fs_cfg<T, LO
                 constexpr int i = decltype(ic)::value;
                 v[i]            = in[i * TT];
             });
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
+            if constexpr (!IP) release_stage();
             stage_compute_tab<P2, 0>(v, t, stw2);
-            run_stages_tab<P2, typename F::X2, SH, NT>(v, xch, m, t, stw2);
+            if (run_stages_full<P2, typename F::X2, SH, NT>(v, xch, m, t, stw2, bad)) return;
+            if constexpr (IP) release_stage();
             T*      dst = reinterpret_cast<T*>(a.dst) + it.r * a.dst_stride + pk<LP>(t * N1 + k1);
             const T sc  = T(a.scale);
             const T sim = a.conj_out ? -sc : sc;

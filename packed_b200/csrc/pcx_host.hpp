@@ -55,6 +55,29 @@ inline cudaError_t smem_attr_cached(const void* kern, int bytes) {
 
 struct v2_args;
 struct v3_args;
+
+// A variant of the one-launch four-step kernel (k_fourstep): the split
+// N = 2^l1 * 2^l2, resident blocks per SM and ring stages.
+struct fs_variant {
+    int l1 = 0, l2 = 0, minb = 0, st = 0;
+    bool operator==(const fs_variant& o) const { return l1 == o.l1 && l2 == o.l2 && minb == o.minb && st == o.st; }
+};
+// The variants built into the library (FP32 and FP64), in the order the
+// autotuner tries them; the first one of a size is its untuned default (the
+// fastest one measured on a B200 on 512 MB batches; at 2^15 and 2^17..2^19 an
+// uneven split with the longer sub-transform in the row pass is fastest).
+constexpr fs_variant kFsVariantsF32[] = {
+    {7, 7, 2, 3},  {7, 7, 1, 3},                                      // 2^14
+    {7, 8, 2, 3},  {8, 7, 2, 3},                                      // 2^15
+    {8, 8, 2, 3},  {8, 8, 1, 3},  {7, 9, 2, 3},  {9, 7, 2, 3},        // 2^16
+    {8, 9, 2, 3},  {9, 8, 2, 3},  {10, 7, 1, 3}, {9, 8, 1, 3},        // 2^17
+    {8, 10, 1, 3}, {10, 8, 1, 3}, {9, 9, 1, 3},  {9, 9, 2, 3},        // 2^18
+    {9, 10, 1, 3}, {9, 10, 1, 2}, {10, 9, 1, 2}, {10, 9, 1, 3},       // 2^19
+    {10, 10, 1, 3}, {10, 10, 1, 2},                                   // 2^20
+};
+constexpr fs_variant kFsVariantsF64[] = {
+    {7, 7, 2, 3}, {8, 7, 2, 3}, {8, 8, 2, 3}, {9, 8, 2, 3}, {9, 9, 2, 3}, {10, 9, 1, 2}, {10, 10, 1, 2},
+};
 }
 
 // Record `msg` as this thread's last error and return `code`.
@@ -109,6 +132,17 @@ struct pcx_plan_s {
     void*  stw2     = nullptr;    // stage twiddles of the row pass (N2)
     void*  tw_b     = nullptr;    // W_{16*N2}^m, m < 16*N2
     void*  stw_one  = nullptr;    // stage twiddles of a one-pass form of a two-pass size (N = 8192)
+    void*  fst      = nullptr;    // one-launch four-step: full stage tables of N1 then N2 (one allocation)
+    void*  fst1     = nullptr;
+    void*  fst2     = nullptr;
+    pcxg::fs_variant fs_var{};    // one-launch four-step: its variant (l1 == 0: none)
+    void*  fs_mem   = nullptr;    // tables of fs_var's split (one allocation):
+    void*  fs_thi   = nullptr;    //   W_N^(i*N2), i < N1
+    void*  fs_tlo   = nullptr;    //   W_N^i, i < N2
+    void*  fs_tb    = nullptr;    //   W_{16*N2}^i, i < N2
+    void*  fs_st1   = nullptr;    //   full stage tables of the N1- and N2-point sub-transforms
+    void*  fs_st2   = nullptr;
+    int    fs_tab_l1 = 0;         // split the tables belong to
     int    fs_tc    = 0;          // one-launch four-step: column and row tiles per transform (0: none)
     int    fs_tr    = 0;
     int    fs_per_sm = 1;         // its resident blocks per SM
@@ -154,8 +188,11 @@ cudaError_t pcx_v3_single(bool f64, int log_n, const pcxg::v3_args& a, cudaStrea
 namespace pcxg {
 struct fs_args;
 }
-cudaError_t pcx_fourstep(bool f64, int log_n1, int log_n2, const pcxg::fs_args& a, cudaStream_t st, int sms,
+cudaError_t pcx_fourstep(bool f64, const pcxg::fs_variant& v, const pcxg::fs_args& a, cudaStream_t st, int sms,
                          bool attr_only, int* col_tiles, int* row_tiles, int* blocks_per_sm);
+// Full stage tables of an L = 2^log_l point sub-transform of the one-launch
+// four-step (entries: their count; out == nullptr only counts).
+cudaError_t pcx_fourstep_tables(int log_l, void* out, bool f64, cudaStream_t st, int* entries);
 cudaError_t pcx_v2_col(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,
                        bool attr_only);
 cudaError_t pcx_v2_row(bool f64, int log_n1, int log_n2, const pcxg::v2_args& a, cudaStream_t st, int sms,

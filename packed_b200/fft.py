@@ -251,11 +251,47 @@ class fft_unit:
         _lib.check(_lib.lib().pcx_plan_form(self._plan, ctypes.byref(f), ctypes.byref(r), ctypes.byref(c)))
         return {"form": self.FORMS.get(f.value, str(f.value)), "rounds": r.value, "chunk_bytes": c.value}
 
+    def tuning(self) -> dict:
+        """The plan's form and, for the one-launch four-step, its variant (pcx_plan_tuning):
+        split N1 x N2, blocks per SM (tile shape), ring stages, dependency distance in rounds."""
+        r = _lib.TuneResult()
+        _lib.check(_lib.lib().pcx_plan_tuning(self._plan, ctypes.byref(r)))
+        out = {"form": self.FORMS.get(r.form, str(r.form)), "rounds": r.rounds, "chunk_bytes": r.chunk_bytes}
+        if r.log_n1 > 0 and r.form in (0, 2):
+            out.update({"split": [1 << r.log_n1, 1 << r.log_n2], "blocks_per_sm": r.blocks_per_sm,
+                        "stages": r.stages})
+        return out
+
+    def set_tuning(self, form: str = "one-launch four-step", *, split: tuple[int, int] | None = None,
+                   blocks_per_sm: int = 0, stages: int = 0, rounds: int = 3, chunk_bytes: int = 0) -> None:
+        """Choose a form (and four-step variant) without timing it (pcx_plan_set_tuning)."""
+        codes = {v: k for k, v in self.FORMS.items()}
+        r = _lib.TuneResult()
+        r.form = codes[form]
+        r.rounds = rounds
+        r.chunk_bytes = chunk_bytes
+        if split is not None:
+            r.log_n1, r.log_n2 = (int(split[0]).bit_length() - 1, int(split[1]).bit_length() - 1)
+            r.blocks_per_sm, r.stages = blocks_per_sm, stages
+        _lib.check(_lib.lib().pcx_plan_set_tuning(self._plan, ctypes.byref(r)))
+
+    def describe_form(self) -> str:
+        """One line naming the form, its split and tile shape (for reports)."""
+        t = self.tuning()
+        if "split" in t and t["form"] in ("default", "one-launch four-step"):
+            n1, n2 = t["split"]
+            return (f"one-launch four-step {n1}x{n2}, {t['blocks_per_sm']} block(s)/SM "
+                    f"({64 // t['blocks_per_sm']} KB tiles), {t['stages']} stages, distance {t['rounds']} rounds")
+        if t["form"] == "chunked four-step":
+            return f"chunked four-step, {t['chunk_bytes'] >> 20} MB scratch per buffer"
+        return t["form"]
+
     def tune(self, batch: int = 1, stream=None) -> str:
-        """Time this size's forms on `batch` rows and keep the fastest (pcx_plan_tune)."""
+        """Time this size's forms and four-step variants on `batch` rows and keep the fastest
+        (pcx_plan_tune); returns describe_form()."""
         form = ctypes.c_int(0)
         _lib.check(_lib.lib().pcx_plan_tune(self._plan, batch, _stream_ptr(stream), ctypes.byref(form)))
-        return self.FORMS.get(form.value, str(form.value))
+        return self.describe_form()
 
     # ---------------------------------------------------------- raw calls
     def exec(self, dst: torch.Tensor, src: torch.Tensor, *, direction: int = 0, normalize: bool = True,

@@ -1,6 +1,8 @@
 """GPU parity of the FFT path (libpcx_cuda.so through its C ABI) against the
 CPU oracle and the reference's golden outputs.  Bar: relative L2 2e-6 (FP32),
 1e-13 (FP64)."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 import torch
@@ -322,7 +324,8 @@ def test_tune_picks_a_form_and_keeps_parity(log_n, batch):
     n = 1 << log_n
     unit = fft_unit(n, dtype=F32)
     form = unit.tune(batch)
-    assert form in ("one-pass", "one-launch four-step", "chunked four-step")
+    assert form.split(" 1")[0].split(" 2")[0].split(",")[0] in ("one-pass", "one-launch four-step",
+                                                                 "chunked four-step"), form
     rng = np.random.default_rng(400 + log_n)
     z = normal_cx(rng, batch, n)
     x = O.pack(z, 8)
@@ -333,6 +336,48 @@ def test_tune_picks_a_form_and_keeps_parity(log_n, batch):
     assert rel_l2(O.unpack(got[:k], n, 8), O.unpack(want, n, 8)) < TOL[np.float32]
     back = run(unit, got, batch, direction=1)
     assert rel_l2(O.unpack(back, n, 8), z) < TOL[np.float32]
+
+
+def _variants():
+    from packed_b200 import _lib as L
+    import re
+    text = (Path(__file__).resolve().parents[1] / "packed_b200" / "csrc" / "pcx_host.hpp").read_text()
+    out = []
+    for name, dt in (("kFsVariantsF32", F32), ("kFsVariantsF64", F64)):
+        body = text[text.index(name):]
+        body = body[: body.index("};")]
+        out += [(dt, *map(int, m)) for m in re.findall(r"\{(\d+), (\d+), (\d+), (\d+)\}", body)]
+    return out
+
+
+@pytest.mark.parametrize("dtype,l1,l2,minb,st", _variants())
+def test_every_fourstep_variant_matches_oracle(dtype, l1, l2, minb, st):
+    """Every built-in variant of the one-launch four-step (split, blocks per
+    SM, ring stages), chosen explicitly through pcx_plan_set_tuning, against
+    the oracle: forward and inverse, a ragged batch."""
+    n = 1 << (l1 + l2)
+    p = 8 if dtype == F32 else 4
+    batch = 5 if n <= (1 << 16) else 2
+    rng = np.random.default_rng(l1 * 100 + l2 * 10 + minb + st)
+    z = normal_cx(rng, batch, n)
+    x = O.pack(z, p, NPD[dtype])
+    unit = fft_unit(n, dtype=dtype)
+    unit.set_tuning("one-launch four-step", split=(1 << l1, 1 << l2), blocks_per_sm=minb, stages=st, rounds=2)
+    t = unit.tuning()
+    assert t["split"] == [1 << l1, 1 << l2] and t["blocks_per_sm"] == minb and t["stages"] == st
+    fwd = run(unit, x, batch, direction=0)
+    back = run(unit, fwd, batch, direction=1)
+    unit.status()
+    tol = TOL[NPD[dtype]]
+    want = np.fft.fft(z, axis=-1)
+    assert rel_l2(O.unpack(fwd, n, p), want) < tol
+    assert rel_l2(O.unpack(back, n, p), z) < tol
+
+
+def test_set_tuning_rejects_unbuilt_variant():
+    unit = fft_unit(1 << 16)
+    with pytest.raises(NotImplementedError):
+        unit.set_tuning("one-launch four-step", split=(1024, 64), blocks_per_sm=1, stages=3)
 
 
 def test_tune_small_size_has_one_form():
