@@ -2,6 +2,8 @@
 #include "pcx_fs_launch.cuh"
 
 PCX_FS_PART(pcx_fs_part0) {
+    PCX_FS_VARIANT(float, 7, 6, 2, 3)
+    PCX_FS_VARIANT(float, 6, 7, 2, 3)
     PCX_FS_VARIANT(float, 7, 7, 2, 3)
     PCX_FS_VARIANT(float, 7, 7, 1, 3)
     PCX_FS_VARIANT(float, 8, 7, 2, 3)

@@ -67,6 +67,7 @@ struct fs_variant {
 // fastest one measured on a B200 on 512 MB batches; at 2^15 and 2^17..2^19 an
 // uneven split with the longer sub-transform in the row pass is fastest).
 constexpr fs_variant kFsVariantsF32[] = {
+    {7, 6, 2, 3},  {6, 7, 2, 3},                                      // 2^13 (beside the one-pass form)
     {7, 7, 2, 3},  {7, 7, 1, 3},                                      // 2^14
     {7, 8, 2, 3},  {8, 7, 2, 3},                                      // 2^15
     {8, 8, 2, 3},  {8, 8, 1, 3},  {7, 9, 2, 3},  {9, 7, 2, 3},        // 2^16

@@ -298,6 +298,12 @@ def test_one_launch_four_step_matches_chunked(log_n, batch, dtype, monkeypatch):
     z = normal_cx(rng, batch, n)
     x = O.pack(z, p, NPD[dtype])
     unit = fft_unit(n, dtype=dtype)
+    # the chunked passes use the plan's own split (the longer sub-transform
+    # first); the one-launch kernel is pinned to a variant of that split, so
+    # the arithmetic is the same
+    l1, l2 = (log_n + 1) // 2, log_n // 2
+    v = next(v for v in _variants() if v[0] == dtype and v[1:3] == (l1, l2))
+    unit.set_tuning("one-launch four-step", split=(1 << l1, 1 << l2), blocks_per_sm=v[3], stages=v[4])
     outs = {}
     for mode in ("chunked", "one-launch"):
         if mode == "chunked":
