@@ -155,8 +155,9 @@ template<int LOGN>
 int init_xc2(pcx_fxcorr_s* h) {
     using C         = xc2_cfg<LOGN>;
     int e1 = 0, e2 = 0;
-    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN1, nullptr, false, 0, &e1));
-    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN2, nullptr, false, 0, &e2));
+    // full stage tables of the two sub-transforms (one entry per twiddle)
+    PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN1, nullptr, false, 0, &e1));
+    PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN2, nullptr, false, 0, &e2));
     e1                  = (e1 + 1) / 2 * 2;    // 16-byte sections
     e2                  = (e2 + 1) / 2 * 2;
     const size_t ntw    = (size_t)C::NB + C::N2 + C::N1;
@@ -169,8 +170,8 @@ int init_xc2(pcx_fxcorr_s* h) {
     auto* tws    = s2 + e2;
     k_perm_spectrum<<<(C::N + 255) / 256, 256>>>(static_cast<const cpx<float>*>(h->kspec), kp, C::LOGN1, C::LOGN2);
     PCX_CUDA_TRY(cudaGetLastError());
-    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN1, s1, false, 0, &e1));
-    PCX_CUDA_TRY(pcx_v2_stage_twiddles(C::LOGN2, s2, false, 0, &e2));
+    PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN1, s1, false, 0, &e1));
+    PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN2, s2, false, 0, &e2));
     PCX_CUDA_TRY(pcx_gen_twiddles(tws, C::NB, LOGN, 1, false, 0));
     PCX_CUDA_TRY(pcx_gen_twiddles(tws + C::NB, C::N2, LOGN, C::TT1, false, 0));
     PCX_CUDA_TRY(pcx_gen_twiddles(tws + C::NB + C::N2, C::N1, LOGN, C::TT2, false, 0));

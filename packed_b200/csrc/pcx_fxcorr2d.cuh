@@ -55,8 +55,8 @@ struct xc2_cfg {
     using X1                   = xch_blocked<N1, G1>;
     using X2                   = xch_blocked<N2, G2>;
     static constexpr int XB    = (X1::size > X2::size ? X1::size : X2::size) * 8;
-    static constexpr int TB1   = stage_tw_smem_bytes<P1, float>();
-    static constexpr int TB2   = stage_tw_smem_bytes<P2, float>();
+    static constexpr int TB1   = smem_align16(fs_full_tw_size<P1>() * 8);    // full stage tables
+    static constexpr int TB2   = smem_align16(fs_full_tw_size<P2>() * 8);
     static constexpr int NB    = N / 16;      // W_N^e, e < N/16 (= TT1*N2 = TT2*N1)
     static constexpr int SMEM  = WIN + XB + TB1 + TB2 + (NB + N2 + N1) * 8;
     static_assert(P1::E == 16 && P2::E == 16, "16 points per thread");
@@ -106,8 +106,8 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
     const cpx<float>*    kp   = reinterpret_cast<const cpx<float>*>(A.kperm);
 
     // constant tables into shared memory
-    stage_tw_to_smem<P1, float>(tw1, A.stw1, tid, NT);
-    stage_tw_to_smem<P2, float>(tw2, A.stw2, tid, NT);
+    copy_table_to_smem<F::TB1>(tw1, A.stw1, tid, NT);
+    copy_table_to_smem<F::TB2>(tw2, A.stw2, tid, NT);
     for (int i = tid; i < (F::NB + N2 + N1) / 2; i += NT) {
         reinterpret_cast<uint4*>(fwb)[i] = __ldg(reinterpret_cast<const uint4*>(A.tws) + i);
     }
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                     v[i]            = win[(t + i * TT1) * RS + n2];
                 });
                 stage_compute_tab<P1, 0>(v, t, tw1);
-                run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
                 apply_fourstep_tw(v, fwb[t * n2], fwu1[n2], [&](auto ic, cpx<float> o) {
                     constexpr int i              = decltype(ic)::value;
                     win[(t + i * TT1) * RS + n2] = o;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                     v[i]            = win[k1 * RS + t + i * TT2];
                 });
                 stage_compute_tab<P2, 0>(v, t, tw2);
-                run_stages_tab<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+                run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
                 // v[i] = X[k1 + N1*k2], k2 = t + i*TT2: conj(X * conj(K)) or conj(X * K)
                 static_for<E>([&](auto ic) {
                     constexpr int    i = decltype(ic)::value;
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                     v[i]               = a.conj_kernel ? cmul(c, k) : cmulc(c, k);
                 });
                 stage_compute_tab<P2, 0>(v, t, tw2);
-                run_stages_tab<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+                run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
                 // v[i] at n2 = t + i*TT2, times W_N^(k1*n2) = W_N^(k1*t) * W_N^(TT2*k1)^i
                 apply_fourstep_tw(v, fwb[k1 * t], fwu2[k1], [&](auto ic, cpx<float> o) {
                     constexpr int i           = decltype(ic)::value;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                     if (tid < 32) claim_and_copy();
                 }
                 stage_compute_tab<P1, 0>(v, t, tw1);
-                run_stages_tab<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
                 float* drow = d + 2 * t * N2 + ((n2 >> 3) << 4) + (n2 & 7);
                 static_for<E>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;

@@ -2,34 +2,55 @@
 // correlations, all in ONE persistent launch fed by a device work queue and
 // replayed from a CUDA graph.
 //
-// Work items (built once on the host, executed in queue order; every CTA
-// claims the next item with an atomic counter):
-//   SINGLE  up to M whole transforms of one size N <= 4096
-//   COL     one column tile of a four-step transform (N = 2^13..2^18): writes
-//           the transform's scratch slot, then counts itself in col_done[t]
+// Work items (built once on the host, claimed in queue order from a device
+// counter):
+//   SINGLE  M whole transforms of one size N <= 4096 (M rows of 16 points per
+//           thread fill the block)
+//   COL     one column tile of a four-step transform (N = 2^13..2^18): TMA copy
+//           of the tile through the transform's own tensor map, column FFTs,
+//           four-step twiddle, written to the transform's scratch slot, then
+//           counted in col_done[t]
 //   ROW     one row tile: waits until col_done[t] reaches the column-tile
-//           count, reads the slot (through L2: slots are reused inside the
-//           launch, so L1 must not serve them), counts itself in row_done[t]
+//           count, bulk-copies the slot rows, row FFTs, natural-order output,
+//           counted in row_done[t] once its rows have landed
 //   XC      up to M consecutive overlap-save blocks of one correlation
-// Scratch slots form a ring; a COL tile first waits until the transform that
-// last used its slot has finished all its ROW tiles.  Every wait is on an item
-// that sits earlier in the queue, so it was claimed earlier by a resident CTA
-// that never waits on a later item: the waits always end.  They are still
-// bounded (about one second); on timeout the CTA records an error and leaves.
+// Each block has NT compute threads and, as the one-launch four-step kernel
+// does, a producer warp and a publisher warp: the producer claims the next
+// item, waits for its dependency (a scratch slot freed by an earlier
+// transform's row tiles, or a transform's column tiles) and issues its
+// copies into a three-stage shared-memory ring, so two items are in flight
+// while one is computed; the publisher counts completions as soon as they
+// happen and never waits on another block.  Every size runs its own
+// compile-time geometry; the exchanges of the sub-transforms run in place in
+// the item's stage.  Correlation items (last in the queue) read their windows
+// with plain loads and use the whole ring as workspace, so the producer drains
+// the ring around them.  Every wait is on an item earlier in the queue,
+// claimed by a resident block whose publisher never waits on a later item:
+// the waits always end.  They are still bounded (about one second); on
+// timeout the block records an error and leaves.
 #include "pcx_fft_v2.cuh"
+#include "pcx_fourstep.cuh"
 #include "pcx_fxcorr_kernels.cuh"
 #include "pcx_host.hpp"
+#include "pcx_v2_launch.cuh"
 
 #include <algorithm>
 #include <map>
+#include <string>
 #include <vector>
 
 namespace pcxg {
 namespace rg {
 
-constexpr int NT     = 512;
-constexpr int LPK    = 3;    // pack 8 (complex64)
-constexpr int MAXLG  = 32;
+constexpr int NT    = 512;    // compute threads; then the producer warp, then the publisher warp
+constexpr int NW    = NT / 32;
+constexpr int ST    = 3;      // ring stages
+constexpr int LPK   = 3;      // pack 8 (complex64)
+constexpr int MAXLG = 32;
+// A stage holds a 64 KB tile (plus row padding) or the item's in-place
+// exchange buffer (one padding slot per 16 elements): 68 KB at every size.
+constexpr int STAGE = 69632;
+constexpr int SMEM  = ST * STAGE;
 
 enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3 };
 
@@ -39,9 +60,10 @@ struct item {
 struct fft_req {
     const float* src;
     float*       dst;
-    int          slot;        // four-step scratch slot
+    int          slot;        // four-step scratch slot (in the size's own ring)
     int          prev;        // transform that used the slot before (-1 none)
     int          prev_rows;   // row tiles of that transform (its completion count)
+    int          tmap;        // its column-tile tensor map (four-step sizes)
 };
 struct xc_req {
     const float*      src;
@@ -51,71 +73,120 @@ struct xc_req {
     const cpx<float>* kspec;
 };
 struct tabs {
-    const cpx<float>* stw[MAXLG];     // single-pass stage twiddles (lg <= 12)
-    const cpx<float>* stw1[MAXLG];    // four-step: column stage twiddles (per total lg)
-    const cpx<float>* stw2[MAXLG];
-    const cpx<float>* thi[MAXLG];
-    const cpx<float>* tlo[MAXLG];
-    const cpx<float>* tb[MAXLG];
+    const cpx<float>* stw[MAXLG];     // single pass: stage factor tables (lg <= 12)
+    const cpx<float>* fst1[MAXLG];    // four-step (per total lg): full stage tables of the N1 / N2 sub-transforms
+    const cpx<float>* fst2[MAXLG];
+    const cpx<float>* thi[MAXLG];     // W_N^(i*N2), i < N1
+    const cpx<float>* tlo[MAXLG];     // W_N^i, i < N2
+    const cpx<float>* tb[MAXLG];      // W_{16*N2}^i, i < N2
+    cpx<float>*       scratch[MAXLG]; // the size's ring of scratch slots
     const cpx<float>* xtw[MAXLG];     // correlator W_N table
 };
 struct args {
-    const item*    items;
-    int            nitems;
-    const fft_req* req;
-    const xc_req*  xreq;
-    int*           col_done;
-    int*           row_done;
-    int            col_tiles[MAXLG];
-    int            row_tiles[MAXLG];
-    cpx<float>*    scratch;
-    long long      slot_elems;
-    unsigned*      counter;
-    int*           error;
-    int            conj;     // inverse: conjugate in and out
-    float          scale;
-    tabs           tb;
+    const item*        items;
+    int                nitems;
+    const fft_req*     req;
+    const xc_req*      xreq;
+    const CUtensorMap* tmaps;
+    int*               col_done;
+    int*               row_done;
+    int                col_tiles[MAXLG];
+    int                row_tiles[MAXLG];
+    unsigned*          counter;
+    int*               error;
+    int                conj;     // inverse: conjugate in and out
+    float              scale;
+    tabs               tb;
 };
 
-__device__ __forceinline__ bool wait_count(const int* p, int target) {
-    if (*reinterpret_cast<const volatile int*>(p) >= target) return true;
-    const unsigned long long t0 = timer_ns();
-    while (true) {
-        int v;
-        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-        if (v >= target) return true;
-        if (timer_ns() - t0 > 1000000000ull) return false;
-        __nanosleep(128);
-    }
+// Geometry of the four-step sizes: N = N1*N2 with N1 = 2^((lg+1)/2), tiles of
+// 8192 elements over NT threads of 16 points.
+template<int L1, int L2>
+struct fsg {
+    static constexpr int N1 = 1 << L1, N2 = 1 << L2;
+    using P1                = splan<L1>;
+    using P2                = splan<L2>;
+    static constexpr int C   = NT / P1::TT;    // columns per column tile
+    static constexpr int CR  = NT / P2::TT;    // rows per row tile
+    static constexpr int SEG = 2 * C;          // reals per tile row (packed, pack 8)
+    static constexpr int RSI = N2 + 2;         // padded row of a row tile (complex)
+    static constexpr int BOXY = N1 < 256 ? N1 : 256;
+    using X1 = xch_interleaved<N1, C>;
+    using X2 = xch_grouped<N2, CR, 8>;
+    static_assert(C >= 8 && CR >= 8 && CR % 8 == 0, "tiles span whole 32-byte sectors");
+    static_assert(N1 * SEG * 4 <= STAGE && CR * RSI * 8 <= STAGE, "tile fits a stage");
+    static_assert(X1::size * 8 <= STAGE && X2::size * 8 <= STAGE, "exchange fits a stage");
+    static_assert(2 * C <= 256, "TMA box width");
+};
+// Whole transforms of N = 2^LOGL <= 4096: M rows of RS reals.
+template<int LOGL>
+struct sgg {
+    using P                 = splan<LOGL>;
+    static constexpr int L  = P::L;
+    static constexpr int TT = P::TT;
+    static constexpr int M  = NT / TT;
+    static constexpr int RS = 2 * L + single3_pad<TT>();
+    using X                 = xch_blocked<L, M>;
+    static_assert(M * RS * 4 <= STAGE && X::size * 8 <= STAGE, "rows and exchange fit a stage");
+};
+
+// Stages of a correlation block through the whole ring, named barrier over
+// the compute threads (the general kernels' run_stages with barrier BARN).
+template<class P, class X, class T, int E>
+__device__ __forceinline__ void run_stages_nb(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
+                                              const cpx<T>* __restrict__ twL) {
+    static_for<P::NST - 1>([&](auto sc) {
+        constexpr int S = decltype(sc)::value;
+        constexpr int G = E / (1 << P::rbits(S));
+        xch_sync<NT>();
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int g = i % G, j = i / G;
+            xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
+        });
+        xch_sync<NT>();
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = xch[X::idx(m, t + i * P::TT)];
+        });
+        stage_compute<P, S + 1>(v, t, twL);
+    });
 }
 
+// ---------------------------------------------------------------- compute
+// Each returns false when a give-up vote made every compute thread leave.
+// They are not inlined: every size and kind is allocated its registers on its
+// own instead of all of them sharing one allocation across the dispatch.
 template<int LOGL>
-__device__ void single_items(const args& A, const item& it, cpx<float>* xch) {
-    using P          = splan<LOGL>;
+__device__ __noinline__ bool single_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
+                                          uint64_t* empty_bar) {
+    using G          = sgg<LOGL>;
+    using P          = typename G::P;
     constexpr int E  = P::E;
-    constexpr int TT = P::TT;
-    constexpr int M  = NT / TT;
-    using X          = xch_blocked<P::L, M>;
-    const int  tid  = threadIdx.x;
-    const int  m    = tid / TT;
-    const int  t    = tid - m * TT;
-    const bool live = m < it.b;
-    const fft_req& r = A.req[it.a + (live ? m : 0)];
-    const float*   s = r.src;
-    float*         d = r.dst;
-    const auto*    stw = A.tb.stw[LOGL];
-    cpx<float>     v[E];
-    // element t + i*TT; its packed offset splits into base + constant only
-    // when TT is a multiple of the pack width
+    constexpr int TT = G::TT;
+    constexpr int SW = TT >= 32 ? 16 : 0;
+    const int     m  = tid / TT;
+    const int     t  = tid - m * TT;
+    const float*  in = reinterpret_cast<const float*>(buf);
+    const auto*   stw = A.tb.stw[LOGL];
+    cpx<float>    v[E];
     static_for<E>([&](auto ic) {
-        constexpr int i  = decltype(ic)::value;
-        const int     o  = pk<LPK>(t + i * TT);
-        const float   re = s[o], im = s[o + 8];
-        v[i]             = {re, A.conj ? -im : im};
+        constexpr int    i = decltype(ic)::value;
+        const cpx<float> x = lds_swapped<float, SW>(in, m * G::RS + pk<LPK>(t + i * TT), 8);
+        v[i]               = {x.re, A.conj ? -x.im : x.im};
     });
     stage_compute_tab<P, 0>(v, t, stw);
-    run_stages_tab<P, X>(v, xch, m, t, stw);
-    if (live) {
+    // the exchanges run in place in the stage: the first (block-wide) barrier
+    // also votes on `bad`
+    if (bar1_any<NT>(bad)) return false;
+    run_stages_tab<P, typename G::X, false, NT>(v, reinterpret_cast<cpx<float>*>(buf), m, t, stw);
+    fence_proxy_async_smem();    // the stage is read: it may be refilled
+    __syncwarp();
+    if (tid % 32 == 0) mbar_arrive(empty_bar);
+    if (m < it.b) {
+        // element t + i*TT; its packed offset splits into a base and a
+        // constant only when TT is a multiple of the pack width
+        float*      d  = A.req[it.a + m].dst;
         const float sc = A.scale, sim = A.conj ? -A.scale : A.scale;
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
@@ -124,103 +195,95 @@ __device__ void single_items(const args& A, const item& it, cpx<float>* xch) {
             d[o + 8]        = v[i].im * sim;
         });
     }
+    return true;
 }
 
-template<int L1, int L2>
-__device__ bool col_item(const args& A, const item& it, cpx<float>* xch, int* s_flag) {
-    using P           = splan<L1>;
-    constexpr int N2  = 1 << L2;
-    constexpr int E   = P::E;
-    constexpr int TT  = P::TT;
-    constexpr int C   = (8192 >> L1) > 8 ? (8192 >> L1) : 8;
-    static_assert(NT == C * TT, "threads");
-    using X           = xch_interleaved<P::L, C>;
-    const int       tid = threadIdx.x;
-    const int       c   = tid % C;
-    const int       t   = tid / C;
-    const fft_req&  r   = A.req[it.a];
-    if (tid == 0) {
-        // the slot is free once the previous user finished all its row tiles
-        *s_flag = r.prev < 0 || wait_count(A.row_done + r.prev, r.prev_rows);
+// The stage is free once this returns true (the caller releases it); the
+// scratch stores wait for `slot_ready`.
+template<int L1, int L2, class SlotWait>
+__device__ __noinline__ bool col_item(const args& A, const item& it, unsigned char* buf, bool& bad, int tid, SlotWait&& slot_ready,
+                         uint64_t* empty_bar) {
+    using F          = fsg<L1, L2>;
+    using P1         = typename F::P1;
+    constexpr int E  = P1::E;
+    constexpr int TT = P1::TT;
+    constexpr int C  = F::C;
+    constexpr int N2 = F::N2;
+    const int     c  = tid % C;
+    const int     t  = tid / C;
+    const int     n2 = it.b * C + c;
+    const fft_req& r = A.req[it.a];
+    // four-step twiddle inputs, used after the stages
+    const uint32_t   e0 = (uint32_t)t * (uint32_t)n2;
+    const cpx<float> th = ldg_cpx(A.tb.thi[L1 + L2] + (e0 >> L2));
+    const cpx<float> tl = ldg_cpx(A.tb.tlo[L1 + L2] + (e0 & (N2 - 1)));
+    const cpx<float> tu = ldg_cpx(A.tb.tb[L1 + L2] + n2);
+    const float*     in = reinterpret_cast<const float*>(buf);
+    cpx<float>       v[E];
+    static_for<E>([&](auto ic) {
+        constexpr int    i = decltype(ic)::value;
+        const cpx<float> x = lds_swapped<float, 16>(in, (t + i * TT) * F::SEG + pk<LPK>(c), 8);
+        v[i]               = {x.re, A.conj ? -x.im : x.im};
+    });
+    const auto* fst = A.tb.fst1[L1 + L2];
+    stage_compute_tab<P1, 0>(v, t, fst);
+    if (run_stages_full<P1, typename F::X1, false, NT>(v, reinterpret_cast<cpx<float>*>(buf), c, t, fst, bad)) {
+        return false;
     }
-    __syncthreads();
-    if (!*s_flag) return false;
-    const int    c0  = it.b * C;
-    const int    n2  = c0 + c;
-    const float* src = r.src + pk<LPK>(t * N2 + n2);
-    cpx<float>   v[E];
-    static_for<E>([&](auto ic) {
-        constexpr int i  = decltype(ic)::value;
-        const float   re = src[2 * i * TT * N2], im = src[2 * i * TT * N2 + 8];
-        v[i]            = {re, A.conj ? -im : im};
-    });
-    const auto* stw = A.tb.stw1[L1 + L2];
-    stage_compute_tab<P, 0>(v, t, stw);
-    run_stages_tab<P, X>(v, xch, c, t, stw);
-    const uint32_t   e0   = (uint32_t)t * (uint32_t)n2;
-    const cpx<float> base = cmul(ldg_cpx(A.tb.thi[L1 + L2] + (e0 >> L2)), ldg_cpx(A.tb.tlo[L1 + L2] + (e0 & (N2 - 1))));
-    cpx<float>       bp[16];
-    powers16(ldg_cpx(A.tb.tb[L1 + L2] + n2), bp);
-    cpx<float>* dst = A.scratch + (long long)r.slot * A.slot_elems + (long long)t * N2 + n2;
-    static_for<E>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        cpx<float>    w = base;
-        if constexpr (i > 0) w = cmul(base, bp[i]);
-        const cpx<float> o = cmul(v[i], w);
-        __stcg(reinterpret_cast<float2*>(dst + (long long)i * TT * N2), make_float2(o.re, o.im));
-    });
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) atomicAdd(A.col_done + it.a, 1);
+    // the stage is read: let the producer refill it while the tile is stored
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (tid % 32 == 0) mbar_arrive(empty_bar);
+    if (!slot_ready()) bad = true;
+    if (!bad) {
+        cpx<float>* dst = A.tb.scratch[L1 + L2] + (long long)r.slot * (F::N1 * N2) + (long long)t * N2 + n2;
+        apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<float> o) {
+            constexpr int i             = decltype(ic)::value;
+            dst[(long long)i * TT * N2] = o;
+        });
+    }
     return true;
 }
 
 template<int L1, int L2>
-__device__ bool row_item(const args& A, const item& it, cpx<float>* xch, int* s_flag) {
-    using P           = splan<L2>;
-    constexpr int N1  = 1 << L1;
-    constexpr int N2  = P::L;
-    constexpr int E   = P::E;
-    constexpr int TT  = P::TT;
-    constexpr int G8  = 8;
-    constexpr int CR  = (8192 >> L2) > 8 ? (8192 >> L2) : 8;
-    static_assert(NT == CR * TT, "threads");
-    using X           = xch_grouped<N2, CR, G8>;
-    const int      tid = threadIdx.x;
-    const int      mlo = tid % G8;
-    const int      t   = (tid / G8) % TT;
-    const int      mhi = tid / (G8 * TT);
-    const int      m   = mhi * G8 + mlo;
-    const fft_req& r   = A.req[it.a];
-    if (tid == 0) *s_flag = wait_count(A.col_done + it.a, A.col_tiles[L1 + L2]);
-    __syncthreads();
-    if (!*s_flag) return false;
-    const int          k1  = it.b * CR + m;
-    const cpx<float>*  src = A.scratch + (long long)r.slot * A.slot_elems + (long long)k1 * N2 + t;
-    cpx<float>         v[E];
+__device__ __noinline__ bool row_item(const args& A, const item& it, unsigned char* buf, bool bad, int tid, uint64_t* empty_bar) {
+    using F          = fsg<L1, L2>;
+    using P2         = typename F::P2;
+    constexpr int E  = P2::E;
+    constexpr int TT = P2::TT;
+    constexpr int N1 = F::N1;
+    const int     mlo = tid % 8;
+    const int     t   = (tid / 8) % TT;
+    const int     mhi = tid / (8 * TT);
+    const int     m   = mhi * 8 + mlo;
+    const int     k1  = it.b * F::CR + m;
+    const cpx<float>* in = reinterpret_cast<const cpx<float>*>(buf) + m * F::RSI + t;
+    cpx<float>        v[E];
     static_for<E>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        const float2  x = __ldcg(reinterpret_cast<const float2*>(src + i * TT));
-        v[i]            = {x.x, x.y};
+        v[i]            = in[i * TT];
     });
-    const auto* stw = A.tb.stw2[L1 + L2];
-    stage_compute_tab<P, 0>(v, t, stw);
-    run_stages_tab<P, X>(v, xch, m, t, stw);
-    float*      dst = r.dst + pk<LPK>(t * N1 + k1);
+    const auto* fst = A.tb.fst2[L1 + L2];
+    stage_compute_tab<P2, 0>(v, t, fst);
+    if (run_stages_full<P2, typename F::X2, false, NT>(v, reinterpret_cast<cpx<float>*>(buf), m, t, fst, bad)) {
+        return false;
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (tid % 32 == 0) mbar_arrive(empty_bar);
+    float*      dst = A.req[it.a].dst + pk<LPK>(t * N1 + k1);
     const float sc = A.scale, sim = A.conj ? -A.scale : A.scale;
     static_for<E>([&](auto ic) {
-        constexpr int i          = decltype(ic)::value;
-        dst[2 * i * TT * N1]     = v[i].re * sc;
-        dst[2 * i * TT * N1 + 8] = v[i].im * sim;
+        constexpr int i = decltype(ic)::value;
+        __stcs(dst + 2 * i * TT * N1, v[i].re * sc);
+        __stcs(dst + 2 * i * TT * N1 + 8, v[i].im * sim);
     });
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) atomicAdd(A.row_done + it.a, 1);
     return true;
 }
 
+// Up to M overlap-save blocks of one correlation; buf is the whole ring.
 template<int LOGN>
-__device__ void xc_items(const args& A, const item& it, cpx<float>* buf) {
+__device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>* buf, int tid) {
     constexpr int EPT = LOGN >= 14 ? 32 : 16;
     using P           = splan<LOGN, EPT>;
     constexpr int L   = P::L;
@@ -228,8 +291,8 @@ __device__ void xc_items(const args& A, const item& it, cpx<float>* buf) {
     constexpr int TT  = P::TT;
     constexpr int M   = NT / TT;
     using X           = xch_blocked<L, M>;
+    static_assert(X::size * 8 <= SMEM, "correlation workspace fits the ring");
     const xc_req& q   = A.xreq[it.a];
-    const int     tid = threadIdx.x;
     const int     m   = tid / TT;
     const int     t   = tid - m * TT;
     // load M windows (blocks b .. b+count-1), zero outside the signal
@@ -243,7 +306,7 @@ __device__ void xc_items(const args& A, const item& it, cpx<float>* buf) {
         }
         buf[e] = w;
     }
-    __syncthreads();
+    xch_sync<NT>();
     const cpx<float>* tw = A.tb.xtw[LOGN];
     cpx<float>        v[E];
     static_for<E>([&](auto ic) {
@@ -251,14 +314,14 @@ __device__ void xc_items(const args& A, const item& it, cpx<float>* buf) {
         v[i]            = buf[m * L + t + i * TT];
     });
     stage_compute<P, 0>(v, t, tw);
-    run_stages<P, X>(v, buf, m, t, tw);
+    run_stages_nb<P, X>(v, buf, m, t, tw);
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
         const cpx<float> k = ldg_cpx(q.kspec + t + i * TT);
         v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
     });
     stage_compute<P, 0>(v, t, tw);
-    run_stages<P, X>(v, buf, m, t, tw);
+    run_stages_nb<P, X>(v, buf, m, t, tw);
     if (m < it.c) {
         const long long b0 = (long long)(it.b + m) * q.step;
         static_for<E>([&](auto ic) {
@@ -272,61 +335,301 @@ __device__ void xc_items(const args& A, const item& it, cpx<float>* buf) {
             }
         });
     }
-    __syncthreads();
+    xch_sync<NT>();    // the ring is read: it may be refilled
 }
 
-__global__ void __launch_bounds__(NT, 1) k_ragged(args A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    cpx<float>*       buf = reinterpret_cast<cpx<float>*>(smem);
-    __shared__ int    s_item;
-    __shared__ int    s_flag;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = (int)atomicAdd(A.counter, 1u);
-        __syncthreads();
-        const int idx = s_item;
-        if (idx >= A.nitems) break;
-        const item it = A.items[idx];
-        bool       ok = true;
-        switch (it.kind * 64 + it.lg) {
-        case K_SINGLE * 64 + 5: single_items<5>(A, it, buf); break;
-        case K_SINGLE * 64 + 6: single_items<6>(A, it, buf); break;
-        case K_SINGLE * 64 + 7: single_items<7>(A, it, buf); break;
-        case K_SINGLE * 64 + 8: single_items<8>(A, it, buf); break;
-        case K_SINGLE * 64 + 9: single_items<9>(A, it, buf); break;
-        case K_SINGLE * 64 + 10: single_items<10>(A, it, buf); break;
-        case K_SINGLE * 64 + 11: single_items<11>(A, it, buf); break;
-        case K_SINGLE * 64 + 12: single_items<12>(A, it, buf); break;
-        case K_COL * 64 + 13: ok = col_item<7, 6>(A, it, buf, &s_flag); break;
-        case K_COL * 64 + 14: ok = col_item<7, 7>(A, it, buf, &s_flag); break;
-        case K_COL * 64 + 15: ok = col_item<8, 7>(A, it, buf, &s_flag); break;
-        case K_COL * 64 + 16: ok = col_item<8, 8>(A, it, buf, &s_flag); break;
-        case K_COL * 64 + 17: ok = col_item<9, 8>(A, it, buf, &s_flag); break;
-        case K_COL * 64 + 18: ok = col_item<9, 9>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 13: ok = row_item<7, 6>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 14: ok = row_item<7, 7>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 15: ok = row_item<8, 7>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 16: ok = row_item<8, 8>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 17: ok = row_item<9, 8>(A, it, buf, &s_flag); break;
-        case K_ROW * 64 + 18: ok = row_item<9, 9>(A, it, buf, &s_flag); break;
-        case K_XC * 64 + 7: xc_items<7>(A, it, buf); break;
-        case K_XC * 64 + 8: xc_items<8>(A, it, buf); break;
-        case K_XC * 64 + 9: xc_items<9>(A, it, buf); break;
-        case K_XC * 64 + 10: xc_items<10>(A, it, buf); break;
-        case K_XC * 64 + 11: xc_items<11>(A, it, buf); break;
-        case K_XC * 64 + 12: xc_items<12>(A, it, buf); break;
-        case K_XC * 64 + 13: xc_items<13>(A, it, buf); break;
-        case K_XC * 64 + 14: xc_items<14>(A, it, buf); break;
-        default: ok = false; break;
-        }
-        if (!ok) {
-            if (threadIdx.x == 0) atomicExch(A.error, 1);
-            return;
-        }
-        __syncthreads();
+// ---------------------------------------------------------------- producer
+// Bytes and copies of an item into stage `buf` (lane 0 registers the bytes
+// on `bar` first; the lanes issue the copies).  XC items copy nothing.
+template<int L1, int L2>
+__device__ void issue_col(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane, uint64_t pol) {
+    using F = fsg<L1, L2>;
+    if (lane == 0) {
+        mbar_arrive_expect_tx(bar, F::N1 * F::SEG * 4);
+        const CUtensorMap* map = A.tmaps + A.req[it.a].tmap;
+#pragma unroll
+        for (int y = 0; y < F::N1; y += F::BOXY) tma_load_3d_hint(buf + y * F::SEG * 4, map, 2 * it.b * F::C, y, 0, bar, pol);
+    }
+}
+template<int L1, int L2>
+__device__ void issue_row(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    using F = fsg<L1, L2>;
+    if (lane == 0) {
+        fence_proxy_async_global();    // other blocks' column stores -> TMA reads
+        mbar_arrive_expect_tx(bar, F::CR * F::N2 * 8);
+    }
+    __syncwarp();
+    const cpx<float>* g = A.tb.scratch[L1 + L2] + (long long)A.req[it.a].slot * (F::N1 * F::N2) +
+                          (long long)it.b * F::CR * F::N2;
+    for (int q = lane; q < F::CR; q += 32) {
+        bulk_g2s(reinterpret_cast<cpx<float>*>(buf) + q * F::RSI, g + (long long)q * F::N2, F::N2 * 8, bar);
+    }
+}
+template<int LOGL>
+__device__ void issue_single(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    using G = sgg<LOGL>;
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)it.b * G::L * 8);
+    __syncwarp();
+    for (int q = lane; q < it.b; q += 32) {
+        bulk_g2s(reinterpret_cast<float*>(buf) + q * G::RS, A.req[it.a + q].src, G::L * 8, bar);
     }
 }
 
-constexpr int SMEM = xch_blocked<16384, 1>::size * (int)sizeof(cpx<float>);    // largest user: 16384-point correlation
+#define PCX_RG_FOURSTEP(X) X(13, 7, 6) X(14, 7, 7) X(15, 8, 7) X(16, 8, 8) X(17, 9, 8) X(18, 9, 9)
+#define PCX_RG_SINGLE(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+#define PCX_RG_XC(X) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
+
+// The arguments sit in device memory (uploaded once at creation): the item
+// functions take them by reference without a per-thread copy.
+__global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ Ap) {
+    const args& A = *Ap;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t full[ST];      // the item's copies landed (XC: the producer arrived)
+    __shared__ uint64_t empty[ST];     // compute warps done with the stage, publisher past its item
+    __shared__ uint64_t slotok[ST];    // column tile: its scratch slot may be written
+    __shared__ uint64_t written[ST];   // column tile: compute warps wrote the slot
+    __shared__ int      s_item[ST];    // item index in the stage (-1: the queue is exhausted)
+    const int           tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < ST; ++s) {
+            s_item[s] = -2;    // no item yet
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NW + 1);
+            mbar_init(&slotok[s], 1);
+            mbar_init(&written[s], NW);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (tid >= NT + 32) {
+        // ======================= publisher warp
+        const int lane     = tid - NT - 32;
+        int       ncol[ST] = {};
+        for (long long k = 0;; ++k) {
+            const int      s   = (int)(k % ST);
+            const uint32_t par = (uint32_t)((k / ST) & 1);
+            int            ok  = 1;
+            if (lane == 0) ok = mbar_wait_bounded(&full[s], par) ? 1 : 0;
+            if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+            const int idx = s_item[s];
+            if (idx < 0) break;
+            const item it = A.items[idx];
+            if (it.kind == K_COL) {
+                if (lane == 0) ok = mbar_wait_bounded(&written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
+                ++ncol[s];
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    if (lane == 0) atomicExch(A.error, 1);
+                    break;
+                }
+                if (lane == 0) {
+                    fence_proxy_async_global();    // the slot is read back by TMA copies
+                    red_release_add(A.col_done + it.a, 1);
+                }
+            } else if (it.kind == K_ROW) {
+                // the rows are in shared memory: drop their L2 lines unwritten
+                const int   lg   = it.lg;
+                const int   l2   = lg / 2, l1 = lg - l2;
+                const int   cr   = NT / ((1 << l2) / 16);
+                const long long n = 1LL << lg;
+                const char* g    = reinterpret_cast<const char*>(A.tb.scratch[lg] + (long long)A.req[it.a].slot * n +
+                                                                  (long long)it.b * cr * (1LL << l2));
+                const int   lines = cr * (1 << l2) * 8 / 128;
+                for (int q = lane; q < lines; q += 32) l2_discard(g + (size_t)q * 128);
+                (void)l1;
+                __syncwarp();
+                if (lane == 0) red_release_add(A.row_done + it.a, 1);
+            }
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        __syncwarp();
+        return;
+    }
+
+    if (tid >= NT) {
+        // ======================= producer warp
+        const int      lane   = tid - NT;
+        const uint64_t pol    = l2_evict_first_policy();
+        bool           fail   = false;
+        long long      issued = 0;
+        long long      drain_until = -1;    // after an XC item: wait for it before the next item
+        auto           wait_empty = [&](long long q) -> bool {    // stage of item q released
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait_bounded(&empty[(int)(q % ST)], (uint32_t)((q / ST) & 1)) ? 1 : 0;
+            return __shfl_sync(0xffffffffu, ok, 0) != 0;
+        };
+        auto need = [&](const int* ctr, int target) -> bool {
+            int ok = 1;
+            if (lane == 0) ok = fs_wait(ctr, target) ? 1 : 0;
+            return __shfl_sync(0xffffffffu, ok, 0) != 0;
+        };
+        for (long long k = 0; !fail; ++k) {
+            const int s = (int)(k % ST);
+            if (k >= ST && !wait_empty(k - ST)) {
+                fail = true;
+                break;
+            }
+            if (drain_until >= 0 && !wait_empty(drain_until)) {
+                fail = true;
+                break;
+            }
+            drain_until = -1;
+            int idx = 0;
+            if (lane == 0) idx = (int)atomicAdd(A.counter, 1u);
+            idx = __shfl_sync(0xffffffffu, idx, 0);
+            unsigned char* buf = smem + s * STAGE;
+            if (idx >= A.nitems) {
+                if (lane == 0) {
+                    s_item[s] = -1;
+                    mbar_arrive(&full[s]);
+                }
+                issued = k + 1;
+                break;
+            }
+            const item it = A.items[idx];
+            if (lane == 0) s_item[s] = idx;
+            __syncwarp();
+            if (it.kind == K_XC) {
+                // the correlation uses the whole ring: the other stages' items
+                // must be done first, and the next item waits for this one
+                for (long long q = k - 1; q >= 0 && q > k - ST && !fail; --q) {
+                    if (!wait_empty(q)) fail = true;
+                }
+                if (fail) break;
+                if (lane == 0) mbar_arrive(&full[s]);
+                drain_until = k;
+                issued      = k + 1;
+                continue;
+            }
+            if (it.kind == K_SINGLE) {
+                switch (it.lg) {
+#define PCX_RG_ISSUE_S(LG) \
+    case LG: issue_single<LG>(A, it, buf, &full[s], lane); break;
+                    PCX_RG_SINGLE(PCX_RG_ISSUE_S)
+#undef PCX_RG_ISSUE_S
+                default: break;
+                }
+                issued = k + 1;
+            } else if (it.kind == K_COL) {
+                switch (it.lg) {
+#define PCX_RG_ISSUE_C(LG, A1, A2) \
+    case LG: issue_col<A1, A2>(A, it, buf, &full[s], lane, pol); break;
+                    PCX_RG_FOURSTEP(PCX_RG_ISSUE_C)
+#undef PCX_RG_ISSUE_C
+                default: break;
+                }
+                issued = k + 1;
+                // the slot: free once the transform that used it before has
+                // read all its rows
+                const fft_req& r = A.req[it.a];
+                if (r.prev >= 0 && !need(A.row_done + r.prev, r.prev_rows)) {
+                    fail = true;
+                    break;
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&slotok[s]);
+            } else {
+                if (!need(A.col_done + it.a, A.col_tiles[it.lg])) {
+                    fail = true;
+                    break;
+                }
+                switch (it.lg) {
+#define PCX_RG_ISSUE_R(LG, A1, A2) \
+    case LG: issue_row<A1, A2>(A, it, buf, &full[s], lane); break;
+                    PCX_RG_FOURSTEP(PCX_RG_ISSUE_R)
+#undef PCX_RG_ISSUE_R
+                default: break;
+                }
+                issued = k + 1;
+            }
+            __syncwarp();
+        }
+        if (fail && lane == 0) {
+            atomicExch(A.error, 1);
+            for (long long q = issued - 1; q >= 0 && q >= issued - ST; --q) {
+                mbar_wait_bounded(&full[(int)(q % ST)], (uint32_t)((q / ST) & 1), 100000000ull);
+            }
+        }
+        __syncwarp();
+        return;
+    }
+
+    // ======================= compute warps
+    const int lane     = tid % 32;
+    int       ncol[ST] = {};
+    bool      bad      = false;
+    for (long long k = 0;; ++k) {
+        const int      s   = (int)(k % ST);
+        const uint32_t par = (uint32_t)((k / ST) & 1);
+        if (!mbar_wait_bounded(&full[s], par)) {
+            // the producer stopped: go on with whatever the stage holds and
+            // leave at the item's first barrier, which votes
+            bad = true;
+            atomicExch(A.error, 1);
+        }
+        const int idx = s_item[s];
+        if (idx < 0) {
+            // the end of the queue (or nothing to work on after a give-up):
+            // vote, so that every compute thread leaves at the same barrier
+            bar1_any<NT>(true);
+            return;
+        }
+        const item     it  = A.items[idx];
+        unsigned char* buf = smem + s * STAGE;
+        auto release = [&]() {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        };
+        bool alive = true;
+        if (it.kind == K_SINGLE) {
+            switch (it.lg) {
+#define PCX_RG_RUN_S(LG) \
+    case LG: alive = single_items<LG>(A, it, buf, bad, tid, &empty[s]); break;
+                PCX_RG_SINGLE(PCX_RG_RUN_S)
+#undef PCX_RG_RUN_S
+            default: bad = true; break;
+            }
+        } else if (it.kind == K_COL) {
+            auto slot_ready = [&]() -> bool {
+                const bool ok = mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1));
+                ++ncol[s];
+                if (!ok) atomicExch(A.error, 1);
+                return ok;
+            };
+            switch (it.lg) {
+#define PCX_RG_RUN_C(LG, A1, A2) \
+    case LG: alive = col_item<A1, A2>(A, it, buf, bad, tid, slot_ready, &empty[s]); break;
+                PCX_RG_FOURSTEP(PCX_RG_RUN_C)
+#undef PCX_RG_RUN_C
+            default: bad = true; break;
+            }
+            if (alive && !bad) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&written[s]);
+            }
+        } else if (it.kind == K_ROW) {
+            switch (it.lg) {
+#define PCX_RG_RUN_R(LG, A1, A2) \
+    case LG: alive = row_item<A1, A2>(A, it, buf, bad, tid, &empty[s]); break;
+                PCX_RG_FOURSTEP(PCX_RG_RUN_R)
+#undef PCX_RG_RUN_R
+            default: bad = true; break;
+            }
+        } else {
+            if (bar1_any<NT>(bad)) return;
+            switch (it.lg) {
+#define PCX_RG_RUN_X(LG) \
+    case LG: xc_items<LG>(A, it, reinterpret_cast<cpx<float>*>(smem), tid); break;
+                PCX_RG_XC(PCX_RG_RUN_X)
+#undef PCX_RG_RUN_X
+            default: bad = true; break;
+            }
+            release();
+        }
+        if (!alive) return;
+    }
+}
 
 }    // namespace rg
 }    // namespace pcxg
@@ -350,16 +653,19 @@ struct pcx_ragged_s {
 namespace {
 
 template<class V>
-void* upload(pcx_ragged_s* h, const std::vector<V>& v, cudaError_t* e) {
+void* upload(pcx_ragged_s* h, const std::vector<V>& v, cudaError_t* e, size_t align = 0) {
     void* p = nullptr;
-    *e      = cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(V));
+    *e      = cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(V) + align);
     if (*e != cudaSuccess) return nullptr;
     h->allocs.push_back(p);
+    if (align) p = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(p) + align - 1) / align * align);
     if (!v.empty()) *e = cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice);
     return p;
 }
 
 int lg2(size_t n) { return n ? __builtin_ctzll(n) : -1; }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 }    // namespace
 
@@ -387,6 +693,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             return rc;
         };
         cudaError_t e = cudaSuccess;
+        auto cuda_fail = [&](cudaError_t err) { return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(err))); };
         // ---- requests and per-size tables
         std::vector<rg::fft_req> req(n_fft);
         std::map<int, std::vector<int>> by_lg;
@@ -395,7 +702,10 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (lg < 5 || lg > 18 || (sizes[i] & (sizes[i] - 1))) {
                 return fail(pcx_fail(PCX_ERR_UNSUPPORTED, "ragged FFT sizes must be powers of two in 2^5..2^18"));
             }
-            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1, 0};
+            if (!aligned16(src[i]) || !aligned16(dst[i])) {
+                return fail(pcx_fail(PCX_ERR_INVALID, "ragged FFT buffers must be 16-byte aligned"));
+            }
+            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1, 0, -1};
             by_lg[lg].push_back((int)i);
         }
         int sms = 148, dev = 0;
@@ -413,21 +723,38 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             plan_of[lg] = p;
             return p;
         };
+        auto dev_alloc = [&](size_t bytes, void** p) -> cudaError_t {
+            cudaError_t r = cudaMalloc(p, bytes);
+            if (r == cudaSuccess) h->allocs.push_back(*p);
+            return r;
+        };
         for (auto& [lg, idx]: by_lg) {
-            pcx_plan p = get_plan(lg);
-            if (!p) return fail(PCX_ERR_CUDA);
             if (lg <= 12) {
+                pcx_plan p = get_plan(lg);
+                if (!p) return fail(PCX_ERR_CUDA);
                 h->A.tb.stw[lg] = static_cast<const cpx<float>*>(p->stwL);
             } else {
-                h->A.tb.stw1[lg] = static_cast<const cpx<float>*>(p->stw1);
-                h->A.tb.stw2[lg] = static_cast<const cpx<float>*>(p->stw2);
-                h->A.tb.thi[lg]  = static_cast<const cpx<float>*>(p->tw_hi);
-                h->A.tb.tlo[lg]  = static_cast<const cpx<float>*>(p->tw_lo);
-                h->A.tb.tb[lg]   = static_cast<const cpx<float>*>(p->tw_b);
+                // the four-step split (N1 = 2^((lg+1)/2)) and its tables
                 const int l1 = (lg + 1) / 2, l2 = lg / 2;
-                const int c  = std::max(8, 8192 >> l1), cr = std::max(8, 8192 >> l2);
-                h->A.col_tiles[lg] = (1 << l2) / c;
-                h->A.row_tiles[lg] = (1 << l1) / cr;
+                const int n1 = 1 << l1, n2 = 1 << l2;
+                int       f1 = 0, f2 = 0;
+                if ((e = pcx_fourstep_tables(l1, nullptr, false, 0, &f1)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_fourstep_tables(l2, nullptr, false, 0, &f2)) != cudaSuccess) return cuda_fail(e);
+                void* m = nullptr;
+                if ((e = dev_alloc(((size_t)n1 + 2 * (size_t)n2 + f1 + f2) * 8, &m)) != cudaSuccess) return cuda_fail(e);
+                auto* b = static_cast<cpx<float>*>(m);
+                h->A.tb.thi[lg]  = b;
+                h->A.tb.tlo[lg]  = b + n1;
+                h->A.tb.tb[lg]   = b + n1 + n2;
+                h->A.tb.fst1[lg] = b + n1 + 2 * n2;
+                h->A.tb.fst2[lg] = b + n1 + 2 * n2 + f1;
+                if ((e = pcx_gen_twiddles(b, n1, lg, n2, false, 0)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_gen_twiddles(b + n1, n2, lg, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_gen_twiddles(b + n1 + n2, n2, l2 + 4, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_fourstep_tables(l1, b + n1 + 2 * n2, false, 0, &f1)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_fourstep_tables(l2, b + n1 + 2 * n2 + f1, false, 0, &f2)) != cudaSuccess) return cuda_fail(e);
+                h->A.col_tiles[lg] = n2 / (rg::NT / std::max(1, n1 / 16));
+                h->A.row_tiles[lg] = n1 / (rg::NT / std::max(1, n2 / 16));
             }
             if (normalize && direction == PCX_INVERSE) {
                 // one scale per launch: every transform of an inverse batch must share N
@@ -446,8 +773,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             }
             const size_t step = (xc_nfft[j] - (xc_k[j] - 1)) / 8 * 8;
             void*        ks   = nullptr;
-            if ((e = cudaMalloc(&ks, xc_nfft[j] * 8)) != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-            h->allocs.push_back(ks);
+            if ((e = dev_alloc(xc_nfft[j] * 8, &ks)) != cudaSuccess) return cuda_fail(e);
             pcx_plan p = get_plan(lg);
             if (!p) return fail(PCX_ERR_CUDA);
             int rc = pcx_fft_run(p, ks, xc_g[j], xc_k[j], 1, 8, PCX_FORWARD, 0, 1, 2 * xc_nfft[j], 2 * xc_nfft[j], nullptr,
@@ -455,120 +781,150 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (rc) return fail(rc);
             if (!h->A.tb.xtw[lg]) {
                 void* tw = nullptr;
-                if ((e = cudaMalloc(&tw, xc_nfft[j] * 8)) != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-                h->allocs.push_back(tw);
-                if ((e = pcx_gen_twiddles(tw, (int)xc_nfft[j], lg, 1, false, 0)) != cudaSuccess) {
-                    return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-                }
+                if ((e = dev_alloc(xc_nfft[j] * 8, &tw)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_gen_twiddles(tw, (int)xc_nfft[j], lg, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
                 h->A.tb.xtw[lg] = static_cast<const cpx<float>*>(tw);
             }
             xreq[j] = {static_cast<const float*>(xc_src[j]), static_cast<float*>(xc_dst[j]), (long long)xc_len[j],
                        (int)step, (int)((xc_len[j] + step - 1) / step), lg, static_cast<const cpx<float>*>(ks)};
         }
-        // ---- work queue
-        std::vector<rg::item> items;
-        std::vector<rg::item> fill;    // single-pass items and correlation blocks, spread between four-step work
-        for (auto& [lg, idx]: by_lg) {
-            if (lg > 12) continue;
-            const int M = rg::NT / std::max(1, (1 << lg) / 16);    // rows per item: one thread row per 16 points
-            for (size_t q = 0; q < idx.size(); q += M) {
-                // requests of one size are consecutive in idx
-                const int cnt = (int)std::min<size_t>(M, idx.size() - q);
-                fill.push_back({rg::K_SINGLE, lg, idx[q], cnt, 0});
-            }
-        }
-        for (size_t j = 0; j < n_xc; ++j) {
-            const int lg = xreq[j].lg;
-            const int tt = (1 << lg) / (lg >= 14 ? 32 : 16);
-            const int M  = std::max(1, rg::NT / tt);
-            for (int b = 0; b < xreq[j].nblk; b += M) fill.push_back({rg::K_XC, lg, (int)j, b, std::min(M, xreq[j].nblk - b)});
-        }
-        std::vector<int> four;
-        for (auto& [lg, idx]: by_lg)
-            if (lg > 12) four.insert(four.end(), idx.begin(), idx.end());
-        // single-pass requests must be grouped by size with consecutive global indices
+        // ---- requests grouped by size (single-pass items take consecutive requests)
         {
             std::vector<rg::fft_req> sorted;
-            std::vector<int>         order;
-            for (auto& [lg, idx]: by_lg) order.insert(order.end(), idx.begin(), idx.end());
-            std::vector<int> newpos(n_fft);
-            for (size_t q = 0; q < order.size(); ++q) newpos[order[q]] = (int)q;
-            for (int o: order) sorted.push_back(req[o]);
+            for (auto& [lg, idx]: by_lg) {
+                for (int& i: idx) {
+                    sorted.push_back(req[i]);
+                    i = (int)sorted.size() - 1;
+                }
+            }
             req.swap(sorted);
-            for (auto& it: fill)
-                if (it.kind == rg::K_SINGLE) it.a = newpos[it.a];
-            for (auto& f: four) f = newpos[f];
         }
-        const int LAG = 2, NSLOT = 8;
-        size_t    slot_elems = 0;
-        for (auto& [lg, idx]: by_lg)
-            if (lg > 12) slot_elems = std::max<size_t>(slot_elems, size_t(1) << lg);
-        // four-step transforms in queue order with their sizes
-        std::vector<int> four_lg;
-        for (auto& [lg, idx]: by_lg)
-            if (lg > 12) four_lg.insert(four_lg.end(), idx.size(), lg);
-        for (size_t q = 0; q < four.size(); ++q) {
-            req[four[q]].slot = (int)(q % NSLOT);
-            req[four[q]].prev = q >= (size_t)NSLOT ? four[q - NSLOT] : -1;
-            req[four[q]].prev_rows = q >= (size_t)NSLOT ? h->A.row_tiles[four_lg[q - NSLOT]] : 0;
+        // ---- work queue
+        // Single-pass items are spread between the four-step work; the
+        // four-step transforms run in order of size, column tiles of transform
+        // q beside the row tiles of transform q - lag, where the lag covers
+        // about three items per block in flight; correlations come last.
+        const long long in_flight = 3LL * sms * rg::ST / 2;
+        std::vector<rg::item> fill;
+        for (auto& [lg, idx]: by_lg) {
+            if (lg > 12) continue;
+            const int M = rg::NT / std::max(1, (1 << lg) / 16);
+            for (size_t q = 0; q < idx.size(); q += M) {
+                fill.push_back({rg::K_SINGLE, lg, idx[q], (int)std::min<size_t>(M, idx.size() - q), 0});
+            }
         }
-        const size_t nfill = fill.size(), nfour = four.size();
-        size_t       fi    = 0;
-        auto         push_fill = [&](size_t upto) {
-            while (fi < std::min(upto, nfill)) items.push_back(fill[fi++]);
+        std::vector<rg::item> items;
+        std::vector<CUtensorMap> maps;
+        size_t fi = 0, nfour_total = 0;
+        for (auto& [lg, idx]: by_lg)
+            if (lg > 12) nfour_total += idx.size();
+        size_t four_seen = 0;
+        auto push_fill = [&](size_t upto) {
+            while (fi < std::min(upto, fill.size())) items.push_back(fill[fi++]);
         };
-        // column tiles of transform q, row tiles of transform q - LAG, then a
-        // proportional share of the single-pass / correlation items
-        for (size_t q = 0; q < nfour + LAG; ++q) {
-            if (q < nfour) {
-                const int lg = four_lg[q];
-                for (int tile = 0; tile < h->A.col_tiles[lg]; ++tile) items.push_back({rg::K_COL, lg, four[q], tile, 0});
+        for (auto& [lg, idx]: by_lg) {
+            if (lg <= 12) continue;
+            const int       l1 = (lg + 1) / 2, l2 = lg / 2;
+            const int       tc = h->A.col_tiles[lg], tr = h->A.row_tiles[lg];
+            const long long lag = std::max<long long>(1, (in_flight + tc + tr - 1) / (tc + tr));
+            // this size's ring of scratch slots: 2*lag + 2 transforms
+            const size_t nslot = std::min<size_t>(idx.size(), (size_t)(2 * lag + 2));
+            void*        scr   = nullptr;
+            if ((e = dev_alloc(nslot * ((size_t)8 << lg), &scr)) != cudaSuccess) return cuda_fail(e);
+            h->A.tb.scratch[lg] = static_cast<cpx<float>*>(scr);
+            for (size_t q = 0; q < idx.size(); ++q) {
+                rg::fft_req& r = req[idx[q]];
+                r.slot         = (int)(q % nslot);
+                r.prev         = q >= nslot ? idx[q - nslot] : -1;
+                r.prev_rows    = tr;
+                // column tiles read the transform through its own tensor map:
+                // [n1][2*N2 reals], box of 2*C reals x min(N1, 256) rows
+                CUtensorMap      map;
+                const int        c      = rg::NT / std::max(1, (1 << l1) / 16);
+                const cuuint64_t dims[3] = {(cuuint64_t)2 << l2, (cuuint64_t)1 << l1, 1};
+                const cuuint64_t strd[2] = {((cuuint64_t)2 << l2) * 4, ((cuuint64_t)2 << lg) * 4};
+                const cuuint32_t box[3]  = {(cuuint32_t)(2 * c), (cuuint32_t)std::min(1 << l1, 256), 1};
+                const cuuint32_t estr[3] = {1, 1, 1};
+                if ((e = encode_tensor_map(&map, false, 3, const_cast<float*>(r.src), dims, strd, box, estr)) !=
+                    cudaSuccess) {
+                    return cuda_fail(e);
+                }
+                r.tmap = (int)maps.size();
+                maps.push_back(map);
             }
-            if (q >= (size_t)LAG && q - LAG < nfour) {
-                const size_t p  = q - LAG;
-                const int    lg = four_lg[p];
-                for (int tile = 0; tile < h->A.row_tiles[lg]; ++tile) items.push_back({rg::K_ROW, lg, four[p], tile, 0});
+            for (size_t q = 0; q < idx.size() + (size_t)lag; ++q) {
+                if (q < idx.size()) {
+                    for (int tile = 0; tile < tc; ++tile) items.push_back({rg::K_COL, lg, idx[q], tile, 0});
+                }
+                if (q >= (size_t)lag && q - lag < idx.size()) {
+                    for (int tile = 0; tile < tr; ++tile) items.push_back({rg::K_ROW, lg, idx[q - lag], tile, 0});
+                }
+                if (q < idx.size()) ++four_seen;
+                push_fill(nfour_total ? four_seen * fill.size() / nfour_total : fill.size());
             }
-            push_fill(nfour ? (q + 1) * nfill / (nfour + LAG) : nfill);
         }
-        push_fill(nfill);
+        push_fill(fill.size());
+        // correlations last, the longest windows first
+        {
+            std::vector<rg::item> xc_items;
+            for (size_t j = 0; j < n_xc; ++j) {
+                const int lg = xreq[j].lg;
+                const int tt = (1 << lg) / (lg >= 14 ? 32 : 16);
+                const int M  = std::max(1, rg::NT / tt);
+                for (int b = 0; b < xreq[j].nblk; b += M) {
+                    xc_items.push_back({rg::K_XC, lg, (int)j, b, std::min(M, xreq[j].nblk - b)});
+                }
+            }
+            std::stable_sort(xc_items.begin(), xc_items.end(),
+                             [](const rg::item& x, const rg::item& y) { return x.lg > y.lg; });
+            items.insert(items.end(), xc_items.begin(), xc_items.end());
+        }
         h->n_fft   = n_fft;
         h->n_items = items.size();
         // ---- device state
         h->A.items = static_cast<const rg::item*>(upload(h, items, &e));
         if (e == cudaSuccess) h->A.req = static_cast<const rg::fft_req*>(upload(h, req, &e));
         if (e == cudaSuccess) h->A.xreq = static_cast<const rg::xc_req*>(upload(h, xreq, &e));
-        if (e != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-        h->A.nitems     = (int)items.size();
-        h->A.slot_elems = (long long)slot_elems;
-        if (slot_elems) {
-            void* s = nullptr;
-            if ((e = cudaMalloc(&s, NSLOT * slot_elems * 8)) != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-            h->allocs.push_back(s);
-            h->A.scratch = static_cast<cpx<float>*>(s);
-        }
+        if (e == cudaSuccess) h->A.tmaps = static_cast<const CUtensorMap*>(upload(h, maps, &e, 128));
+        if (e != cudaSuccess) return cuda_fail(e);
+        h->A.nitems  = (int)items.size();
         h->ctl_bytes = (2 + 2 * std::max<size_t>(n_fft, 1)) * sizeof(int);
-        if ((e = cudaMalloc(&h->ctl, h->ctl_bytes)) != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-        h->allocs.push_back(h->ctl);
+        void* ctl    = nullptr;
+        if ((e = dev_alloc(h->ctl_bytes, &ctl)) != cudaSuccess) return cuda_fail(e);
+        h->ctl        = ctl;
         int* c        = static_cast<int*>(h->ctl);
         h->A.counter  = reinterpret_cast<unsigned*>(c);
         h->A.error    = c + 1;
         h->A.col_done = c + 2;
         h->A.row_done = c + 2 + std::max<size_t>(n_fft, 1);
-        if ((e = cudaFuncSetAttribute(rg::k_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, rg::SMEM)) != cudaSuccess) {
-            return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
+        if ((e = cudaFuncSetAttribute(rg::k_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, rg::SMEM)) !=
+            cudaSuccess) {
+            return cuda_fail(e);
         }
-        h->grid = sms;
-        if ((e = cudaMemset(h->ctl, 0, h->ctl_bytes)) != cudaSuccess) return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
+        int per_sm = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rg::k_ragged, rg::NT + 64, rg::SMEM)) !=
+            cudaSuccess) {
+            return cuda_fail(e);
+        }
+        const rg::args* d_args = static_cast<const rg::args*>(upload(h, std::vector<rg::args>{h->A}, &e));
+        if (e != cudaSuccess) return cuda_fail(e);
+        if (per_sm < 1) {
+            cudaFuncAttributes fa{};
+            cudaFuncGetAttributes(&fa, rg::k_ragged);
+            return fail(pcx_fail(PCX_ERR_CUDA, "ragged kernel does not fit an SM (registers " + std::to_string(fa.numRegs) +
+                                                   ", max threads " + std::to_string(fa.maxThreadsPerBlock) +
+                                                   ", static smem " + std::to_string(fa.sharedSizeBytes) + ")"));
+        }
+        h->grid = sms * per_sm;
+        if ((e = cudaMemset(h->ctl, 0, h->ctl_bytes)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(e);
         // ---- capture: reset counters, one persistent launch
         cudaStream_t cs = nullptr;
-        if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) {
-            return fail(pcx_fail(PCX_ERR_CUDA, cudaGetErrorString(e)));
-        }
+        if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
         e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) e = cudaMemsetAsync(h->ctl, 0, h->ctl_bytes, cs);
         if (e == cudaSuccess) {
-            rg::k_ragged<<<h->grid, rg::NT, rg::SMEM, cs>>>(h->A);
+            rg::k_ragged<<<h->grid, rg::NT + 64, rg::SMEM, cs>>>(d_args);
             e = cudaGetLastError();
         }
         cudaError_t e2 = cudaStreamEndCapture(cs, &h->graph);
