@@ -618,14 +618,15 @@ class C5Ragged:
 
     def config(self, world):
         return {"workload": "C5: 10,000 complex64 FFTs, N log-uniform 2^8..2^18, plus 500 correlations "
-                            "(S log-uniform 2^12..2^20, K log-uniform 64..8192, N_fft = next pow2 >= 2K), "
+                            "(S log-uniform 2^12..2^20, K log-uniform 64..8192, N_fft per request from "
+                            "correlation_fft_size(K)), "
                             "N(0,1) seed 5; one persistent launch from a device work queue replayed as a CUDA "
                             "graph, vs per-size plain launches",
                 "global_batch_points": None, "parallelism": f"independent shards x{world}"}
 
     def setup(self, dev, rank):
         import torch
-        from packed_b200 import fft_unit, fxcorr_unit, ragged_batch, vector
+        from packed_b200 import correlation_fft_size, fft_unit, fxcorr_unit, ragged_batch, vector
         rng = np.random.default_rng(5)
         lgs = np.floor(rng.uniform(8, 19, self.n_fft)).astype(int)
         self.groups = {}
@@ -644,7 +645,7 @@ class C5Ragged:
         k_all = np.floor(2 ** rng.uniform(6, 13, self.n_xc)).astype(int)
         self.xc_points = int(s_all.sum())
         for s, k in zip(s_all, k_all):
-            nf = max(128, 1 << int(np.ceil(np.log2(2 * k))))
+            nf = correlation_fft_size(int(k))    # per request, from the transform-work model
             taps = vector.from_complex(rng.standard_normal(k) + 1j * rng.standard_normal(k), device=dev)
             x = torch.randn(2 * int(s), device=dev)
             y = torch.empty_like(x)

@@ -671,11 +671,14 @@ __device__ __forceinline__ void copy_table_to_smem(cpx<T>* dst, const void* src,
 // input by its table entry, where the factor tables of pcx_fft_v2.cuh form
 // nine of the fifteen radix-16 twiddles as products of two entries (36 more
 // FP32 instructions per butterfly).  For the sub-transforms of the four-step
-// (64..1024 points) a full table is 1-10 KB.
+// (64..1024 points) a full table is 1-11 KB.  Each position's row is padded
+// by 16 bytes (32 bytes for radix 2): the threads of a warp read up to eight
+// positions at once, and with power-of-two rows those would share banks.
+__host__ __device__ constexpr int full_tw_row(int rb) { return (1 << rb) + (rb == 1 ? 4 : 2); }
 template<class P>
 __host__ __device__ constexpr int fs_full_tw_offset(int S) {
     int off = 0;
-    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) << P::rbits(s);
+    for (int s = 1; s < S; ++s) off += (1 << P::nsbits(s)) * full_tw_row(P::rbits(s));
     return off;
 }
 template<class P>
@@ -685,9 +688,15 @@ __host__ __device__ constexpr int fs_full_tw_size() {
 
 template<class T>
 __global__ void k_full_twiddles(cpx<T>* out, int ns, int rb, int log_nsr) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (ns << rb)) return;
-    const long long e = (long long)(q >> rb) * (q & ((1 << rb) - 1));
+    const int row = full_tw_row(rb);
+    const int q   = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns * row) return;
+    const int k = q / row, j = q - k * row;
+    if (j >= (1 << rb)) {
+        out[q] = {T(0), T(0)};    // padding
+        return;
+    }
+    const long long e = (long long)k * j;
     double          sn, cs;
     sincospi(2.0 * (double)e / (double)(1LL << log_nsr), &sn, &cs);
     out[q] = {T(cs), T(-sn)};
@@ -703,7 +712,7 @@ __device__ __forceinline__ void stage_apply_full(cpx<T> (&v)[E], int t, const cp
     static_for<G>([&](auto gc) {
         constexpr int g  = decltype(gc)::value;
         const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
-        const cpx<T>* tw = tab + fs_full_tw_offset<P>(S) + (k << RB);
+        const cpx<T>* tw = tab + fs_full_tw_offset<P>(S) + k * full_tw_row(RB);
         cpx<T>        a[R];
         static_for<R / 2>([&](auto qc) {
             constexpr int q = decltype(qc)::value;

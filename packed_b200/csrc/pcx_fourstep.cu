@@ -43,7 +43,7 @@ template<int LOGL, class T>
 cudaError_t gen_full_tables(void* out, cudaStream_t st) {
     using P = pcxg::splan<LOGL>;
     for (int s = 1; s < P::NST; ++s) {
-        const int n = (1 << P::nsbits(s)) << P::rbits(s);
+        const int n = (1 << P::nsbits(s)) * pcxg::full_tw_row(P::rbits(s));
         auto*     o = static_cast<pcxg::cpx<T>*>(out) + pcxg::fs_full_tw_offset<P>(s);
         pcxg::k_full_twiddles<T><<<(n + 255) / 256, 256, 0, st>>>(o, 1 << P::nsbits(s), P::rbits(s),
                                                                  P::nsbits(s) + P::rbits(s));
@@ -62,11 +62,16 @@ cudaError_t full_tables(void* out, bool f64, cudaStream_t st, int* entries) {
 
 cudaError_t pcx_fourstep_tables(int log_l, void* out, bool f64, cudaStream_t st, int* entries) {
     switch (log_l) {
+    case 5: return full_tables<5>(out, f64, st, entries);
     case 6: return full_tables<6>(out, f64, st, entries);
     case 7: return full_tables<7>(out, f64, st, entries);
     case 8: return full_tables<8>(out, f64, st, entries);
     case 9: return full_tables<9>(out, f64, st, entries);
     case 10: return full_tables<10>(out, f64, st, entries);
+    case 11: return full_tables<11>(out, f64, st, entries);
+    case 12: return full_tables<12>(out, f64, st, entries);
+    case 13: return full_tables<13>(out, f64, st, entries);
+    case 14: return full_tables<14>(out, f64, st, entries);
     default: return cudaErrorNotSupported;
     }
 }

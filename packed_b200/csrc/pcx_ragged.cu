@@ -13,7 +13,10 @@
 //   ROW     one row tile: waits until col_done[t] reaches the column-tile
 //           count, bulk-copies the slot rows, row FFTs, natural-order output,
 //           counted in row_done[t] once its rows have landed
-//   XC      up to M consecutive overlap-save blocks of one correlation
+//   XR      up to M consecutive overlap-save blocks of one correlation with
+//           N_fft <= 8192: the producer bulk-copies the M packed windows into
+//           the stage; forward FFT, times conj(K), inverse, in the stage
+//   XC      the same with N_fft = 16384, whose exchange takes the whole ring
 // Each block has NT compute threads and, as the one-launch four-step kernel
 // does, a producer warp and a publisher warp: the producer claims the next
 // item, waits for its dependency (a scratch slot freed by an earlier
@@ -22,9 +25,9 @@
 // while one is computed; the publisher counts completions as soon as they
 // happen and never waits on another block.  Every size runs its own
 // compile-time geometry; the exchanges of the sub-transforms run in place in
-// the item's stage.  Correlation items (last in the queue) read their windows
-// with plain loads and use the whole ring as workspace, so the producer drains
-// the ring around them.  Every wait is on an item earlier in the queue,
+// the item's stage.  16384-point correlation items (last in the queue) read
+// their windows with plain loads and use the whole ring as workspace, so the
+// producer drains the ring around them.  Every wait is on an item earlier in the queue,
 // claimed by a resident block whose publisher never waits on a later item:
 // the waits always end.  They are still bounded (about one second); on
 // timeout the block records an error and leaves.
@@ -52,7 +55,7 @@ constexpr int MAXLG = 32;
 constexpr int STAGE = 69632;
 constexpr int SMEM  = ST * STAGE;
 
-enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3 };
+enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3, K_XR = 4 };
 
 struct item {
     int kind, lg, a, b, c;    // SINGLE: a first transform, b count; COL/ROW: a transform, b tile; XC: a request, b first block, c count
@@ -80,7 +83,7 @@ struct tabs {
     const cpx<float>* tlo[MAXLG];     // W_N^i, i < N2
     const cpx<float>* tb[MAXLG];      // W_{16*N2}^i, i < N2
     cpx<float>*       scratch[MAXLG]; // the size's ring of scratch slots
-    const cpx<float>* xtw[MAXLG];     // correlator W_N table
+    const cpx<float>* xft[MAXLG];     // correlator full stage tables
 };
 struct args {
     const item*        items;
@@ -130,28 +133,17 @@ struct sgg {
     static_assert(M * RS * 4 <= STAGE && X::size * 8 <= STAGE, "rows and exchange fit a stage");
 };
 
-// Stages of a correlation block through the whole ring, named barrier over
-// the compute threads (the general kernels' run_stages with barrier BARN).
-template<class P, class X, class T, int E>
-__device__ __forceinline__ void run_stages_nb(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
-                                              const cpx<T>* __restrict__ twL) {
-    static_for<P::NST - 1>([&](auto sc) {
-        constexpr int S = decltype(sc)::value;
-        constexpr int G = E / (1 << P::rbits(S));
-        xch_sync<NT>();
-        static_for<E>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int g = i % G, j = i / G;
-            xch[X::idx(m, stage_out_index<P, S>(t, g, j))] = v[i];
-        });
-        xch_sync<NT>();
-        static_for<E>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            v[i]            = xch[X::idx(m, t + i * P::TT)];
-        });
-        stage_compute<P, S + 1>(v, t, twL);
-    });
-}
+// Correlation blocks of N = 2^LOGN <= 8192 on the ring: M windows of WS reals.
+template<int LOGN>
+struct xrg {
+    using P                 = splan<LOGN>;
+    static constexpr int L  = P::L;
+    static constexpr int TT = P::TT;
+    static constexpr int M  = NT / TT;
+    static constexpr int WS = 2 * L + single3_pad<TT>();
+    using X                 = xch_blocked<L, M>;
+    static_assert(M * WS * 4 <= STAGE && X::size * 8 <= STAGE, "windows and exchange fit a stage");
+};
 
 // ---------------------------------------------------------------- compute
 // Each returns false when a give-up vote made every compute thread leave.
@@ -286,6 +278,7 @@ template<int LOGN>
 __device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>* buf, int tid) {
     constexpr int EPT = LOGN >= 14 ? 32 : 16;
     using P           = splan<LOGN, EPT>;
+    static_assert(fs_full_tw_size<P>() == fs_full_tw_size<splan<LOGN>>(), "same stage radices");
     constexpr int L   = P::L;
     constexpr int E   = P::E;
     constexpr int TT  = P::TT;
@@ -307,21 +300,23 @@ __device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>*
         buf[e] = w;
     }
     xch_sync<NT>();
-    const cpx<float>* tw = A.tb.xtw[LOGN];
+    // full stage tables: the layout depends only on the stage radices, which
+    // are those of the 16-points-per-thread plan of the same size
+    const cpx<float>* tw = A.tb.xft[LOGN];
     cpx<float>        v[E];
     static_for<E>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         v[i]            = buf[m * L + t + i * TT];
     });
-    stage_compute<P, 0>(v, t, tw);
-    run_stages_nb<P, X>(v, buf, m, t, tw);
+    stage_compute_tab<P, 0>(v, t, tw);
+    run_stages_full<P, X, false, NT>(v, buf, m, t, tw);
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
         const cpx<float> k = ldg_cpx(q.kspec + t + i * TT);
         v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
     });
-    stage_compute<P, 0>(v, t, tw);
-    run_stages_nb<P, X>(v, buf, m, t, tw);
+    stage_compute_tab<P, 0>(v, t, tw);
+    run_stages_full<P, X, false, NT>(v, buf, m, t, tw);
     if (m < it.c) {
         const long long b0 = (long long)(it.b + m) * q.step;
         static_for<E>([&](auto ic) {
@@ -336,6 +331,63 @@ __device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>*
         });
     }
     xch_sync<NT>();    // the ring is read: it may be refilled
+}
+
+// Up to M overlap-save blocks of one correlation (N_fft <= 8192) from their
+// packed windows in the stage.
+template<int LOGN>
+__device__ __noinline__ bool xr_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
+                                      uint64_t* empty_bar) {
+    using G          = xrg<LOGN>;
+    using P          = typename G::P;
+    constexpr int E  = P::E;
+    constexpr int TT = G::TT;
+    constexpr int SW = TT >= 32 ? 16 : 0;
+    static_assert(TT % 8 == 0, "whole packs per thread stride");
+    const xc_req& q  = A.xreq[it.a];
+    const int     m  = tid / TT;
+    const int     t  = tid - m * TT;
+    const long long b0 = (long long)(it.b + m) * q.step;
+    // window samples left before the signal's end (0 for windows past the item)
+    const long long left = m < it.c ? q.len - b0 : 0;
+    const int       lim  = (int)(left < G::L ? (left > 0 ? left : 0) : G::L);
+    const float*  in = reinterpret_cast<const float*>(buf);
+    cpx<float>    v[E];
+    static_for<E>([&](auto ic) {
+        constexpr int    i = decltype(ic)::value;
+        const cpx<float> x = lds_swapped<float, SW>(in, m * G::WS + pk<LPK>(t) + 2 * i * TT, 8);
+        // the window is zero past the signal (the copy took whole packs)
+        v[i] = t + i * TT < lim ? x : cpx<float>{0.f, 0.f};
+    });
+    const auto* fst = A.tb.xft[LOGN];
+    auto* xch = reinterpret_cast<cpx<float>*>(buf);
+    stage_compute_tab<P, 0>(v, t, fst);
+    if (run_stages_full<P, typename G::X, false, NT>(v, xch, m, t, fst, bad)) return false;
+    // v[i] = X[t + i*TT]: conj(X) * K, then the forward transform again
+    static_for<E>([&](auto ic) {
+        constexpr int    i = decltype(ic)::value;
+        const cpx<float> k = ldg_cpx(q.kspec + t + i * TT);
+        v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
+    });
+    stage_compute_tab<P, 0>(v, t, fst);
+    run_stages_full<P, typename G::X, false, NT>(v, xch, m, t, fst);
+    fence_proxy_async_smem();    // the stage is read: it may be refilled
+    __syncwarp();
+    if (tid % 32 == 0) mbar_arrive(empty_bar);
+    if (m < it.c) {
+        // outputs t + i*TT < min(step, samples left); the window starts on a
+        // whole pack, so the packed offset is a base plus a constant
+        const int olim = lim < q.step ? lim : q.step;
+        float*    d    = q.dst + 2 * b0 + pk<LPK>(t);
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            if (t + i * TT < olim) {
+                d[2 * i * TT]     = v[i].re;
+                d[2 * i * TT + 8] = -v[i].im;
+            }
+        });
+    }
+    return true;
 }
 
 // ---------------------------------------------------------------- producer
@@ -375,9 +427,31 @@ __device__ void issue_single(const args& A, const item& it, unsigned char* buf, 
     }
 }
 
+template<int LOGN>
+__device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    using G          = xrg<LOGN>;
+    const xc_req& q  = A.xreq[it.a];
+    // window m: samples [(b+m)*step, +L) of the packed signal, whole packs
+    // up to the signal's end
+    uint32_t bytes = 0;
+    for (int m = 0; m < it.c; ++m) {
+        const long long pos   = (long long)(it.b + m) * q.step;
+        const long long valid = q.len - pos < G::L ? q.len - pos : G::L;
+        bytes += (uint32_t)((valid + 7) / 8) * 64;
+    }
+    if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+    __syncwarp();
+    for (int m = lane; m < it.c; m += 32) {
+        const long long pos   = (long long)(it.b + m) * q.step;
+        const long long valid = q.len - pos < G::L ? q.len - pos : G::L;
+        bulk_g2s(reinterpret_cast<float*>(buf) + m * G::WS, q.src + 2 * pos, (uint32_t)((valid + 7) / 8) * 64, bar);
+    }
+}
+
 #define PCX_RG_FOURSTEP(X) X(13, 7, 6) X(14, 7, 7) X(15, 8, 7) X(16, 8, 8) X(17, 9, 8) X(18, 9, 9)
 #define PCX_RG_SINGLE(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
-#define PCX_RG_XC(X) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
+#define PCX_RG_XC(X) X(14)
+#define PCX_RG_XR(X) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
 // The arguments sit in device memory (uploaded once at creation): the item
 // functions take them by reference without a per-thread copy.
@@ -501,7 +575,16 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 issued      = k + 1;
                 continue;
             }
-            if (it.kind == K_SINGLE) {
+            if (it.kind == K_XR) {
+                switch (it.lg) {
+#define PCX_RG_ISSUE_X(LG) \
+    case LG: issue_xr<LG>(A, it, buf, &full[s], lane); break;
+                    PCX_RG_XR(PCX_RG_ISSUE_X)
+#undef PCX_RG_ISSUE_X
+                default: break;
+                }
+                issued = k + 1;
+            } else if (it.kind == K_SINGLE) {
                 switch (it.lg) {
 #define PCX_RG_ISSUE_S(LG) \
     case LG: issue_single<LG>(A, it, buf, &full[s], lane); break;
@@ -607,6 +690,14 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             if (alive && !bad) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&written[s]);
+            }
+        } else if (it.kind == K_XR) {
+            switch (it.lg) {
+#define PCX_RG_RUN_XR(LG) \
+    case LG: alive = xr_items<LG>(A, it, buf, bad, tid, &empty[s]); break;
+                PCX_RG_XR(PCX_RG_RUN_XR)
+#undef PCX_RG_RUN_XR
+            default: bad = true; break;
             }
         } else if (it.kind == K_ROW) {
             switch (it.lg) {
@@ -779,11 +870,18 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             int rc = pcx_fft_run(p, ks, xc_g[j], xc_k[j], 1, 8, PCX_FORWARD, 0, 1, 2 * xc_nfft[j], 2 * xc_nfft[j], nullptr,
                                  0, 0, 1.0 / (double)xc_nfft[j]);
             if (rc) return fail(rc);
-            if (!h->A.tb.xtw[lg]) {
-                void* tw = nullptr;
-                if ((e = dev_alloc(xc_nfft[j] * 8, &tw)) != cudaSuccess) return cuda_fail(e);
-                if ((e = pcx_gen_twiddles(tw, (int)xc_nfft[j], lg, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
-                h->A.tb.xtw[lg] = static_cast<const cpx<float>*>(tw);
+            // on the ring (up to 8192 points) the windows come by bulk copies
+            // of whole packs
+            if (lg <= 13 && (!aligned16(xc_src[j]) || !aligned16(xc_dst[j]))) {
+                return fail(pcx_fail(PCX_ERR_INVALID, "ragged correlation buffers must be 16-byte aligned"));
+            }
+            if (!h->A.tb.xft[lg]) {
+                int   fe = 0;
+                void* ft = nullptr;
+                if ((e = pcx_fourstep_tables(lg, nullptr, false, 0, &fe)) != cudaSuccess) return cuda_fail(e);
+                if ((e = dev_alloc((size_t)fe * 8, &ft)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_fourstep_tables(lg, ft, false, 0, &fe)) != cudaSuccess) return cuda_fail(e);
+                h->A.tb.xft[lg] = static_cast<const cpx<float>*>(ft);
             }
             xreq[j] = {static_cast<const float*>(xc_src[j]), static_cast<float*>(xc_dst[j]), (long long)xc_len[j],
                        (int)step, (int)((xc_len[j] + step - 1) / step), lg, static_cast<const cpx<float>*>(ks)};
@@ -811,6 +909,15 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             const int M = rg::NT / std::max(1, (1 << lg) / 16);
             for (size_t q = 0; q < idx.size(); q += M) {
                 fill.push_back({rg::K_SINGLE, lg, idx[q], (int)std::min<size_t>(M, idx.size() - q), 0});
+            }
+        }
+        // correlations of up to 8192 points: M windows per item, on the ring
+        for (size_t j = 0; j < n_xc; ++j) {
+            const int lg = xreq[j].lg;
+            if (lg > 13) continue;
+            const int M = rg::NT / ((1 << lg) / 16);
+            for (int b = 0; b < xreq[j].nblk; b += M) {
+                fill.push_back({rg::K_XR, lg, (int)j, b, std::min(M, xreq[j].nblk - b)});
             }
         }
         std::vector<rg::item> items;
@@ -864,11 +971,12 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             }
         }
         push_fill(fill.size());
-        // correlations last, the longest windows first
+        // 16384-point correlations last
         {
             std::vector<rg::item> xc_items;
             for (size_t j = 0; j < n_xc; ++j) {
                 const int lg = xreq[j].lg;
+                if (lg <= 13) continue;
                 const int tt = (1 << lg) / (lg >= 14 ? 32 : 16);
                 const int M  = std::max(1, rg::NT / tt);
                 for (int b = 0; b < xreq[j].nblk; b += M) {

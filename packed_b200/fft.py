@@ -516,6 +516,27 @@ class fxcorr_unit:
         return gx, gg
 
 
+def correlation_fft_size(k: int, max_size: int = 16384) -> int:
+    """FFT size for an overlap-save correlation with a k-tap kernel: the power
+    of two N >= k + 7 that minimises the transform work per output sample,
+    2 * N * log2(N) / (N - k + 1) (a forward and an inverse transform per
+    block of N - k + 1 outputs), over 128 <= N <= max_size.  Sizes above 8192
+    are taken only for kernels of more than 4096 taps, where they halve the
+    block overlap; up to 8192 the ragged batch runs a correlation's blocks in
+    its shared-memory ring."""
+    best, best_cost = None, None
+    n = 128
+    while n <= max_size:
+        if n >= k + 7 and (n <= 8192 or k > 4096):
+            cost = 2 * n * (n.bit_length() - 1) / (n - k + 1)
+            if best_cost is None or cost < best_cost:
+                best, best_cost = n, cost
+        n *= 2
+    if best is None:
+        raise ValueError(f"kernel size (which is {k}) needs an FFT size above {max_size}")
+    return best
+
+
 class ragged_batch:
     """Many FFTs of uneven power-of-two sizes and correlations in ONE
     persistent launch fed by a device work queue, replayed from a CUDA graph

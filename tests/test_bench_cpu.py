@@ -37,3 +37,21 @@ def test_reference_arm_prints_one_json_line():
     assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"].startswith("C1")
+
+
+def test_correlation_fft_size_model():
+    """The ragged batch's FFT size per correlation: a power of two with room
+    for the kernel, minimising 2 N log2 N / (N - k + 1), at most 8192 unless
+    the kernel has more than 4096 taps."""
+    from packed_b200 import correlation_fft_size as f
+    for k in (1, 64, 100, 700, 3000, 4096, 4097, 8192, 16377):
+        n = f(k)
+        assert n & (n - 1) == 0 and n >= k + 7 and 128 <= n <= 16384
+        assert n <= 8192 or k > 4096
+        cost = 2 * n * (n.bit_length() - 1) / (n - k + 1)
+        for m in (128 << i for i in range(8)):
+            if m >= k + 7 and (m <= 8192 or k > 4096):
+                assert cost <= 2 * m * (m.bit_length() - 1) / (m - k + 1) + 1e-12
+    import pytest
+    with pytest.raises(ValueError):
+        f(16378)

@@ -26,9 +26,11 @@ def test_ragged_batch_matches_oracle(seed):
         zs.append(z)
         ffts.append((torch.full((2 * n,), float("nan"), device="cuda"), dev(O.pack(z, 8)), n))
     xcs, xin = [], []
-    for _ in range(6):
-        s = int(2 ** rng.uniform(12, 17))
-        k = int(2 ** rng.uniform(6, 12))
+    # correlations of 128..8192 points (on the ring) and one of 16384 points
+    # (its own path through the whole ring)
+    for q in range(7):
+        s = int(2 ** rng.uniform(12, 17)) if q < 6 else 50000
+        k = int(2 ** rng.uniform(6, 12)) if q < 6 else 5000
         nf = max(128, 1 << int(np.ceil(np.log2(2 * k))))
         x, g = normal_cx(rng, s), normal_cx(rng, k)
         xin.append((x, g, nf))
