@@ -671,10 +671,12 @@ __device__ __forceinline__ void copy_table_to_smem(cpx<T>* dst, const void* src,
 // input by its table entry, where the factor tables of pcx_fft_v2.cuh form
 // nine of the fifteen radix-16 twiddles as products of two entries (36 more
 // FP32 instructions per butterfly).  For the sub-transforms of the four-step
-// (64..1024 points) a full table is 1-11 KB.  Each position's row is padded
-// by 16 bytes (32 bytes for radix 2): the threads of a warp read up to eight
-// positions at once, and with power-of-two rows those would share banks.
-__host__ __device__ constexpr int full_tw_row(int rb) { return (1 << rb) + (rb == 1 ? 4 : 2); }
+// (64..1024 points) a full table is 1-15 KB.  Each position's row of 4 or more
+// entries is padded by 16 bytes: the threads of a warp read up to eight
+// positions at once, and with power-of-two rows of 32 bytes or more those
+// would share banks.  Radix-2 rows (16 bytes in FP32) are not padded: eight
+// neighbouring positions fill 128 contiguous bytes.
+__host__ __device__ constexpr int full_tw_row(int rb) { return (1 << rb) + (rb == 1 ? 0 : 2); }
 template<class P>
 __host__ __device__ constexpr int fs_full_tw_offset(int S) {
     int off = 0;
@@ -702,22 +704,44 @@ __global__ void k_full_twiddles(cpx<T>* out, int ns, int rb, int log_nsr) {
     out[q] = {T(cs), T(-sn)};
 }
 
-// Butterflies of stage S >= 1 with the full table (tab: this sub-transform's).
-template<class P, int S, bool SH, class T, int E>
+// Whether the full table of splan PL serves splan P as well: the same stages
+// with the same butterfly positions, only the last stage's radix of PL may be
+// larger.  Position k of P's last stage (radix R) then needs W_{Ns*R}^(j*k) =
+// entry j*D of PL's row k, D = R_PL / R.
+template<class P, class PL>
+__host__ __device__ constexpr bool full_tab_serves() {
+    if (P::NST != PL::NST) return false;
+    for (int s = 0; s < P::NST; ++s) {
+        if (P::nsbits(s) != PL::nsbits(s)) return false;
+        if (s + 1 < P::NST ? P::rbits(s) != PL::rbits(s) : P::rbits(s) > PL::rbits(s)) return false;
+    }
+    return true;
+}
+
+// Butterflies of stage S >= 1 with the full table `tab` of splan PT (P's own,
+// or a larger sub-transform's that serves P: full_tab_serves).
+template<class P, int S, bool SH, class PT = P, class T, int E>
 __device__ __forceinline__ void stage_apply_full(cpx<T> (&v)[E], int t, const cpx<T>* __restrict__ tab) {
+    static_assert(full_tab_serves<P, PT>(), "table of another stage structure");
     constexpr int RB  = P::rbits(S);
     constexpr int R   = 1 << RB;
     constexpr int NSB = P::nsbits(S);
     constexpr int G   = E / R;
+    constexpr int D   = 1 << (PT::rbits(S) - RB);    // column step in PT's rows
     static_for<G>([&](auto gc) {
         constexpr int g  = decltype(gc)::value;
         const int     k  = (t + g * P::TT) & ((1 << NSB) - 1);
-        const cpx<T>* tw = tab + fs_full_tw_offset<P>(S) + k * full_tw_row(RB);
+        const cpx<T>* tw = tab + fs_full_tw_offset<PT>(S) + k * full_tw_row(PT::rbits(S));
         cpx<T>        a[R];
         static_for<R / 2>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             cpx<T>        w0, w1;
-            ld2<SH>(tw + 2 * q, w0, w1);
+            if constexpr (D == 1) {
+                ld2<SH>(tw + 2 * q, w0, w1);
+            } else {
+                if constexpr (q > 0) w0 = SH ? tw[2 * q * D] : ldg_cpx(tw + 2 * q * D);
+                w1 = SH ? tw[(2 * q + 1) * D] : ldg_cpx(tw + (2 * q + 1) * D);
+            }
             a[2 * q]     = q == 0 ? v[g] : cmul(v[g + 2 * q * G], w0);
             a[2 * q + 1] = cmul(v[g + (2 * q + 1) * G], w1);
         });
@@ -748,7 +772,7 @@ __device__ __forceinline__ bool bar1_any(bool bad) {
 // anything is written, when any of those threads passes `bad`, so all of them
 // leave at the same point without a barrier of its own.  With BARN <= 0 `bad`
 // is ignored and the result is false.
-template<class P, class X, bool SH, int BARN, class T, int E>
+template<class P, class X, bool SH, int BARN, class PT = P, class T, int E>
 __device__ __forceinline__ bool run_stages_full(cpx<T> (&v)[E], cpx<T>* xch, int m, int t,
                                                 const cpx<T>* __restrict__ tab, bool bad = false) {
     bool abort = false;
@@ -774,7 +798,7 @@ __device__ __forceinline__ bool run_stages_full(cpx<T> (&v)[E], cpx<T>* xch, int
             constexpr int i = decltype(ic)::value;
             v[i]            = xch[X::idx(m, t + i * P::TT)];
         });
-        stage_apply_full<P, S + 1, SH>(v, t, tab);
+        stage_apply_full<P, S + 1, SH, PT>(v, t, tab);
     });
     return abort;
 }

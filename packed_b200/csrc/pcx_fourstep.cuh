@@ -97,8 +97,15 @@ struct fs_cfg {
     static constexpr int TILEB = COLB > ROWB ? COLB : ROWB;
     static constexpr int STAGE = ((IP ? (TILEB > XB ? TILEB : XB) : TILEB) + 127) / 128 * 128;
     static constexpr int BASE = ST * STAGE + (IP ? 0 : XB);
-    static constexpr int TB1  = fs_full_tw_size<P1>() * (int)sizeof(cpx<T>);
-    static constexpr int TB2  = fs_full_tw_size<P2>() * (int)sizeof(cpx<T>);
+    // one stage table for both passes when the larger sub-transform's serves
+    // the smaller one (equal halves, or 512 with 1024 points): room for it
+    // beside a three-stage ring of 64 KB tiles
+    using PL                  = std::conditional_t<(LOGN1 >= LOGN2), P1, P2>;
+    static constexpr bool ONE = full_tab_serves<P1, PL>() && full_tab_serves<P2, PL>();
+    using PT1                 = std::conditional_t<ONE, PL, P1>;
+    using PT2                 = std::conditional_t<ONE, PL, P2>;
+    static constexpr int TB1  = fs_full_tw_size<PT1>() * (int)sizeof(cpx<T>);
+    static constexpr int TB2  = ONE ? 0 : fs_full_tw_size<P2>() * (int)sizeof(cpx<T>);
     static constexpr bool SH  = stw_fits(BASE, TB1 + TB2, MINB);
     static constexpr int SMEM = SH ? BASE + TB1 + TB2 : BASE;
     static constexpr int BOXY = N1 < 256 ? N1 : 256;
@@ -179,7 +186,10 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char*      ring = smem;
     cpx<T>*             tws1 = reinterpret_cast<cpx<T>*>(smem + F::BASE);
-    cpx<T>*             tws2 = tws1 + F::TB1 / (int)sizeof(cpx<T>);
+    cpx<T>*             tws2 = F::ONE ? tws1 : tws1 + F::TB1 / (int)sizeof(cpx<T>);
+    // with one table it is the larger sub-transform's
+    const void*         gtab1 = F::ONE && LOGN2 > LOGN1 ? a.stw2 : a.stw1;
+    const void*         gtab2 = F::ONE && LOGN1 > LOGN2 ? a.stw1 : a.stw2;
     __shared__ uint64_t full[ST];      // TMA bytes landed
     __shared__ uint64_t empty[ST];     // compute warps done with the stage, publisher past its item
     __shared__ uint64_t slotok[ST];    // column tile: its scratch slot may be written
@@ -191,8 +201,8 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
     const long long     mask  = a.nslot - 1;
 
     if constexpr (SH) {
-        copy_table_to_smem<F::TB1>(tws1, a.stw1, tid, NT + 64);
-        copy_table_to_smem<F::TB2>(tws2, a.stw2, tid, NT + 64);
+        copy_table_to_smem<F::TB1>(tws1, gtab1, tid, NT + 64);
+        if constexpr (!F::ONE) copy_table_to_smem<F::TB2>(tws2, a.stw2, tid, NT + 64);
     }
     if (tid == 0) {
         for (int s = 0; s < ST; ++s) {
@@ -370,7 +380,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             const int     t    = tid / C;
             const int     n2   = it.tile * C + c;
             const T*      in   = reinterpret_cast<const T*>(ring + s * F::STAGE);
-            const auto*   stw1 = SH ? tws1 : reinterpret_cast<const cpx<T>*>(a.stw1);
+            const auto*   stw1 = SH ? tws1 : reinterpret_cast<const cpx<T>*>(gtab1);
             cpx<T>        v[E];
             static_for<E>([&](auto ic) {
                 constexpr int i = decltype(ic)::value;
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             });
             if constexpr (!IP) release_stage();
             stage_compute_tab<P1, 0>(v, t, stw1);
-            if (run_stages_full<P1, typename F::X1, SH, NT>(v, xch, c, t, stw1, bad)) return;
+            if (run_stages_full<P1, typename F::X1, SH, NT, typename F::PT1>(v, xch, c, t, stw1, bad)) return;
             if constexpr (IP) release_stage();
             if (!mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1))) {
                 // the producer gave up on this slot: nothing is written, and
@@ -406,7 +416,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             const int     mhi  = tid / (G8 * TT);
             const int     m    = mhi * G8 + mlo;
             const int     k1   = it.tile * CR + m;
-            const auto*   stw2 = SH ? tws2 : reinterpret_cast<const cpx<T>*>(a.stw2);
+            const auto*   stw2 = SH ? tws2 : reinterpret_cast<const cpx<T>*>(gtab2);
             const cpx<T>* in   = reinterpret_cast<const cpx<T>*>(ring + s * F::STAGE) + m * RSI + t;
             cpx<T>        v[E];
             static_for<E>([&](auto ic) {
@@ -415,7 +425,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             });
             if constexpr (!IP) release_stage();
             stage_compute_tab<P2, 0>(v, t, stw2);
-            if (run_stages_full<P2, typename F::X2, SH, NT>(v, xch, m, t, stw2, bad)) return;
+            if (run_stages_full<P2, typename F::X2, SH, NT, typename F::PT2>(v, xch, m, t, stw2, bad)) return;
             if constexpr (IP) release_stage();
             T*      dst = reinterpret_cast<T*>(a.dst) + it.r * a.dst_stride + pk<LP>(t * N1 + k1);
             const T sc  = T(a.scale);
