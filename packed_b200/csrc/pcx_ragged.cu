@@ -53,7 +53,33 @@ constexpr int MAXLG = 32;
 // A stage holds a 64 KB tile (plus row padding) or the item's in-place
 // exchange buffer (one padding slot per 16 elements): 68 KB at every size.
 constexpr int STAGE = 69632;
-constexpr int SMEM  = ST * STAGE;
+constexpr int RING  = ST * STAGE;
+// Behind the ring: the full stage tables of the 64..512-point sub-transforms
+// (the four-step passes of 2^13..2^18 and the correlations of 128..512
+// points), copied from global memory once per launch.
+constexpr int SUB_LO = 6, SUB_HI = 9;
+template<int L>
+__host__ __device__ constexpr int sub_off() {    // entries before the table of 2^L points
+    int o = 0;
+    if constexpr (L > SUB_LO) o = sub_off<L - 1>() + fs_full_tw_size<splan<L - 1>>();
+    return o;
+}
+constexpr int SUBTAB = sub_off<SUB_HI + 1>() * 8;
+constexpr int SMEM   = RING + SUBTAB;
+static_assert(SUBTAB % 16 == 0 && SMEM <= 232448, "tables beside the ring");
+
+extern __shared__ __align__(128) unsigned char rg_smem[];
+__shared__ uint64_t s_full[ST];       // the item's copies landed (XC: the producer arrived)
+__shared__ uint64_t s_empty[ST];      // compute warps done with the stage, publisher past its item
+__shared__ uint64_t s_slotok[ST];     // column tile: its scratch slot may be written
+__shared__ uint64_t s_written[ST];    // column tile: compute warps wrote the slot
+__shared__ int      s_item[ST];       // item index in the stage (-1: the queue is exhausted)
+
+template<int L>
+__device__ __forceinline__ const cpx<float>* sub_tab() {
+    static_assert(L >= SUB_LO && L <= SUB_HI, "table kept in shared memory");
+    return reinterpret_cast<const cpx<float>*>(rg_smem + RING) + sub_off<L>();
+}
 
 enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3, K_XR = 4 };
 
@@ -77,13 +103,12 @@ struct xc_req {
 };
 struct tabs {
     const cpx<float>* stw[MAXLG];     // single pass: stage factor tables (lg <= 12)
-    const cpx<float>* fst1[MAXLG];    // four-step (per total lg): full stage tables of the N1 / N2 sub-transforms
-    const cpx<float>* fst2[MAXLG];
     const cpx<float>* thi[MAXLG];     // W_N^(i*N2), i < N1
     const cpx<float>* tlo[MAXLG];     // W_N^i, i < N2
     const cpx<float>* tb[MAXLG];      // W_{16*N2}^i, i < N2
     cpx<float>*       scratch[MAXLG]; // the size's ring of scratch slots
     const cpx<float>* xft[MAXLG];     // correlator full stage tables
+    const void*       sub;            // SUBTAB bytes: full tables of 2^6..2^9 points, in order
 };
 struct args {
     const item*        items;
@@ -147,10 +172,9 @@ struct xrg {
 
 // ---------------------------------------------------------------- compute
 // Each returns false when a give-up vote made every compute thread leave.
-// They are not inlined: every size and kind is allocated its registers on its
-// own instead of all of them sharing one allocation across the dispatch.
+// They are inlined into the run loops below (one per kind and size).
 template<int LOGL>
-__device__ __noinline__ bool single_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
+__device__ __forceinline__ bool single_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
                                           uint64_t* empty_bar) {
     using G          = sgg<LOGL>;
     using P          = typename G::P;
@@ -193,7 +217,7 @@ __device__ __noinline__ bool single_items(const args& A, const item& it, unsigne
 // The stage is free once this returns true (the caller releases it); the
 // scratch stores wait for `slot_ready`.
 template<int L1, int L2, class SlotWait>
-__device__ __noinline__ bool col_item(const args& A, const item& it, unsigned char* buf, bool& bad, int tid, SlotWait&& slot_ready,
+__device__ __forceinline__ bool col_item(const args& A, const item& it, unsigned char* buf, bool& bad, int tid, SlotWait&& slot_ready,
                          uint64_t* empty_bar) {
     using F          = fsg<L1, L2>;
     using P1         = typename F::P1;
@@ -217,9 +241,9 @@ __device__ __noinline__ bool col_item(const args& A, const item& it, unsigned ch
         const cpx<float> x = lds_swapped<float, 16>(in, (t + i * TT) * F::SEG + pk<LPK>(c), 8);
         v[i]               = {x.re, A.conj ? -x.im : x.im};
     });
-    const auto* fst = A.tb.fst1[L1 + L2];
+    const auto* fst = sub_tab<L1>();
     stage_compute_tab<P1, 0>(v, t, fst);
-    if (run_stages_full<P1, typename F::X1, false, NT>(v, reinterpret_cast<cpx<float>*>(buf), c, t, fst, bad)) {
+    if (run_stages_full<P1, typename F::X1, true, NT>(v, reinterpret_cast<cpx<float>*>(buf), c, t, fst, bad)) {
         return false;
     }
     // the stage is read: let the producer refill it while the tile is stored
@@ -238,7 +262,7 @@ __device__ __noinline__ bool col_item(const args& A, const item& it, unsigned ch
 }
 
 template<int L1, int L2>
-__device__ __noinline__ bool row_item(const args& A, const item& it, unsigned char* buf, bool bad, int tid, uint64_t* empty_bar) {
+__device__ __forceinline__ bool row_item(const args& A, const item& it, unsigned char* buf, bool bad, int tid, uint64_t* empty_bar) {
     using F          = fsg<L1, L2>;
     using P2         = typename F::P2;
     constexpr int E  = P2::E;
@@ -255,9 +279,9 @@ __device__ __noinline__ bool row_item(const args& A, const item& it, unsigned ch
         constexpr int i = decltype(ic)::value;
         v[i]            = in[i * TT];
     });
-    const auto* fst = A.tb.fst2[L1 + L2];
+    const auto* fst = sub_tab<L2>();
     stage_compute_tab<P2, 0>(v, t, fst);
-    if (run_stages_full<P2, typename F::X2, false, NT>(v, reinterpret_cast<cpx<float>*>(buf), m, t, fst, bad)) {
+    if (run_stages_full<P2, typename F::X2, true, NT>(v, reinterpret_cast<cpx<float>*>(buf), m, t, fst, bad)) {
         return false;
     }
     fence_proxy_async_smem();
@@ -275,7 +299,7 @@ __device__ __noinline__ bool row_item(const args& A, const item& it, unsigned ch
 
 // Up to M overlap-save blocks of one correlation; buf is the whole ring.
 template<int LOGN>
-__device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>* buf, int tid) {
+__device__ __forceinline__ void xc_items(const args& A, const item& it, cpx<float>* buf, int tid) {
     constexpr int EPT = LOGN >= 14 ? 32 : 16;
     using P           = splan<LOGN, EPT>;
     static_assert(fs_full_tw_size<P>() == fs_full_tw_size<splan<LOGN>>(), "same stage radices");
@@ -284,7 +308,7 @@ __device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>*
     constexpr int TT  = P::TT;
     constexpr int M   = NT / TT;
     using X           = xch_blocked<L, M>;
-    static_assert(X::size * 8 <= SMEM, "correlation workspace fits the ring");
+    static_assert(X::size * 8 <= RING, "correlation workspace fits the ring");
     const xc_req& q   = A.xreq[it.a];
     const int     m   = tid / TT;
     const int     t   = tid - m * TT;
@@ -335,6 +359,8 @@ __device__ __noinline__ void xc_items(const args& A, const item& it, cpx<float>*
 
 // Up to M overlap-save blocks of one correlation (N_fft <= 8192) from their
 // packed windows in the stage.
+// Not inlined into its run loop: the correlation's two transforms need every
+// register (inlined, the loop's state spilled).
 template<int LOGN>
 __device__ __noinline__ bool xr_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
                                       uint64_t* empty_bar) {
@@ -359,10 +385,14 @@ __device__ __noinline__ bool xr_items(const args& A, const item& it, unsigned ch
         // the window is zero past the signal (the copy took whole packs)
         v[i] = t + i * TT < lim ? x : cpx<float>{0.f, 0.f};
     });
-    const auto* fst = A.tb.xft[LOGN];
+    constexpr bool TS  = LOGN <= SUB_HI;    // its table is in shared memory
+    const auto*    fst = [&]() {
+        if constexpr (TS) return sub_tab<(TS ? LOGN : SUB_LO)>();
+        else return A.tb.xft[LOGN];
+    }();
     auto* xch = reinterpret_cast<cpx<float>*>(buf);
     stage_compute_tab<P, 0>(v, t, fst);
-    if (run_stages_full<P, typename G::X, false, NT>(v, xch, m, t, fst, bad)) return false;
+    if (run_stages_full<P, typename G::X, TS, NT>(v, xch, m, t, fst, bad)) return false;
     // v[i] = X[t + i*TT]: conj(X) * K, then the forward transform again
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
@@ -370,7 +400,7 @@ __device__ __noinline__ bool xr_items(const args& A, const item& it, unsigned ch
         v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
     });
     stage_compute_tab<P, 0>(v, t, fst);
-    run_stages_full<P, typename G::X, false, NT>(v, xch, m, t, fst);
+    run_stages_full<P, typename G::X, TS, NT>(v, xch, m, t, fst);
     fence_proxy_async_smem();    // the stage is read: it may be refilled
     __syncwarp();
     if (tid % 32 == 0) mbar_arrive(empty_bar);
@@ -453,29 +483,150 @@ __device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint
 #define PCX_RG_XC(X) X(14)
 #define PCX_RG_XR(X) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
+// ---------------------------------------------------------------- runs
+// The compute warps take the items of the ring in order.  Consecutive items
+// of one kind and size are worked by one run function, which loops until the
+// next item is of another kind or size; the runs are not inlined into the
+// dispatch, so each is allocated its registers on its own, and a call is made
+// per run of items rather than per item.
+
+// Compute-warp state carried from one run to the next.
+struct cstate {
+    long long k;         // position of the next item in the block's ring sequence
+    uint32_t  colpar;    // bit s: parity of the next slot hand-off wait on stage s
+    bool      bad;       // a bounded wait of this thread gave up
+};
+
+enum : int { RUN_NEXT = 0, RUN_LEAVE = 1 };
+
+// Waits (bounded) until item k's copies have landed and returns its index:
+// -1 at the end of the queue, -2 when the wait gave up (the thread then votes
+// at barrier 1, where every other compute thread meets it at the first
+// barrier of its next item, and all of them leave).
+__device__ __forceinline__ int next_item(const args& A, long long k) {
+    const int s = (int)(k % ST);
+    if (!mbar_wait_bounded(&s_full[s], (uint32_t)((k / ST) & 1))) {
+        atomicExch(A.error, 1);
+        return -2;
+    }
+    return s_item[s];
+}
+
+// The stage of item k is no longer read: it may be refilled.
+__device__ __forceinline__ void release_stage(long long k, int tid) {
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (tid % 32 == 0) mbar_arrive(&s_empty[(int)(k % ST)]);
+}
+
+// Runs items from cs.k on while Match(item) holds, with Work(item, k, stage)
+// returning false when the block leaves.
+template<class Match, class Work>
+__device__ __forceinline__ int run_loop(const args& A, cstate& cs, Match&& match, Work&& work) {
+    long long k = cs.k;
+    int       r = RUN_NEXT;
+    for (;; ++k) {
+        const int idx = next_item(A, k);
+        if (idx == -2) {
+            bar1_any<NT>(true);
+            r = RUN_LEAVE;
+            break;
+        }
+        if (idx < 0) break;    // the dispatch votes and leaves
+        const item it = A.items[idx];
+        if (!match(it)) break;
+        if (!work(it, k, rg_smem + (int)(k % ST) * STAGE)) {
+            r = RUN_LEAVE;
+            break;
+        }
+    }
+    cs.k = k;
+    return r;
+}
+
+template<int L1, int L2>
+__device__ __noinline__ int run_fourstep(const args& A, int tid, cstate& cs) {
+    uint32_t colpar = cs.colpar;
+    bool     bad    = cs.bad;
+    const int r = run_loop(
+        A, cs, [](const item& it) { return (it.kind == K_COL || it.kind == K_ROW) && it.lg == L1 + L2; },
+        [&](const item& it, long long k, unsigned char* buf) -> bool {
+            const int s = (int)(k % ST);
+            if (it.kind == K_COL) {
+                auto slot_ready = [&]() -> bool {
+                    const bool ok = mbar_wait_bounded(&s_slotok[s], (colpar >> s) & 1u);
+                    colpar ^= 1u << s;
+                    if (!ok) atomicExch(A.error, 1);
+                    return ok;
+                };
+                if (!col_item<L1, L2>(A, it, buf, bad, tid, slot_ready, &s_empty[s])) return false;
+                if (!bad) {
+                    __syncwarp();
+                    if (tid % 32 == 0) mbar_arrive(&s_written[s]);
+                }
+                return true;
+            }
+            return row_item<L1, L2>(A, it, buf, bad, tid, &s_empty[s]);
+        });
+    cs.colpar = colpar;
+    cs.bad    = bad;
+    return r;
+}
+
+template<int LOGL>
+__device__ __noinline__ int run_single(const args& A, int tid, cstate& cs) {
+    bool      bad = cs.bad;
+    const int r   = run_loop(
+        A, cs, [](const item& it) { return it.kind == K_SINGLE && it.lg == LOGL; },
+        [&](const item& it, long long k, unsigned char* buf) -> bool {
+            return single_items<LOGL>(A, it, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        });
+    cs.bad = bad;
+    return r;
+}
+
+template<int LOGN>
+__device__ __noinline__ int run_xr(const args& A, int tid, cstate& cs) {
+    bool      bad = cs.bad;
+    const int r   = run_loop(
+        A, cs, [](const item& it) { return it.kind == K_XR && it.lg == LOGN; },
+        [&](const item& it, long long k, unsigned char* buf) -> bool {
+            return xr_items<LOGN>(A, it, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        });
+    cs.bad = bad;
+    return r;
+}
+
+template<int LOGN>
+__device__ __noinline__ int run_xc(const args& A, int tid, cstate& cs) {
+    const bool bad = cs.bad;
+    return run_loop(
+        A, cs, [](const item& it) { return it.kind == K_XC && it.lg == LOGN; },
+        [&](const item& it, long long k, unsigned char*) -> bool {
+            if (bar1_any<NT>(bad)) return false;
+            xc_items<LOGN>(A, it, reinterpret_cast<cpx<float>*>(rg_smem), tid);
+            release_stage(k, tid);
+            return true;
+        });
+}
+
 // The arguments sit in device memory (uploaded once at creation): the item
 // functions take them by reference without a per-thread copy.
 __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ Ap) {
-    const args& A = *Ap;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t full[ST];      // the item's copies landed (XC: the producer arrived)
-    __shared__ uint64_t empty[ST];     // compute warps done with the stage, publisher past its item
-    __shared__ uint64_t slotok[ST];    // column tile: its scratch slot may be written
-    __shared__ uint64_t written[ST];   // column tile: compute warps wrote the slot
-    __shared__ int      s_item[ST];    // item index in the stage (-1: the queue is exhausted)
-    const int           tid = threadIdx.x;
+    const args& A   = *Ap;
+    const int   tid = threadIdx.x;
+    copy_table_to_smem<SUBTAB>(reinterpret_cast<cpx<float>*>(rg_smem + RING), A.tb.sub, tid, NT + 64);
     if (tid == 0) {
         for (int s = 0; s < ST; ++s) {
             s_item[s] = -2;    // no item yet
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NW + 1);
-            mbar_init(&slotok[s], 1);
-            mbar_init(&written[s], NW);
+            mbar_init(&s_full[s], 1);
+            mbar_init(&s_empty[s], NW + 1);
+            mbar_init(&s_slotok[s], 1);
+            mbar_init(&s_written[s], NW);
         }
         fence_barrier_init();
     }
     __syncthreads();
-
     if (tid >= NT + 32) {
         // ======================= publisher warp
         const int lane     = tid - NT - 32;
@@ -484,13 +635,13 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             const int      s   = (int)(k % ST);
             const uint32_t par = (uint32_t)((k / ST) & 1);
             int            ok  = 1;
-            if (lane == 0) ok = mbar_wait_bounded(&full[s], par) ? 1 : 0;
+            if (lane == 0) ok = mbar_wait_bounded(&s_full[s], par) ? 1 : 0;
             if (!__shfl_sync(0xffffffffu, ok, 0)) break;
             const int idx = s_item[s];
             if (idx < 0) break;
             const item it = A.items[idx];
             if (it.kind == K_COL) {
-                if (lane == 0) ok = mbar_wait_bounded(&written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
+                if (lane == 0) ok = mbar_wait_bounded(&s_written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
                 ++ncol[s];
                 if (!__shfl_sync(0xffffffffu, ok, 0)) {
                     if (lane == 0) atomicExch(A.error, 1);
@@ -514,7 +665,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 __syncwarp();
                 if (lane == 0) red_release_add(A.row_done + it.a, 1);
             }
-            if (lane == 0) mbar_arrive(&empty[s]);
+            if (lane == 0) mbar_arrive(&s_empty[s]);
         }
         __syncwarp();
         return;
@@ -529,7 +680,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
         long long      drain_until = -1;    // after an XC item: wait for it before the next item
         auto           wait_empty = [&](long long q) -> bool {    // stage of item q released
             int ok = 1;
-            if (lane == 0) ok = mbar_wait_bounded(&empty[(int)(q % ST)], (uint32_t)((q / ST) & 1)) ? 1 : 0;
+            if (lane == 0) ok = mbar_wait_bounded(&s_empty[(int)(q % ST)], (uint32_t)((q / ST) & 1)) ? 1 : 0;
             return __shfl_sync(0xffffffffu, ok, 0) != 0;
         };
         auto need = [&](const int* ctr, int target) -> bool {
@@ -551,11 +702,11 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             int idx = 0;
             if (lane == 0) idx = (int)atomicAdd(A.counter, 1u);
             idx = __shfl_sync(0xffffffffu, idx, 0);
-            unsigned char* buf = smem + s * STAGE;
+            unsigned char* buf = rg_smem + s * STAGE;
             if (idx >= A.nitems) {
                 if (lane == 0) {
                     s_item[s] = -1;
-                    mbar_arrive(&full[s]);
+                    mbar_arrive(&s_full[s]);
                 }
                 issued = k + 1;
                 break;
@@ -570,7 +721,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                     if (!wait_empty(q)) fail = true;
                 }
                 if (fail) break;
-                if (lane == 0) mbar_arrive(&full[s]);
+                if (lane == 0) mbar_arrive(&s_full[s]);
                 drain_until = k;
                 issued      = k + 1;
                 continue;
@@ -578,7 +729,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             if (it.kind == K_XR) {
                 switch (it.lg) {
 #define PCX_RG_ISSUE_X(LG) \
-    case LG: issue_xr<LG>(A, it, buf, &full[s], lane); break;
+    case LG: issue_xr<LG>(A, it, buf, &s_full[s], lane); break;
                     PCX_RG_XR(PCX_RG_ISSUE_X)
 #undef PCX_RG_ISSUE_X
                 default: break;
@@ -587,7 +738,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             } else if (it.kind == K_SINGLE) {
                 switch (it.lg) {
 #define PCX_RG_ISSUE_S(LG) \
-    case LG: issue_single<LG>(A, it, buf, &full[s], lane); break;
+    case LG: issue_single<LG>(A, it, buf, &s_full[s], lane); break;
                     PCX_RG_SINGLE(PCX_RG_ISSUE_S)
 #undef PCX_RG_ISSUE_S
                 default: break;
@@ -596,7 +747,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             } else if (it.kind == K_COL) {
                 switch (it.lg) {
 #define PCX_RG_ISSUE_C(LG, A1, A2) \
-    case LG: issue_col<A1, A2>(A, it, buf, &full[s], lane, pol); break;
+    case LG: issue_col<A1, A2>(A, it, buf, &s_full[s], lane, pol); break;
                     PCX_RG_FOURSTEP(PCX_RG_ISSUE_C)
 #undef PCX_RG_ISSUE_C
                 default: break;
@@ -610,7 +761,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                     break;
                 }
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&slotok[s]);
+                if (lane == 0) mbar_arrive(&s_slotok[s]);
             } else {
                 if (!need(A.col_done + it.a, A.col_tiles[it.lg])) {
                     fail = true;
@@ -618,7 +769,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 }
                 switch (it.lg) {
 #define PCX_RG_ISSUE_R(LG, A1, A2) \
-    case LG: issue_row<A1, A2>(A, it, buf, &full[s], lane); break;
+    case LG: issue_row<A1, A2>(A, it, buf, &s_full[s], lane); break;
                     PCX_RG_FOURSTEP(PCX_RG_ISSUE_R)
 #undef PCX_RG_ISSUE_R
                 default: break;
@@ -630,7 +781,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
         if (fail && lane == 0) {
             atomicExch(A.error, 1);
             for (long long q = issued - 1; q >= 0 && q >= issued - ST; --q) {
-                mbar_wait_bounded(&full[(int)(q % ST)], (uint32_t)((q / ST) & 1), 100000000ull);
+                mbar_wait_bounded(&s_full[(int)(q % ST)], (uint32_t)((q / ST) & 1), 100000000ull);
             }
         }
         __syncwarp();
@@ -638,87 +789,51 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
     }
 
     // ======================= compute warps
-    const int lane     = tid % 32;
-    int       ncol[ST] = {};
-    bool      bad      = false;
-    for (long long k = 0;; ++k) {
-        const int      s   = (int)(k % ST);
-        const uint32_t par = (uint32_t)((k / ST) & 1);
-        if (!mbar_wait_bounded(&full[s], par)) {
-            // the producer stopped: go on with whatever the stage holds and
-            // leave at the item's first barrier, which votes
-            bad = true;
-            atomicExch(A.error, 1);
-        }
-        const int idx = s_item[s];
+    cstate cs{0, 0u, false};
+    for (;;) {
+        const int idx = next_item(A, cs.k);
         if (idx < 0) {
-            // the end of the queue (or nothing to work on after a give-up):
-            // vote, so that every compute thread leaves at the same barrier
+            // the end of the queue, or a wait that gave up: vote, so that
+            // every compute thread leaves at the same barrier
             bar1_any<NT>(true);
             return;
         }
-        const item     it  = A.items[idx];
-        unsigned char* buf = smem + s * STAGE;
-        auto release = [&]() {
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
-        };
-        bool alive = true;
+        const item it = A.items[idx];
+        int        r  = RUN_LEAVE;
         if (it.kind == K_SINGLE) {
             switch (it.lg) {
 #define PCX_RG_RUN_S(LG) \
-    case LG: alive = single_items<LG>(A, it, buf, bad, tid, &empty[s]); break;
+    case LG: r = run_single<LG>(A, tid, cs); break;
                 PCX_RG_SINGLE(PCX_RG_RUN_S)
 #undef PCX_RG_RUN_S
-            default: bad = true; break;
+            default: bar1_any<NT>(true); break;
             }
-        } else if (it.kind == K_COL) {
-            auto slot_ready = [&]() -> bool {
-                const bool ok = mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1));
-                ++ncol[s];
-                if (!ok) atomicExch(A.error, 1);
-                return ok;
-            };
+        } else if (it.kind == K_COL || it.kind == K_ROW) {
             switch (it.lg) {
-#define PCX_RG_RUN_C(LG, A1, A2) \
-    case LG: alive = col_item<A1, A2>(A, it, buf, bad, tid, slot_ready, &empty[s]); break;
-                PCX_RG_FOURSTEP(PCX_RG_RUN_C)
-#undef PCX_RG_RUN_C
-            default: bad = true; break;
-            }
-            if (alive && !bad) {
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&written[s]);
+#define PCX_RG_RUN_F(LG, A1, A2) \
+    case LG: r = run_fourstep<A1, A2>(A, tid, cs); break;
+                PCX_RG_FOURSTEP(PCX_RG_RUN_F)
+#undef PCX_RG_RUN_F
+            default: bar1_any<NT>(true); break;
             }
         } else if (it.kind == K_XR) {
             switch (it.lg) {
 #define PCX_RG_RUN_XR(LG) \
-    case LG: alive = xr_items<LG>(A, it, buf, bad, tid, &empty[s]); break;
+    case LG: r = run_xr<LG>(A, tid, cs); break;
                 PCX_RG_XR(PCX_RG_RUN_XR)
 #undef PCX_RG_RUN_XR
-            default: bad = true; break;
-            }
-        } else if (it.kind == K_ROW) {
-            switch (it.lg) {
-#define PCX_RG_RUN_R(LG, A1, A2) \
-    case LG: alive = row_item<A1, A2>(A, it, buf, bad, tid, &empty[s]); break;
-                PCX_RG_FOURSTEP(PCX_RG_RUN_R)
-#undef PCX_RG_RUN_R
-            default: bad = true; break;
+            default: bar1_any<NT>(true); break;
             }
         } else {
-            if (bar1_any<NT>(bad)) return;
             switch (it.lg) {
 #define PCX_RG_RUN_X(LG) \
-    case LG: xc_items<LG>(A, it, reinterpret_cast<cpx<float>*>(smem), tid); break;
+    case LG: r = run_xc<LG>(A, tid, cs); break;
                 PCX_RG_XC(PCX_RG_RUN_X)
 #undef PCX_RG_RUN_X
-            default: bad = true; break;
+            default: bar1_any<NT>(true); break;
             }
-            release();
         }
-        if (!alive) return;
+        if (r == RUN_LEAVE) return;
     }
 }
 
@@ -825,25 +940,19 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 if (!p) return fail(PCX_ERR_CUDA);
                 h->A.tb.stw[lg] = static_cast<const cpx<float>*>(p->stwL);
             } else {
-                // the four-step split (N1 = 2^((lg+1)/2)) and its tables
+                // the four-step split (N1 = 2^((lg+1)/2)) and its twiddles; the
+                // sub-transforms' stage tables are the shared ones (SUBTAB)
                 const int l1 = (lg + 1) / 2, l2 = lg / 2;
                 const int n1 = 1 << l1, n2 = 1 << l2;
-                int       f1 = 0, f2 = 0;
-                if ((e = pcx_fourstep_tables(l1, nullptr, false, 0, &f1)) != cudaSuccess) return cuda_fail(e);
-                if ((e = pcx_fourstep_tables(l2, nullptr, false, 0, &f2)) != cudaSuccess) return cuda_fail(e);
-                void* m = nullptr;
-                if ((e = dev_alloc(((size_t)n1 + 2 * (size_t)n2 + f1 + f2) * 8, &m)) != cudaSuccess) return cuda_fail(e);
+                void*     m  = nullptr;
+                if ((e = dev_alloc(((size_t)n1 + 2 * (size_t)n2) * 8, &m)) != cudaSuccess) return cuda_fail(e);
                 auto* b = static_cast<cpx<float>*>(m);
                 h->A.tb.thi[lg]  = b;
                 h->A.tb.tlo[lg]  = b + n1;
                 h->A.tb.tb[lg]   = b + n1 + n2;
-                h->A.tb.fst1[lg] = b + n1 + 2 * n2;
-                h->A.tb.fst2[lg] = b + n1 + 2 * n2 + f1;
                 if ((e = pcx_gen_twiddles(b, n1, lg, n2, false, 0)) != cudaSuccess) return cuda_fail(e);
                 if ((e = pcx_gen_twiddles(b + n1, n2, lg, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
                 if ((e = pcx_gen_twiddles(b + n1 + n2, n2, l2 + 4, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
-                if ((e = pcx_fourstep_tables(l1, b + n1 + 2 * n2, false, 0, &f1)) != cudaSuccess) return cuda_fail(e);
-                if ((e = pcx_fourstep_tables(l2, b + n1 + 2 * n2 + f1, false, 0, &f2)) != cudaSuccess) return cuda_fail(e);
                 h->A.col_tiles[lg] = n2 / (rg::NT / std::max(1, n1 / 16));
                 h->A.row_tiles[lg] = n1 / (rg::NT / std::max(1, n2 / 16));
             }
@@ -854,6 +963,20 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 }
                 h->A.scale = 1.0f / float(size_t(1) << lg);
             }
+        }
+        // full stage tables of 2^6..2^9 points, copied to shared memory by every block
+        {
+            void* sub = nullptr;
+            if ((e = dev_alloc(rg::SUBTAB, &sub)) != cudaSuccess) return cuda_fail(e);
+            auto*     sb   = static_cast<cpx<float>*>(sub);
+            const int offs[4] = {rg::sub_off<6>(), rg::sub_off<7>(), rg::sub_off<8>(), rg::sub_off<9>()};
+            for (int l = rg::SUB_LO; l <= rg::SUB_HI; ++l) {
+                int fe = 0;
+                if ((e = pcx_fourstep_tables(l, sb + offs[l - rg::SUB_LO], false, 0, &fe)) != cudaSuccess) {
+                    return cuda_fail(e);
+                }
+            }
+            h->A.tb.sub = sub;
         }
         // correlation requests
         std::vector<rg::xc_req> xreq(n_xc);
