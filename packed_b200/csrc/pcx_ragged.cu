@@ -127,6 +127,21 @@ struct args {
     tabs               tb;
 };
 
+// What the compute warps need of the item in each stage.  The producer fills
+// it from the queue and the requests while earlier items are computed, so
+// that no chain of dependent global loads opens an item.
+struct stage_meta {
+    item        it;
+    const void* p0;    // COL: the transform's scratch slot; ROW, SINGLE: destination / stage tables
+    const void* p1;    // COL: W_N^(i*N2)
+    const void* p2;    // COL: W_N^i
+    const void* p3;    // COL: W_{16*N2}^i
+    xc_req      xq;    // XR, XC: the correlation request
+};
+__shared__ stage_meta s_meta[ST];
+__shared__ int        s_conj;     // inverse: conjugate in and out
+__shared__ float      s_scale;
+
 // Geometry of the four-step sizes: N = N1*N2 with N1 = 2^((lg+1)/2), tiles of
 // 8192 elements over NT threads of 16 points.
 template<int L1, int L2>
@@ -174,8 +189,9 @@ struct xrg {
 // Each returns false when a give-up vote made every compute thread leave.
 // They are inlined into the run loops below (one per kind and size).
 template<int LOGL>
-__device__ __forceinline__ bool single_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
+__device__ __forceinline__ bool single_items(const args& A, const stage_meta& mt, unsigned char* buf, bool bad, int tid,
                                           uint64_t* empty_bar) {
+    const item&   it = mt.it;
     using G          = sgg<LOGL>;
     using P          = typename G::P;
     constexpr int E  = P::E;
@@ -184,12 +200,13 @@ __device__ __forceinline__ bool single_items(const args& A, const item& it, unsi
     const int     m  = tid / TT;
     const int     t  = tid - m * TT;
     const float*  in = reinterpret_cast<const float*>(buf);
-    const auto*   stw = A.tb.stw[LOGL];
+    const auto*   stw  = static_cast<const cpx<float>*>(mt.p0);
+    const bool    conj = s_conj != 0;
     cpx<float>    v[E];
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
         const cpx<float> x = lds_swapped<float, SW>(in, m * G::RS + pk<LPK>(t + i * TT), 8);
-        v[i]               = {x.re, A.conj ? -x.im : x.im};
+        v[i]               = {x.re, conj ? -x.im : x.im};
     });
     stage_compute_tab<P, 0>(v, t, stw);
     // the exchanges run in place in the stage: the first (block-wide) barrier
@@ -203,7 +220,7 @@ __device__ __forceinline__ bool single_items(const args& A, const item& it, unsi
         // element t + i*TT; its packed offset splits into a base and a
         // constant only when TT is a multiple of the pack width
         float*      d  = A.req[it.a + m].dst;
-        const float sc = A.scale, sim = A.conj ? -A.scale : A.scale;
+        const float sc = s_scale, sim = conj ? -sc : sc;
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
             const int     o = pk<LPK>(t + i * TT);
@@ -217,8 +234,8 @@ __device__ __forceinline__ bool single_items(const args& A, const item& it, unsi
 // The stage is free once this returns true (the caller releases it); the
 // scratch stores wait for `slot_ready`.
 template<int L1, int L2, class SlotWait>
-__device__ __forceinline__ bool col_item(const args& A, const item& it, unsigned char* buf, bool& bad, int tid, SlotWait&& slot_ready,
-                         uint64_t* empty_bar) {
+__device__ __forceinline__ bool col_item(const stage_meta& mt, unsigned char* buf, bool& bad, int tid, SlotWait&& slot_ready,
+                                         uint64_t* empty_bar) {
     using F          = fsg<L1, L2>;
     using P1         = typename F::P1;
     constexpr int E  = P1::E;
@@ -227,19 +244,19 @@ __device__ __forceinline__ bool col_item(const args& A, const item& it, unsigned
     constexpr int N2 = F::N2;
     const int     c  = tid % C;
     const int     t  = tid / C;
-    const int     n2 = it.b * C + c;
-    const fft_req& r = A.req[it.a];
+    const int     n2 = mt.it.b * C + c;
     // four-step twiddle inputs, used after the stages
     const uint32_t   e0 = (uint32_t)t * (uint32_t)n2;
-    const cpx<float> th = ldg_cpx(A.tb.thi[L1 + L2] + (e0 >> L2));
-    const cpx<float> tl = ldg_cpx(A.tb.tlo[L1 + L2] + (e0 & (N2 - 1)));
-    const cpx<float> tu = ldg_cpx(A.tb.tb[L1 + L2] + n2);
-    const float*     in = reinterpret_cast<const float*>(buf);
+    const cpx<float> th = ldg_cpx(static_cast<const cpx<float>*>(mt.p1) + (e0 >> L2));
+    const cpx<float> tl = ldg_cpx(static_cast<const cpx<float>*>(mt.p2) + (e0 & (N2 - 1)));
+    const cpx<float> tu = ldg_cpx(static_cast<const cpx<float>*>(mt.p3) + n2);
+    const float*     in   = reinterpret_cast<const float*>(buf);
+    const bool       conj = s_conj != 0;
     cpx<float>       v[E];
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
         const cpx<float> x = lds_swapped<float, 16>(in, (t + i * TT) * F::SEG + pk<LPK>(c), 8);
-        v[i]               = {x.re, A.conj ? -x.im : x.im};
+        v[i]               = {x.re, conj ? -x.im : x.im};
     });
     const auto* fst = sub_tab<L1>();
     stage_compute_tab<P1, 0>(v, t, fst);
@@ -252,7 +269,7 @@ __device__ __forceinline__ bool col_item(const args& A, const item& it, unsigned
     if (tid % 32 == 0) mbar_arrive(empty_bar);
     if (!slot_ready()) bad = true;
     if (!bad) {
-        cpx<float>* dst = A.tb.scratch[L1 + L2] + (long long)r.slot * (F::N1 * N2) + (long long)t * N2 + n2;
+        cpx<float>* dst = const_cast<cpx<float>*>(static_cast<const cpx<float>*>(mt.p0)) + (long long)t * N2 + n2;
         apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<float> o) {
             constexpr int i             = decltype(ic)::value;
             dst[(long long)i * TT * N2] = o;
@@ -262,7 +279,7 @@ __device__ __forceinline__ bool col_item(const args& A, const item& it, unsigned
 }
 
 template<int L1, int L2>
-__device__ __forceinline__ bool row_item(const args& A, const item& it, unsigned char* buf, bool bad, int tid, uint64_t* empty_bar) {
+__device__ __forceinline__ bool row_item(const stage_meta& mt, unsigned char* buf, bool bad, int tid, uint64_t* empty_bar) {
     using F          = fsg<L1, L2>;
     using P2         = typename F::P2;
     constexpr int E  = P2::E;
@@ -272,7 +289,7 @@ __device__ __forceinline__ bool row_item(const args& A, const item& it, unsigned
     const int     t   = (tid / 8) % TT;
     const int     mhi = tid / (8 * TT);
     const int     m   = mhi * 8 + mlo;
-    const int     k1  = it.b * F::CR + m;
+    const int     k1  = mt.it.b * F::CR + m;
     const cpx<float>* in = reinterpret_cast<const cpx<float>*>(buf) + m * F::RSI + t;
     cpx<float>        v[E];
     static_for<E>([&](auto ic) {
@@ -287,8 +304,8 @@ __device__ __forceinline__ bool row_item(const args& A, const item& it, unsigned
     fence_proxy_async_smem();
     __syncwarp();
     if (tid % 32 == 0) mbar_arrive(empty_bar);
-    float*      dst = A.req[it.a].dst + pk<LPK>(t * N1 + k1);
-    const float sc = A.scale, sim = A.conj ? -A.scale : A.scale;
+    float*      dst = const_cast<float*>(static_cast<const float*>(mt.p0)) + pk<LPK>(t * N1 + k1);
+    const float sc = s_scale, sim = s_conj ? -sc : sc;
     static_for<E>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         __stcs(dst + 2 * i * TT * N1, v[i].re * sc);
@@ -299,7 +316,8 @@ __device__ __forceinline__ bool row_item(const args& A, const item& it, unsigned
 
 // Up to M overlap-save blocks of one correlation; buf is the whole ring.
 template<int LOGN>
-__device__ __forceinline__ void xc_items(const args& A, const item& it, cpx<float>* buf, int tid) {
+__device__ __forceinline__ void xc_items(const args& A, const stage_meta& mt, cpx<float>* buf, int tid) {
+    const item&   it  = mt.it;
     constexpr int EPT = LOGN >= 14 ? 32 : 16;
     using P           = splan<LOGN, EPT>;
     static_assert(fs_full_tw_size<P>() == fs_full_tw_size<splan<LOGN>>(), "same stage radices");
@@ -309,7 +327,7 @@ __device__ __forceinline__ void xc_items(const args& A, const item& it, cpx<floa
     constexpr int M   = NT / TT;
     using X           = xch_blocked<L, M>;
     static_assert(X::size * 8 <= RING, "correlation workspace fits the ring");
-    const xc_req& q   = A.xreq[it.a];
+    const xc_req  q   = mt.xq;
     const int     m   = tid / TT;
     const int     t   = tid - m * TT;
     // load M windows (blocks b .. b+count-1), zero outside the signal
@@ -362,15 +380,16 @@ __device__ __forceinline__ void xc_items(const args& A, const item& it, cpx<floa
 // Not inlined into its run loop: the correlation's two transforms need every
 // register (inlined, the loop's state spilled).
 template<int LOGN>
-__device__ __noinline__ bool xr_items(const args& A, const item& it, unsigned char* buf, bool bad, int tid,
+__device__ __noinline__ bool xr_items(const args& A, const stage_meta& mt, unsigned char* buf, bool bad, int tid,
                                       uint64_t* empty_bar) {
+    const item&   it = mt.it;
     using G          = xrg<LOGN>;
     using P          = typename G::P;
     constexpr int E  = P::E;
     constexpr int TT = G::TT;
     constexpr int SW = TT >= 32 ? 16 : 0;
     static_assert(TT % 8 == 0, "whole packs per thread stride");
-    const xc_req& q  = A.xreq[it.a];
+    const xc_req& q  = mt.xq;
     const int     m  = tid / TT;
     const int     t  = tid - m * TT;
     const long long b0 = (long long)(it.b + m) * q.step;
@@ -519,8 +538,8 @@ __device__ __forceinline__ void release_stage(long long k, int tid) {
     if (tid % 32 == 0) mbar_arrive(&s_empty[(int)(k % ST)]);
 }
 
-// Runs items from cs.k on while Match(item) holds, with Work(item, k, stage)
-// returning false when the block leaves.
+// Runs items from cs.k on while Match(item) holds, with Work(stage_meta, k,
+// stage) returning false when the block leaves.
 template<class Match, class Work>
 __device__ __forceinline__ int run_loop(const args& A, cstate& cs, Match&& match, Work&& work) {
     long long k = cs.k;
@@ -533,9 +552,9 @@ __device__ __forceinline__ int run_loop(const args& A, cstate& cs, Match&& match
             break;
         }
         if (idx < 0) break;    // the dispatch votes and leaves
-        const item it = A.items[idx];
-        if (!match(it)) break;
-        if (!work(it, k, rg_smem + (int)(k % ST) * STAGE)) {
+        const stage_meta& mt = s_meta[(int)(k % ST)];
+        if (!match(mt.it)) break;
+        if (!work(mt, k, rg_smem + (int)(k % ST) * STAGE)) {
             r = RUN_LEAVE;
             break;
         }
@@ -550,23 +569,23 @@ __device__ __noinline__ int run_fourstep(const args& A, int tid, cstate& cs) {
     bool     bad    = cs.bad;
     const int r = run_loop(
         A, cs, [](const item& it) { return (it.kind == K_COL || it.kind == K_ROW) && it.lg == L1 + L2; },
-        [&](const item& it, long long k, unsigned char* buf) -> bool {
+        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
             const int s = (int)(k % ST);
-            if (it.kind == K_COL) {
+            if (mt.it.kind == K_COL) {
                 auto slot_ready = [&]() -> bool {
                     const bool ok = mbar_wait_bounded(&s_slotok[s], (colpar >> s) & 1u);
                     colpar ^= 1u << s;
                     if (!ok) atomicExch(A.error, 1);
                     return ok;
                 };
-                if (!col_item<L1, L2>(A, it, buf, bad, tid, slot_ready, &s_empty[s])) return false;
+                if (!col_item<L1, L2>(mt, buf, bad, tid, slot_ready, &s_empty[s])) return false;
                 if (!bad) {
                     __syncwarp();
                     if (tid % 32 == 0) mbar_arrive(&s_written[s]);
                 }
                 return true;
             }
-            return row_item<L1, L2>(A, it, buf, bad, tid, &s_empty[s]);
+            return row_item<L1, L2>(mt, buf, bad, tid, &s_empty[s]);
         });
     cs.colpar = colpar;
     cs.bad    = bad;
@@ -578,8 +597,8 @@ __device__ __noinline__ int run_single(const args& A, int tid, cstate& cs) {
     bool      bad = cs.bad;
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_SINGLE && it.lg == LOGL; },
-        [&](const item& it, long long k, unsigned char* buf) -> bool {
-            return single_items<LOGL>(A, it, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
+            return single_items<LOGL>(A, mt, buf, bad, tid, &s_empty[(int)(k % ST)]);
         });
     cs.bad = bad;
     return r;
@@ -590,8 +609,8 @@ __device__ __noinline__ int run_xr(const args& A, int tid, cstate& cs) {
     bool      bad = cs.bad;
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_XR && it.lg == LOGN; },
-        [&](const item& it, long long k, unsigned char* buf) -> bool {
-            return xr_items<LOGN>(A, it, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
+            return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[(int)(k % ST)]);
         });
     cs.bad = bad;
     return r;
@@ -602,9 +621,9 @@ __device__ __noinline__ int run_xc(const args& A, int tid, cstate& cs) {
     const bool bad = cs.bad;
     return run_loop(
         A, cs, [](const item& it) { return it.kind == K_XC && it.lg == LOGN; },
-        [&](const item& it, long long k, unsigned char*) -> bool {
+        [&](const stage_meta& mt, long long k, unsigned char*) -> bool {
             if (bar1_any<NT>(bad)) return false;
-            xc_items<LOGN>(A, it, reinterpret_cast<cpx<float>*>(rg_smem), tid);
+            xc_items<LOGN>(A, mt, reinterpret_cast<cpx<float>*>(rg_smem), tid);
             release_stage(k, tid);
             return true;
         });
@@ -617,6 +636,8 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
     const int   tid = threadIdx.x;
     copy_table_to_smem<SUBTAB>(reinterpret_cast<cpx<float>*>(rg_smem + RING), A.tb.sub, tid, NT + 64);
     if (tid == 0) {
+        s_conj  = A.conj;
+        s_scale = A.scale;
         for (int s = 0; s < ST; ++s) {
             s_item[s] = -2;    // no item yet
             mbar_init(&s_full[s], 1);
@@ -712,7 +733,24 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 break;
             }
             const item it = A.items[idx];
-            if (lane == 0) s_item[s] = idx;
+            if (lane == 0) {
+                // published to the compute warps by this lane's arrival on full[s]
+                stage_meta& mt = s_meta[s];
+                mt.it          = it;
+                if (it.kind == K_COL) {
+                    mt.p0 = A.tb.scratch[it.lg] + (long long)A.req[it.a].slot * (1LL << it.lg);
+                    mt.p1 = A.tb.thi[it.lg];
+                    mt.p2 = A.tb.tlo[it.lg];
+                    mt.p3 = A.tb.tb[it.lg];
+                } else if (it.kind == K_ROW) {
+                    mt.p0 = A.req[it.a].dst;
+                } else if (it.kind == K_SINGLE) {
+                    mt.p0 = A.tb.stw[it.lg];
+                } else {
+                    mt.xq = A.xreq[it.a];
+                }
+                s_item[s] = idx;
+            }
             __syncwarp();
             if (it.kind == K_XC) {
                 // the correlation uses the whole ring: the other stages' items
