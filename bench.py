@@ -617,7 +617,7 @@ class C5Ragged:
     n_fft, n_xc = 10000, 500
 
     def config(self, world):
-        return {"workload": "C5: 10,000 complex64 FFTs, N log-uniform 2^8..2^18, plus 500 correlations "
+        return {"workload": f"C5: {self.n_fft:,} complex64 FFTs, N log-uniform 2^8..2^18, plus {self.n_xc} correlations "
                             "(S log-uniform 2^12..2^20, K log-uniform 64..8192, N_fft per request from "
                             "correlation_fft_size(K)), "
                             "N(0,1) seed 5; one persistent launch from a device work queue replayed as a CUDA "
@@ -688,6 +688,39 @@ class C5Ragged:
 
     def bytes_per_step(self):
         return self.part_bytes("ragged_graph")
+
+    def accuracy(self):
+        """Worst relative L2 error over every transform and every correlation of
+        one ragged replay, against FP64 references computed on the device from
+        the same FP32 inputs (torch.fft as the checker), outside the timed region."""
+        import torch
+
+        def rows(t, n):    # pack-8 rows -> complex128 [rows, n]
+            v = t.reshape(-1, n // 8, 2, 8).double()
+            return torch.complex(v[:, :, 0, :].reshape(-1, n), v[:, :, 1, :].reshape(-1, n))
+
+        def rel(got, want):
+            return torch.linalg.vector_norm(got - want, dim=-1) / torch.linalg.vector_norm(want, dim=-1)
+
+        self.batch()
+        torch.cuda.synchronize()
+        self.batch.status()
+        w_fft = w_xc = 0.0
+        for lg, (cnt, src, dst, _) in self.groups.items():
+            n = 1 << lg
+            for r0 in range(0, cnt, 128):
+                r1 = min(cnt, r0 + 128)
+                e = rel(rows(dst[r0 * 2 * n:r1 * 2 * n], n), torch.fft.fft(rows(src[r0 * 2 * n:r1 * 2 * n], n)))
+                w_fft = max(w_fft, float(e.max()))
+        for y, x, s, taps, _ in self.xcs:
+            k = taps.size()
+            kp = (k + 7) // 8 * 8
+            g = rows(taps.data[: 2 * kp], kp)[0, :k]
+            L = 1 << int(np.ceil(np.log2(s + k)))
+            want = torch.fft.ifft(torch.fft.fft(rows(x, s)[0], L) * torch.conj(torch.fft.fft(g, L)))[:s]
+            w_xc = max(w_xc, float(rel(rows(y, s)[0], want)))
+        return {"ragged_fft_max_rel_l2": w_fft, "ragged_xcorr_max_rel_l2": w_xc,
+                "transforms": sum(c for c, _, _, _ in self.groups.values()), "correlations": len(self.xcs)}
 
     def e2e(self, torch, stream):
         return None
@@ -773,6 +806,8 @@ def main() -> None:
     ap.add_argument("--points", type=int, default=None, help="log2 complex points per buffer (profiling captures)")
     ap.add_argument("--sizes", type=str, default=None, help="comma list of log2 N (profiling captures)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (built-in form choice)")
+    ap.add_argument("--items", type=float, default=None,
+                    help="c5: fraction of the 10,000 FFTs and 500 correlations (profiling captures)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -785,6 +820,9 @@ def main() -> None:
         wl.log_ns = [int(v) for v in args.sizes.split(",")]
     if args.no_tune:
         wl.tune = False
+    if args.items is not None and hasattr(wl, "n_xc"):
+        wl.n_fft = max(1, int(round(wl.n_fft * args.items)))
+        wl.n_xc = max(1, int(round(wl.n_xc * args.items)))
     config = wl.config(world)
 
     if args.impl == "reference":

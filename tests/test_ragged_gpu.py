@@ -64,3 +64,68 @@ def test_ragged_matches_plain_launch_bits():
     got = torch.cat(dst)
     assert rel_l2(O.unpack(got.cpu().numpy().reshape(5, -1), n, 8),
                   O.unpack(ref.cpu().numpy().reshape(5, -1), n, 8)) < TOL[np.float32]
+
+
+def _unpack_rows(t: torch.Tensor, n: int) -> torch.Tensor:
+    """Pack-8 rows of n points (n a multiple of 8) -> complex128 [rows, n], on the device."""
+    v = t.reshape(-1, n // 8, 2, 8).double()
+    return torch.complex(v[:, :, 0, :].reshape(-1, n), v[:, :, 1, :].reshape(-1, n))
+
+
+def _row_rel_l2(got: torch.Tensor, want: torch.Tensor) -> torch.Tensor:
+    return torch.linalg.vector_norm(got - want, dim=-1) / torch.linalg.vector_norm(want, dim=-1)
+
+
+def test_full_c5_scale_against_fp64():
+    """The full C5 configuration (10,000 FFTs of 2^8..2^18 points and 500
+    correlations, seed 5, as the benchmark builds it) in one graph replay,
+    every transform and every correlation against an FP64 reference computed
+    on the device from the same FP32 inputs (torch.fft as the checker): each
+    one within the FP32 bar of 2e-6 relative L2."""
+    from packed_b200 import correlation_fft_size
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    lgs = np.floor(rng.uniform(8, 19, 10000)).astype(int)
+    groups, ffts = {}, []
+    for lg in sorted(set(lgs.tolist())):
+        cnt, n = int((lgs == lg).sum()), 1 << lg
+        src = torch.randn(cnt * 2 * n, device=dev)
+        dst = torch.full_like(src, float("nan"))
+        groups[lg] = (cnt, src, dst)
+        ffts += [(dst[i * 2 * n:(i + 1) * 2 * n], src[i * 2 * n:(i + 1) * 2 * n], n) for i in range(cnt)]
+    s_all = np.floor(2 ** rng.uniform(12, 20, 500)).astype(int) // 8 * 8
+    k_all = np.floor(2 ** rng.uniform(6, 13, 500)).astype(int)
+    xcs = []
+    for s, k in zip(s_all, k_all):
+        taps = vector.from_complex(rng.standard_normal(k) + 1j * rng.standard_normal(k), device=dev)
+        x = torch.randn(2 * int(s), device=dev)
+        xcs.append((torch.full_like(x, float("nan")), x, int(s), taps, correlation_fft_size(int(k))))
+    batch = ragged_batch(ffts, xcs)
+    batch()
+    for _, _, d in groups.values():
+        d.fill_(float("nan"))
+    for y, _, _, _, _ in xcs:
+        y.fill_(float("nan"))
+    batch()    # the second replay is checked
+    torch.cuda.synchronize()
+    batch.status()
+    worst = 0.0
+    for lg, (cnt, src, dst) in groups.items():
+        n = 1 << lg
+        for r0 in range(0, cnt, 128):    # bounded FP64 working set
+            r1 = min(cnt, r0 + 128)
+            want = torch.fft.fft(_unpack_rows(src[r0 * 2 * n:r1 * 2 * n], n))
+            err = _row_rel_l2(_unpack_rows(dst[r0 * 2 * n:r1 * 2 * n], n), want)
+            assert not torch.isnan(err).any(), (n, r0)
+            worst = max(worst, float(err.max()))
+            assert float(err.max()) < TOL[np.float32], (n, r0, float(err.max()))
+    for y, x, s, taps, nf in xcs:
+        k = taps.size()
+        g = _unpack_rows(taps.data[: 2 * ((k + 7) // 8 * 8)], (k + 7) // 8 * 8)[0, :k]
+        L = 1 << int(np.ceil(np.log2(s + k)))
+        want = torch.fft.ifft(torch.fft.fft(_unpack_rows(x, s)[0], L) * torch.conj(torch.fft.fft(g, L)))[:s]
+        err = float(_row_rel_l2(_unpack_rows(y, s)[0], want))
+        worst = max(worst, err)
+        assert err < TOL[np.float32], (s, k, nf, err)
+    print(f"full C5: worst relative L2 {worst:.3g}")
