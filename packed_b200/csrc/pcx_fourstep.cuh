@@ -133,9 +133,9 @@ __device__ __forceinline__ bool fs_wait(const int* p, int target) {
 }
 
 struct fs_item {
-    int       row;     // 0: column tile, 1: row tile
-    long long r;       // transform
-    int       tile;
+    int row;     // 0: column tile, 1: row tile
+    int r;       // transform
+    int tile;
 };
 
 // counter += 1 with release semantics at GPU scope: this thread's earlier
@@ -144,19 +144,22 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
     asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ fs_item fs_decode(long long j, long long batch, int lag, int TC, int TR) {
-    const long long A = (long long)lag * TC;
-    if (j < A) return {0, j / TC, (int)(j % TC)};
+// Item j of the queue (32-bit: the launch holds fewer than 2^31 items).  TC
+// and TR are powers of two, TC + TR a constant: no division is a real one.
+template<int TC, int TR>
+__device__ __forceinline__ fs_item fs_decode(uint32_t j, uint32_t batch, uint32_t lag) {
+    const uint32_t A = lag * TC;
+    if (j < A) return {0, (int)(j / TC), (int)(j % TC)};
     j -= A;
-    const long long G      = TC + TR;
-    const long long steady = (batch - lag) * G;
+    constexpr uint32_t G      = TC + TR;
+    const uint32_t     steady = (batch - lag) * G;
     if (j < steady) {
-        const long long q = j / G;
-        const int       w = (int)(j - q * G);
-        return w < TC ? fs_item{0, q + lag, w} : fs_item{1, q, w - TC};
+        const uint32_t q = j / G;
+        const int      w = (int)(j - q * G);
+        return w < TC ? fs_item{0, (int)(q + lag), w} : fs_item{1, (int)q, w - TC};
     }
     j -= steady;
-    return {1, batch - lag + j / TR, (int)(j % TR)};
+    return {1, (int)(batch - lag + j / TR), (int)(j % TR)};
 }
 
 template<class T, int LOGN1, int LOGN2, int MINB, int ST_>
@@ -196,8 +199,10 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
     __shared__ uint64_t written[ST];   // column tile: compute warps wrote the slot
     cpx<T>*             scr   = reinterpret_cast<cpx<T>*>(a.scratch);
     const int           tid   = threadIdx.x;
-    const long long     items = a.batch * (TC + TR);
-    const long long     G     = gridDim.x;
+    const uint32_t      items = (uint32_t)a.batch * (uint32_t)(TC + TR);    // < 2^31 (host check)
+    const uint32_t      batch = (uint32_t)a.batch;
+    const uint32_t      lag   = (uint32_t)a.lag;
+    const uint32_t      G     = gridDim.x;
     const long long     mask  = a.nslot - 1;
 
     if constexpr (SH) {
@@ -218,20 +223,19 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
     if (tid >= NT + 32) {
         // ======================= publisher warp
         const int lane    = tid - NT - 32;
-        int       ncol[ST] = {};
+        uint32_t  colpar  = 0;    // bit s: parity of the next `written` wait on stage s
         bool      fail    = false;
-        long long k       = 0;
-        for (long long j = blockIdx.x; j < items && !fail; j += G, ++k) {
-            const int      s   = (int)(k % ST);
-            const uint32_t par = (uint32_t)((k / ST) & 1);
-            const fs_item  it  = fs_decode(j, a.batch, a.lag, TC, TR);
+        int       s       = 0;
+        uint32_t  par     = 0;
+        for (uint32_t j = blockIdx.x; j < items && !fail; j += G, s = s + 1 == ST ? 0 : s + 1, par ^= s == 0) {
+            const fs_item  it  = fs_decode<TC, TR>(j, batch, lag);
             int            ok  = 1;
             if (!it.row) {
                 // the compute warps' stores of the tile are done: make them
                 // visible to other CTAs' TMA reads, then count the tile
-                if (lane == 0) ok = mbar_wait_bounded(&written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
+                if (lane == 0) ok = mbar_wait_bounded(&written[s], (colpar >> s) & 1u) ? 1 : 0;
                 ok = __shfl_sync(0xffffffffu, ok, 0);
-                ++ncol[s];
+                colpar ^= 1u << s;
                 if (ok && lane == 0) {
                     fence_proxy_async_global();
                     red_release_add(a.col_done + it.r, 1);
@@ -273,9 +277,9 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             if (lane == 0) ok = fs_wait(ctr, target) ? 1 : 0;
             return __shfl_sync(0xffffffffu, ok, 0) != 0;
         };
-        for (long long j = blockIdx.x; j < items && !fail; j += G, ++k) {
-            const int      s   = (int)(k % ST);
-            const uint32_t par = (uint32_t)((k / ST) & 1);
+        int            s      = 0;
+        uint32_t       par    = 0;
+        for (uint32_t j = blockIdx.x; j < items && !fail; j += G, ++k, s = s + 1 == ST ? 0 : s + 1, par ^= s == 0) {
             if (k >= ST) {
                 int ok = 1;
                 if (lane == 0) ok = mbar_wait_bounded(&empty[s], par ^ 1u) ? 1 : 0;
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
                     break;
                 }
             }
-            const fs_item  it  = fs_decode(j, a.batch, a.lag, TC, TR);
+            const fs_item  it  = fs_decode<TC, TR>(j, batch, lag);
             unsigned char* buf = ring + s * F::STAGE;
             if (!it.row) {
                 // the source tile does not depend on anything: copy it first
@@ -341,15 +345,14 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
     // in `bad`; the work of that item goes on with whatever the stage holds,
     // nothing is stored, and at the next exchange barrier, which doubles as
     // a vote, every compute thread leaves together (run_stages_full).
-    const int lane     = tid % 32;
-    int       ncol[ST] = {};
-    bool      bad      = false;
-    long long k        = 0;
-    cpx<T>*   xsep     = reinterpret_cast<cpx<T>*>(smem + ST * F::STAGE);    // exchange buffer when !IP
-    for (long long j = blockIdx.x; j < items; j += G, ++k) {
-        const int      s   = (int)(k % ST);
-        const uint32_t par = (uint32_t)((k / ST) & 1);
-        const fs_item it = fs_decode(j, a.batch, a.lag, TC, TR);
+    const int lane   = tid % 32;
+    uint32_t  colpar = 0;    // bit s: parity of the next slot hand-off on stage s
+    bool      bad    = false;
+    int       s      = 0;
+    uint32_t  par    = 0;
+    cpx<T>*   xsep   = reinterpret_cast<cpx<T>*>(smem + ST * F::STAGE);    // exchange buffer when !IP
+    for (uint32_t j = blockIdx.x; j < items; j += G, s = s + 1 == ST ? 0 : s + 1, par ^= s == 0) {
+        const fs_item it = fs_decode<TC, TR>(j, batch, lag);
         cpx<T>*        xch = IP ? reinterpret_cast<cpx<T>*>(ring + s * F::STAGE) : xsep;
         // the stage is no longer read: it may be refilled (the publisher adds
         // its own arrival once it has passed the item)
@@ -391,13 +394,13 @@ __global__ void __launch_bounds__(fs_cfg<T, LOGN1, LOGN2, MINB, ST_>::NT + 64, M
             stage_compute_tab<P1, 0>(v, t, stw1);
             if (run_stages_full<P1, typename F::X1, SH, NT, typename F::PT1>(v, xch, c, t, stw1, bad)) return;
             if constexpr (IP) release_stage();
-            if (!mbar_wait_bounded(&slotok[s], (uint32_t)(ncol[s] & 1))) {
+            if (!mbar_wait_bounded(&slotok[s], (colpar >> s) & 1u)) {
                 // the producer gave up on this slot: nothing is written, and
                 // the compute warps leave at the next item's vote
                 bad = true;
                 atomicExch(a.error, 1);
             }
-            ++ncol[s];
+            colpar ^= 1u << s;
             if (!bad) {
                 cpx<T>* dst = scr + (it.r & mask) * (long long)(N1 * N2) + (long long)t * N2 + n2;
                 apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<T> o) {

@@ -27,6 +27,7 @@ cudaError_t launch_fs(const fs_args& a, cudaStream_t st, int sms, bool attr_only
     }
     const long long items = a.batch * (F::TC + F::TR);
     if (items == 0) return cudaSuccess;
+    if (items >= (1LL << 31)) return cudaErrorInvalidValue;    // the kernel counts items in 32 bits
     // 3-D view of the source: [transform][n1][2*N2 reals], box = 2*C reals x min(N1, 256) rows
     CUtensorMap      map;
     const cuuint64_t dims[3]    = {(cuuint64_t)2 << LOGN2, (cuuint64_t)1 << LOGN1, (cuuint64_t)a.batch};
