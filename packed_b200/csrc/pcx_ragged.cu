@@ -511,55 +511,58 @@ __device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint
 
 // Compute-warp state carried from one run to the next.
 struct cstate {
-    long long k;         // position of the next item in the block's ring sequence
+    int       s;         // stage of the next item in the block's ring sequence
+    uint32_t  par;       // parity of that stage's current phase
     uint32_t  colpar;    // bit s: parity of the next slot hand-off wait on stage s
     bool      bad;       // a bounded wait of this thread gave up
 };
 
 enum : int { RUN_NEXT = 0, RUN_LEAVE = 1 };
 
-// Waits (bounded) until item k's copies have landed and returns its index:
+// Waits (bounded) until the copies of the item in stage s (phase parity par)
+// have landed and returns its index:
 // -1 at the end of the queue, -2 when the wait gave up (the thread then votes
 // at barrier 1, where every other compute thread meets it at the first
 // barrier of its next item, and all of them leave).
-__device__ __forceinline__ int next_item(const args& A, long long k) {
-    const int s = (int)(k % ST);
-    if (!mbar_wait_bounded(&s_full[s], (uint32_t)((k / ST) & 1))) {
+__device__ __forceinline__ int next_item(const args& A, int s, uint32_t par) {
+    if (!mbar_wait_bounded(&s_full[s], par)) {
         atomicExch(A.error, 1);
         return -2;
     }
     return s_item[s];
 }
 
-// The stage of item k is no longer read: it may be refilled.
-__device__ __forceinline__ void release_stage(long long k, int tid) {
+// Stage s is no longer read: it may be refilled.
+__device__ __forceinline__ void release_stage(int s, int tid) {
     fence_proxy_async_smem();
     __syncwarp();
-    if (tid % 32 == 0) mbar_arrive(&s_empty[(int)(k % ST)]);
+    if (tid % 32 == 0) mbar_arrive(&s_empty[s]);
 }
 
-// Runs items from cs.k on while Match(item) holds, with Work(stage_meta, k,
-// stage) returning false when the block leaves.
+// Runs the items from stage cs.s on while Match(item) holds, with
+// Work(stage_meta, s, stage buffer) returning false when the block leaves.
 template<class Match, class Work>
 __device__ __forceinline__ int run_loop(const args& A, cstate& cs, Match&& match, Work&& work) {
-    long long k = cs.k;
-    int       r = RUN_NEXT;
-    for (;; ++k) {
-        const int idx = next_item(A, k);
+    int      s   = cs.s;
+    uint32_t par = cs.par;
+    int      r   = RUN_NEXT;
+    for (;; s = s + 1 == ST ? 0 : s + 1, par ^= s == 0) {
+        const int idx = next_item(A, s, par);
         if (idx == -2) {
             bar1_any<NT>(true);
             r = RUN_LEAVE;
             break;
         }
         if (idx < 0) break;    // the dispatch votes and leaves
-        const stage_meta& mt = s_meta[(int)(k % ST)];
+        const stage_meta& mt = s_meta[s];
         if (!match(mt.it)) break;
-        if (!work(mt, k, rg_smem + (int)(k % ST) * STAGE)) {
+        if (!work(mt, s, rg_smem + s * STAGE)) {
             r = RUN_LEAVE;
             break;
         }
     }
-    cs.k = k;
+    cs.s   = s;
+    cs.par = par;
     return r;
 }
 
@@ -569,8 +572,7 @@ __device__ __noinline__ int run_fourstep(const args& A, int tid, cstate& cs) {
     bool     bad    = cs.bad;
     const int r = run_loop(
         A, cs, [](const item& it) { return (it.kind == K_COL || it.kind == K_ROW) && it.lg == L1 + L2; },
-        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
-            const int s = (int)(k % ST);
+        [&](const stage_meta& mt, int s, unsigned char* buf) -> bool {
             if (mt.it.kind == K_COL) {
                 auto slot_ready = [&]() -> bool {
                     const bool ok = mbar_wait_bounded(&s_slotok[s], (colpar >> s) & 1u);
@@ -597,8 +599,8 @@ __device__ __noinline__ int run_single(const args& A, int tid, cstate& cs) {
     bool      bad = cs.bad;
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_SINGLE && it.lg == LOGL; },
-        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
-            return single_items<LOGL>(A, mt, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        [&](const stage_meta& mt, int s, unsigned char* buf) -> bool {
+            return single_items<LOGL>(A, mt, buf, bad, tid, &s_empty[s]);
         });
     cs.bad = bad;
     return r;
@@ -609,8 +611,8 @@ __device__ __noinline__ int run_xr(const args& A, int tid, cstate& cs) {
     bool      bad = cs.bad;
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_XR && it.lg == LOGN; },
-        [&](const stage_meta& mt, long long k, unsigned char* buf) -> bool {
-            return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[(int)(k % ST)]);
+        [&](const stage_meta& mt, int s, unsigned char* buf) -> bool {
+            return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
         });
     cs.bad = bad;
     return r;
@@ -621,10 +623,10 @@ __device__ __noinline__ int run_xc(const args& A, int tid, cstate& cs) {
     const bool bad = cs.bad;
     return run_loop(
         A, cs, [](const item& it) { return it.kind == K_XC && it.lg == LOGN; },
-        [&](const stage_meta& mt, long long k, unsigned char*) -> bool {
+        [&](const stage_meta& mt, int s, unsigned char*) -> bool {
             if (bar1_any<NT>(bad)) return false;
             xc_items<LOGN>(A, mt, reinterpret_cast<cpx<float>*>(rg_smem), tid);
-            release_stage(k, tid);
+            release_stage(s, tid);
             return true;
         });
 }
@@ -650,20 +652,18 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
     __syncthreads();
     if (tid >= NT + 32) {
         // ======================= publisher warp
-        const int lane     = tid - NT - 32;
-        int       ncol[ST] = {};
-        for (long long k = 0;; ++k) {
-            const int      s   = (int)(k % ST);
-            const uint32_t par = (uint32_t)((k / ST) & 1);
-            int            ok  = 1;
-            if (lane == 0) ok = mbar_wait_bounded(&s_full[s], par) ? 1 : 0;
+        const int lane   = tid - NT - 32;
+        uint32_t  colpar = 0;    // bit s: parity of the next `written` wait on stage s
+        for (int s = 0, par = 0;; s = s + 1 == ST ? 0 : s + 1, par ^= s == 0) {
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait_bounded(&s_full[s], (uint32_t)par) ? 1 : 0;
             if (!__shfl_sync(0xffffffffu, ok, 0)) break;
             const int idx = s_item[s];
             if (idx < 0) break;
             const item it = A.items[idx];
             if (it.kind == K_COL) {
-                if (lane == 0) ok = mbar_wait_bounded(&s_written[s], (uint32_t)(ncol[s] & 1)) ? 1 : 0;
-                ++ncol[s];
+                if (lane == 0) ok = mbar_wait_bounded(&s_written[s], (colpar >> s) & 1u) ? 1 : 0;
+                colpar ^= 1u << s;
                 if (!__shfl_sync(0xffffffffu, ok, 0)) {
                     if (lane == 0) atomicExch(A.error, 1);
                     break;
@@ -827,9 +827,9 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
     }
 
     // ======================= compute warps
-    cstate cs{0, 0u, false};
+    cstate cs{0, 0u, 0u, false};
     for (;;) {
-        const int idx = next_item(A, cs.k);
+        const int idx = next_item(A, cs.s, cs.par);
         if (idx < 0) {
             // the end of the queue, or a wait that gave up: vote, so that
             // every compute thread leaves at the same barrier

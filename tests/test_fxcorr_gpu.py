@@ -98,9 +98,12 @@ def test_c3_shape_reduced_channels():
 
 
 @pytest.mark.slow
-def test_c3_full_size_sampled():
-    # full C3: 256 channels x 2^20, in place; 64 random outputs per 8 channels
-    # checked against direct FP64 sums (size-independent property)
+def test_c3_full_size_all_channels():
+    """Full C3 (256 channels x 2^20, K 4096, N_fft 16384, in place): every
+    output of every channel against an FP64 reference computed on the device
+    from the same FP32 inputs (linear correlation by a 2^21-point torch.fft in
+    complex128, the checker); each channel within the FP32 bar of 2e-6
+    relative L2."""
     ch, s, k, n = 256, 1 << 20, 4096, 16384
     gen = torch.Generator(device="cuda").manual_seed(2)
     x = torch.randn(ch * 2 * s, device="cuda", generator=gen)
@@ -110,16 +113,21 @@ def test_c3_full_size_sampled():
     orig = x.clone()
     unit.exec(x, x, s, channels=ch)
     unit.status()
-    xo = orig.view(ch, 2 * s)
-    y = x.view(ch, 2 * s)
-    gd = g.astype(np.complex128)
-    for c in rng.integers(0, ch, 8):
-        zc = O.unpack(xo[c].cpu().numpy(), s, 8)
-        yc = O.unpack(y[c].cpu().numpy(), s, 8)
-        idx = np.concatenate([rng.integers(0, s, 60), [0, 12287, 12288, s - 1]])
-        want = np.array([np.sum(zc[i:i + k] * np.conj(gd[: len(zc[i:i + k])])) for i in idx])
-        # the sampled outputs, as a vector, meet the FP32 bar
-        assert rel_l2(yc[idx], want) < TOL[np.float32]
+
+    def rows(t, m):    # pack-8 rows -> complex128 [rows, m]
+        v = t.reshape(-1, m // 8, 2, 8).double()
+        return torch.complex(v[:, :, 0, :].reshape(-1, m), v[:, :, 1, :].reshape(-1, m))
+
+    L = 1 << 21    # >= s + k - 1: the circular correlation is the linear one on [0, s)
+    gs = torch.conj(torch.fft.fft(torch.as_tensor(g.astype(np.complex128), device="cuda"), L))
+    worst = 0.0
+    for c0 in range(0, ch, 16):
+        want = torch.fft.ifft(torch.fft.fft(rows(orig[c0 * 2 * s:(c0 + 16) * 2 * s], s), L) * gs)[:, :s]
+        got = rows(x[c0 * 2 * s:(c0 + 16) * 2 * s], s)
+        err = torch.linalg.vector_norm(got - want, dim=-1) / torch.linalg.vector_norm(want, dim=-1)
+        worst = max(worst, float(err.max()))
+        assert float(err.max()) < TOL[np.float32], (c0, float(err.max()))
+    print(f"C3 full size: worst channel relative L2 {worst:.3g}")
 
 
 def test_vjp_against_oracle():
