@@ -58,11 +58,15 @@ struct xc2_cfg {
     static constexpr int TB1   = smem_align16(fs_full_tw_size<P1>() * 8);    // full stage tables
     static constexpr int TB2   = smem_align16(fs_full_tw_size<P2>() * 8);
     static constexpr int NB    = N / 16;      // W_N^e, e < N/16 (= TT1*N2 = TT2*N1)
-    static constexpr int SMEM  = WIN + XB + TB1 + TB2 + (NB + N2 + N1) * 8;
+    // in shared memory entry e sits at e + e/16: the threads of a warp read
+    // e = t*n2 for eight t, which would share banks whenever n2 is a multiple of 16
+    static constexpr int NBP   = NB + NB / 16;
+    static constexpr int SMEM  = WIN + XB + TB1 + TB2 + (NBP + N2 + N1) * 8;
     static_assert(P1::E == 16 && P2::E == 16, "16 points per thread");
     static_assert(TT1 <= 32 && TT2 <= 32 && TT2 >= 2, "sub-FFT groups inside one warp");
     static_assert(R1 >= 1 && R2 >= 1 && G1 * R1 == N2 && G2 * R2 == N1, "rounds");
     static_assert(TT1 * N2 == NB && TT2 * N1 == NB, "twiddle split");
+    static_assert(NBP % 2 == 0, "16-byte offset of the tables behind it");
     static_assert(WIN % 16 == 0 && XB % 16 == 0 && TB1 % 16 == 0 && TB2 % 16 == 0, "16-byte sections");
 };
 
@@ -93,7 +97,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
     cpx<float>*          tw1  = reinterpret_cast<cpx<float>*>(smem + F::WIN + F::XB);
     cpx<float>*          tw2  = tw1 + F::TB1 / 8;
     cpx<float>*          fwb  = tw2 + F::TB2 / 8;    // W_N^e
-    cpx<float>*          fwu1 = fwb + F::NB;         // W_N^(TT1*n2)
+    cpx<float>*          fwu1 = fwb + F::NBP;        // W_N^(TT1*n2)
     cpx<float>*          fwu2 = fwu1 + N2;           // W_N^(TT2*k1)
     __shared__ uint64_t  full;
     __shared__ long long s_item;
@@ -108,8 +112,10 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
     // constant tables into shared memory
     copy_table_to_smem<F::TB1>(tw1, A.stw1, tid, NT);
     copy_table_to_smem<F::TB2>(tw2, A.stw2, tid, NT);
-    for (int i = tid; i < (F::NB + N2 + N1) / 2; i += NT) {
-        reinterpret_cast<uint4*>(fwb)[i] = __ldg(reinterpret_cast<const uint4*>(A.tws) + i);
+    const cpx<float>* tws = reinterpret_cast<const cpx<float>*>(A.tws);
+    for (int e = tid; e < F::NB; e += NT) fwb[e + (e >> 4)] = ldg_cpx(tws + e);
+    for (int i = tid; i < (N2 + N1) / 2; i += NT) {
+        reinterpret_cast<uint4*>(fwu1)[i] = __ldg(reinterpret_cast<const uint4*>(tws + F::NB) + i);
     }
     if (tid == 0) {
         mbar_init(&full, 1);
@@ -217,7 +223,8 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 });
                 stage_compute_tab<P1, 0>(v, t, tw1);
                 run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
-                apply_fourstep_tw(v, fwb[t * n2], fwu1[n2], [&](auto ic, cpx<float> o) {
+                const int e = t * n2;
+                apply_fourstep_tw(v, fwb[e + (e >> 4)], fwu1[n2], [&](auto ic, cpx<float> o) {
                     constexpr int i              = decltype(ic)::value;
                     win[(t + i * TT1) * RS + n2] = o;
                 });
@@ -263,7 +270,8 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 stage_compute_tab<P2, 0>(v, t, tw2);
                 run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
                 // v[i] at n2 = t + i*TT2, times W_N^(k1*n2) = W_N^(k1*t) * W_N^(TT2*k1)^i
-                apply_fourstep_tw(v, fwb[k1 * t], fwu2[k1], [&](auto ic, cpx<float> o) {
+                const int e = k1 * t;
+                apply_fourstep_tw(v, fwb[e + (e >> 4)], fwu2[k1], [&](auto ic, cpx<float> o) {
                     constexpr int i           = decltype(ic)::value;
                     win[k1 * RS + t + i * TT2] = o;
                 });

@@ -39,6 +39,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// As mbar_try_wait, but a thread that finds the phase incomplete may sleep up
+// to `hint_ns` before the answer false; it is woken as soon as the phase
+// completes, so a long hint costs no latency and spares the issue slots that
+// repeated polls would take from the warps that have work.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ unsigned long long timer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
@@ -50,7 +66,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
                                                   unsigned long long limit_ns = 1000000000ull) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = timer_ns();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_hint(bar, parity, 200000u)) {    // sleeps at most 0.2 ms per poll
         if (timer_ns() - t0 > limit_ns) return false;
     }
     return true;
