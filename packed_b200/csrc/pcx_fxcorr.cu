@@ -134,6 +134,19 @@ __global__ void k_perm_spectrum(const cpx<float>* __restrict__ ks, cpx<float>* _
     kp[q]        = ks[k1 + (k2 << log_n1)];
 }
 
+}    // namespace
+
+// The spectrum K[k1 + N1*k2] stored at [k1*N2 + k2] (the (k1, k2) order of the
+// in-CTA four-step correlator's rows), on `st`.
+cudaError_t pcx_xc2_perm_spectrum(const void* ks, void* kp, int log_n1, int log_n2, cudaStream_t st) {
+    const int n = 1 << (log_n1 + log_n2);
+    k_perm_spectrum<<<(n + 255) / 256, 256, 0, st>>>(static_cast<const cpx<float>*>(ks), static_cast<cpx<float>*>(kp),
+                                                      log_n1, log_n2);
+    return cudaGetLastError();
+}
+
+namespace {
+
 template<int LOGN>
 int launch_xc2(const xc2_args& a, cudaStream_t st, int sms, bool attr_only) {
     using C   = xc2_cfg<LOGN>;
@@ -168,8 +181,7 @@ int init_xc2(pcx_fxcorr_s* h) {
     auto* s1     = kp + C::N;
     auto* s2     = s1 + e1;
     auto* tws    = s2 + e2;
-    k_perm_spectrum<<<(C::N + 255) / 256, 256>>>(static_cast<const cpx<float>*>(h->kspec), kp, C::LOGN1, C::LOGN2);
-    PCX_CUDA_TRY(cudaGetLastError());
+    PCX_CUDA_TRY(pcx_xc2_perm_spectrum(h->kspec, kp, C::LOGN1, C::LOGN2, 0));
     PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN1, s1, false, 0, &e1));
     PCX_CUDA_TRY(pcx_fourstep_tables(C::LOGN2, s2, false, 0, &e2));
     PCX_CUDA_TRY(pcx_gen_twiddles(tws, C::NB, LOGN, 1, false, 0));

@@ -182,6 +182,9 @@ int pcx_fft_run(pcx_plan_s* p, void* dst, const void* src, size_t src_len, int p
 
 // Table W_N^(i*mult), i < count, N = 2^log_n, generated in FP64 and rounded once.
 cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bool f64, cudaStream_t st);
+// A correlation spectrum K[k1 + N1*k2] (complex64) reordered to [k1*N2 + k2]
+// for the in-CTA four-step correlator (pcx_fxcorr.cu).
+cudaError_t pcx_xc2_perm_spectrum(const void* ks, void* kp, int log_n1, int log_n2, cudaStream_t st);
 
 // Hot-path launches (pcx_v2_*.cu); cudaErrorNotSupported when no variant exists.
 cudaError_t pcx_v2_single(bool f64, int log_n, const pcxg::v2_args& a, cudaStream_t st, bool attr_only);

@@ -16,7 +16,9 @@
 //   XR      up to M consecutive overlap-save blocks of one correlation with
 //           N_fft <= 8192: the producer bulk-copies the M packed windows into
 //           the stage; forward FFT, times conj(K), inverse, in the stage
-//   XC      the same with N_fft = 16384, whose exchange takes the whole ring
+//   XC      one overlap-save window of a correlation with N_fft = 16384 on
+//           the whole ring: the producer bulk-copies the window's rows, the
+//           compute warps run the in-CTA four-step of the C3 correlator
 // Each block has NT compute threads and, as the one-launch four-step kernel
 // does, a producer warp and a publisher warp: the producer claims the next
 // item, waits for its dependency (a scratch slot freed by an earlier
@@ -25,14 +27,15 @@
 // while one is computed; the publisher counts completions as soon as they
 // happen and never waits on another block.  Every size runs its own
 // compile-time geometry; the exchanges of the sub-transforms run in place in
-// the item's stage.  16384-point correlation items (last in the queue) read
-// their windows with plain loads and use the whole ring as workspace, so the
-// producer drains the ring around them.  Every wait is on an item earlier in the queue,
+// the item's stage.  16384-point correlation items (last in the queue) use the
+// whole ring, so the producer drains the ring around them.  Every wait is on
+// an item earlier in the queue,
 // claimed by a resident block whose publisher never waits on a later item:
 // the waits always end.  They are still bounded (about one second); on
 // timeout the block records an error and leaves.
 #include "pcx_fft_v2.cuh"
 #include "pcx_fourstep.cuh"
+#include "pcx_fxcorr2d.cuh"
 #include "pcx_fxcorr_kernels.cuh"
 #include "pcx_host.hpp"
 #include "pcx_v2_launch.cuh"
@@ -75,6 +78,14 @@ __shared__ uint64_t s_slotok[ST];     // column tile: its scratch slot may be wr
 __shared__ uint64_t s_written[ST];    // column tile: compute warps wrote the slot
 __shared__ int      s_item[ST];       // item index in the stage (-1: the queue is exhausted)
 
+// Rows of a correlation window (N1 rows of N2 samples) that lie wholly inside
+// the signal, given the samples left from the window's start.
+template<int N1, int N2>
+__host__ __device__ __forceinline__ int xc2_rows_inside(long long left) {
+    const long long r = left > 0 ? left / N2 : 0;
+    return (int)(r < N1 ? r : N1);
+}
+
 template<int L>
 __device__ __forceinline__ const cpx<float>* sub_tab() {
     static_assert(L >= SUB_LO && L <= SUB_HI, "table kept in shared memory");
@@ -108,6 +119,7 @@ struct tabs {
     const cpx<float>* tb[MAXLG];      // W_{16*N2}^i, i < N2
     cpx<float>*       scratch[MAXLG]; // the size's ring of scratch slots
     const cpx<float>* xft[MAXLG];     // correlator full stage tables
+    const cpx<float>* x2tw[MAXLG];    // in-CTA four-step correlator: W_N^e (e < N/16), W_N^(TT1*n2), W_N^(TT2*k1)
     const void*       sub;            // SUBTAB bytes: full tables of 2^6..2^9 points, in order
 };
 struct args {
@@ -314,63 +326,143 @@ __device__ __forceinline__ bool row_item(const stage_meta& mt, unsigned char* bu
     return true;
 }
 
-// Up to M overlap-save blocks of one correlation; buf is the whole ring.
+// One overlap-save window of a 2^LOGN-point correlation (N_fft = 16384) on the
+// whole ring: the in-CTA four-step of the C3 correlator, N = N1 x N2 with the
+// window in shared memory as N1 rows of N2 samples.  The producer copied the
+// rows that lie inside the signal (packed); the compute threads fill the
+// others, convert to interleaved complex in place, and run
+//   1. columns: N1-point FFTs, times W_N^(k1*n2);
+//   2. rows: N2-point FFTs, times the request's spectrum (stored in the same
+//      (k1, k2) order), inverse N2-point FFTs (as FFTs of the conjugate),
+//      times W_N^(k1*n2) again;
+//   3. columns: N1-point FFTs give conj(y), stored straight to the output.
+// Block barriers are named barrier 1 over the NT compute threads; each sub-FFT
+// belongs to TT threads of one warp and exchanges with warp barriers only.
 template<int LOGN>
-__device__ __forceinline__ void xc_items(const args& A, const stage_meta& mt, cpx<float>* buf, int tid) {
-    const item&   it  = mt.it;
-    constexpr int EPT = LOGN >= 14 ? 32 : 16;
-    using P           = splan<LOGN, EPT>;
-    static_assert(fs_full_tw_size<P>() == fs_full_tw_size<splan<LOGN>>(), "same stage radices");
-    constexpr int L   = P::L;
-    constexpr int E   = P::E;
-    constexpr int TT  = P::TT;
-    constexpr int M   = NT / TT;
-    using X           = xch_blocked<L, M>;
-    static_assert(X::size * 8 <= RING, "correlation workspace fits the ring");
-    const xc_req  q   = mt.xq;
-    const int     m   = tid / TT;
-    const int     t   = tid - m * TT;
-    // load M windows (blocks b .. b+count-1), zero outside the signal
-    for (int e = tid; e < M * L; e += NT) {
-        const int       mm  = e / L, l = e - mm * L;
-        const long long pos = (long long)(it.b + mm) * q.step + l;
-        cpx<float>      w   = {0.f, 0.f};
-        if (mm < it.c && pos < q.len) {
+__device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int tid) {
+    using F            = xc2_cfg<LOGN>;
+    using P1           = typename F::P1;
+    using P2           = typename F::P2;
+    constexpr int N1   = F::N1;
+    constexpr int N2   = F::N2;
+    constexpr int TT1  = F::TT1;
+    constexpr int TT2  = F::TT2;
+    constexpr int RS   = F::RS;
+    constexpr int E    = 16;
+    static_assert(F::NT == NT, "one compute thread per correlator thread");
+    static_assert(F::WIN + F::XB <= RING, "window and exchange rows fit the ring");
+    cpx<float>*       win  = reinterpret_cast<cpx<float>*>(rg_smem);
+    cpx<float>*       xch  = reinterpret_cast<cpx<float>*>(rg_smem + F::WIN);
+    const cpx<float>* tw1  = sub_tab<F::LOGN1>();
+    const cpx<float>* tw2  = sub_tab<F::LOGN2>();
+    const cpx<float>* fwb  = A.tb.x2tw[LOGN];
+    const cpx<float>* fwu1 = fwb + F::NB;
+    const cpx<float>* fwu2 = fwu1 + N2;
+    const xc_req&     q    = mt.xq;
+    const cpx<float>* kp   = q.kspec;    // K[k1 + N1*k2] / N at [k1*N2 + k2]
+    const long long   b0   = (long long)mt.it.b * q.step;
+    const int         rin  = xc2_rows_inside<N1, N2>(q.len - b0);
+    // rows past the copied ones: packed samples, zeros past the signal
+    for (int e = tid; e < (N1 - rin) * N2; e += NT) {
+        const int       r   = rin + e / N2, c = e % N2;
+        const long long pos = b0 + (long long)r * N2 + c;
+        float           re = 0.f, im = 0.f;
+        if (pos < q.len) {
             const long long o = ((pos >> 3) << 4) + (pos & 7);
-            w                 = {q.src[o], q.src[o + 8]};
+            re                = q.src[o];
+            im                = q.src[o + 8];
         }
-        buf[e] = w;
+        float* row                         = reinterpret_cast<float*>(win + r * RS);
+        row[((c >> 3) << 4) + (c & 7)]     = re;
+        row[((c >> 3) << 4) + (c & 7) + 8] = im;
     }
     xch_sync<NT>();
-    // full stage tables: the layout depends only on the stage radices, which
-    // are those of the 16-points-per-thread plan of the same size
-    const cpx<float>* tw = A.tb.xft[LOGN];
-    cpx<float>        v[E];
-    static_for<E>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        v[i]            = buf[m * L + t + i * TT];
-    });
-    stage_compute_tab<P, 0>(v, t, tw);
-    run_stages_full<P, X, false, NT>(v, buf, m, t, tw);
-    static_for<E>([&](auto ic) {
-        constexpr int    i = decltype(ic)::value;
-        const cpx<float> k = ldg_cpx(q.kspec + t + i * TT);
-        v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
-    });
-    stage_compute_tab<P, 0>(v, t, tw);
-    run_stages_full<P, X, false, NT>(v, buf, m, t, tw);
-    if (m < it.c) {
-        const long long b0 = (long long)(it.b + m) * q.step;
-        static_for<E>([&](auto ic) {
-            constexpr int   i  = decltype(ic)::value;
-            const int       mo = t + i * TT;
-            const long long e  = b0 + mo;
-            if (mo < q.step && e < q.len) {
-                const long long o = ((e >> 3) << 4) + (e & 7);
-                q.dst[o]          = v[i].re;
-                q.dst[o + 8]      = -v[i].im;
-            }
-        });
+    // packed -> interleaved, in place, one 64-byte pack per thread and step
+    // (consecutive threads take consecutive rows: distinct bank groups)
+    for (int e = tid; e < N1 * N2 / 8; e += NT) {
+        const int    r  = e % N1, p = e / N1;
+        float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
+        const float4 r0 = w[0], r1 = w[1], i0 = w[2], i1 = w[3];
+        w[0]            = make_float4(r0.x, i0.x, r0.y, i0.y);
+        w[1]            = make_float4(r0.z, i0.z, r0.w, i0.w);
+        w[2]            = make_float4(r1.x, i1.x, r1.y, i1.y);
+        w[3]            = make_float4(r1.z, i1.z, r1.w, i1.w);
+    }
+    xch_sync<NT>();
+    // ---- step 1: columns, forward, times W_N^(k1*n2)
+    {
+        const int g = tid / TT1, t = tid % TT1;
+        for (int rd = 0; rd < F::R1; ++rd) {
+            const int  n2 = rd * F::G1 + g;
+            cpx<float> v[E];
+            static_for<E>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                v[i]            = win[(t + i * TT1) * RS + n2];
+            });
+            stage_compute_tab<P1, 0>(v, t, tw1);
+            run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+            apply_fourstep_tw(v, ldg_cpx(fwb + t * n2), ldg_cpx(fwu1 + n2), [&](auto ic, cpx<float> o) {
+                constexpr int i              = decltype(ic)::value;
+                win[(t + i * TT1) * RS + n2] = o;
+            });
+        }
+    }
+    xch_sync<NT>();
+    // ---- step 2: rows; spectrum times the kernel's; inverse rows
+    {
+        constexpr int S  = TT2 / 2;    // the U groups of a half-warp take rows S apart:
+        constexpr int U  = 16 / TT2;   // their window rows fall in disjoint banks (RS = 2 mod 16)
+        const int     g  = tid / TT2, t = tid % TT2;
+        const int     bb = g / U, u = g % U;
+        const int     r0 = (bb / S) * 8 + (bb % S) + u * S;
+        for (int rd = 0; rd < F::R2; ++rd) {
+            const int  k1 = rd * F::G2 + r0;
+            cpx<float> v[E];
+            static_for<E>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                v[i]            = win[k1 * RS + t + i * TT2];
+            });
+            stage_compute_tab<P2, 0>(v, t, tw2);
+            run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+            // v[i] = X[k1 + N1*k2], k2 = t + i*TT2: conj(X * conj(K)) = conj(X) * K
+            static_for<E>([&](auto ic) {
+                constexpr int    i = decltype(ic)::value;
+                const cpx<float> k = ldg_cpx(kp + k1 * N2 + t + i * TT2);
+                v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
+            });
+            stage_compute_tab<P2, 0>(v, t, tw2);
+            run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
+            apply_fourstep_tw(v, ldg_cpx(fwb + k1 * t), ldg_cpx(fwu2 + k1), [&](auto ic, cpx<float> o) {
+                constexpr int i            = decltype(ic)::value;
+                win[k1 * RS + t + i * TT2] = o;
+            });
+        }
+    }
+    xch_sync<NT>();
+    // ---- step 3: columns again; outputs y = conj(.) for window positions
+    // n < step inside the signal (the window starts on a whole pack)
+    {
+        const int g  = tid / TT1, t = tid % TT1;
+        const int hi = (int)min((long long)q.step, q.len - b0);
+        float*    d  = q.dst + 2 * b0;
+        for (int rd = 0; rd < F::R1; ++rd) {
+            const int  n2 = rd * F::G1 + g;
+            cpx<float> v[E];
+            static_for<E>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                v[i]            = win[(t + i * TT1) * RS + n2];
+            });
+            stage_compute_tab<P1, 0>(v, t, tw1);
+            run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+            float* drow = d + 2 * t * N2 + ((n2 >> 3) << 4) + (n2 & 7);
+            static_for<E>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                if ((t + i * TT1) * N2 + n2 < hi) {
+                    __stcs(drow + 2 * i * TT1 * N2, v[i].re);
+                    __stcs(drow + 2 * i * TT1 * N2 + 8, -v[i].im);
+                }
+            });
+        }
     }
     xch_sync<NT>();    // the ring is read: it may be refilled
 }
@@ -494,6 +586,23 @@ __device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint
         const long long pos   = (long long)(it.b + m) * q.step;
         const long long valid = q.len - pos < G::L ? q.len - pos : G::L;
         bulk_g2s(reinterpret_cast<float*>(buf) + m * G::WS, q.src + 2 * pos, (uint32_t)((valid + 7) / 8) * 64, bar);
+    }
+}
+
+// The rows of a 16384-point correlation window that lie inside the signal,
+// one bulk copy of N2 packed samples per row, to the window rows at the
+// ring's start (the ring is drained first).
+template<int LOGN>
+__device__ void issue_xc2(const args& A, const item& it, uint64_t* bar, int lane) {
+    using F          = xc2_cfg<LOGN>;
+    const xc_req& q  = A.xreq[it.a];
+    const long long b0 = (long long)it.b * q.step;
+    const int     rin = xc2_rows_inside<F::N1, F::N2>(q.len - b0);
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rin * F::N2 * 8);
+    __syncwarp();
+    cpx<float>* win = reinterpret_cast<cpx<float>*>(rg_smem);
+    for (int r = lane; r < rin; r += 32) {
+        bulk_g2s(win + r * F::RS, q.src + 2 * (b0 + (long long)r * F::N2), F::N2 * 8, bar);
     }
 }
 
@@ -625,7 +734,7 @@ __device__ __noinline__ int run_xc(const args& A, int tid, cstate& cs) {
         A, cs, [](const item& it) { return it.kind == K_XC && it.lg == LOGN; },
         [&](const stage_meta& mt, int s, unsigned char*) -> bool {
             if (bar1_any<NT>(bad)) return false;
-            xc_items<LOGN>(A, mt, reinterpret_cast<cpx<float>*>(rg_smem), tid);
+            xc2_window<LOGN>(A, mt, tid);
             release_stage(s, tid);
             return true;
         });
@@ -759,7 +868,15 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                     if (!wait_empty(q)) fail = true;
                 }
                 if (fail) break;
-                if (lane == 0) mbar_arrive(&s_full[s]);
+                switch (it.lg) {
+#define PCX_RG_ISSUE_XC(LG) \
+    case LG: issue_xc2<LG>(A, it, &s_full[s], lane); break;
+                    PCX_RG_XC(PCX_RG_ISSUE_XC)
+#undef PCX_RG_ISSUE_XC
+                default:
+                    if (lane == 0) mbar_arrive(&s_full[s]);
+                    break;
+                }
                 drain_until = k;
                 issued      = k + 1;
                 continue;
@@ -1031,12 +1148,30 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             int rc = pcx_fft_run(p, ks, xc_g[j], xc_k[j], 1, 8, PCX_FORWARD, 0, 1, 2 * xc_nfft[j], 2 * xc_nfft[j], nullptr,
                                  0, 0, 1.0 / (double)xc_nfft[j]);
             if (rc) return fail(rc);
-            // on the ring (up to 8192 points) the windows come by bulk copies
-            // of whole packs
-            if (lg <= 13 && (!aligned16(xc_src[j]) || !aligned16(xc_dst[j]))) {
+            // the windows come by bulk copies of whole packs
+            if (!aligned16(xc_src[j]) || !aligned16(xc_dst[j])) {
                 return fail(pcx_fail(PCX_ERR_INVALID, "ragged correlation buffers must be 16-byte aligned"));
             }
-            if (!h->A.tb.xft[lg]) {
+            if (lg == 14) {
+                // the in-CTA four-step window: the spectrum in its (k1, k2) order
+                // and the four-step twiddles (shared by the 16384-point requests)
+                using C  = xc2_cfg<14>;
+                void* kp = nullptr;
+                if ((e = dev_alloc(xc_nfft[j] * 8, &kp)) != cudaSuccess) return cuda_fail(e);
+                if ((e = pcx_xc2_perm_spectrum(ks, kp, C::LOGN1, C::LOGN2, 0)) != cudaSuccess) return cuda_fail(e);
+                ks = kp;
+                if (!h->A.tb.x2tw[lg]) {
+                    void* tw = nullptr;
+                    if ((e = dev_alloc(((size_t)C::NB + C::N2 + C::N1) * 8, &tw)) != cudaSuccess) return cuda_fail(e);
+                    auto* t = static_cast<cpx<float>*>(tw);
+                    if ((e = pcx_gen_twiddles(t, C::NB, lg, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
+                    if ((e = pcx_gen_twiddles(t + C::NB, C::N2, lg, C::TT1, false, 0)) != cudaSuccess) return cuda_fail(e);
+                    if ((e = pcx_gen_twiddles(t + C::NB + C::N2, C::N1, lg, C::TT2, false, 0)) != cudaSuccess) {
+                        return cuda_fail(e);
+                    }
+                    h->A.tb.x2tw[lg] = t;
+                }
+            } else if (!h->A.tb.xft[lg]) {
                 int   fe = 0;
                 void* ft = nullptr;
                 if ((e = pcx_fourstep_tables(lg, nullptr, false, 0, &fe)) != cudaSuccess) return cuda_fail(e);
@@ -1132,21 +1267,10 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             }
         }
         push_fill(fill.size());
-        // 16384-point correlations last
-        {
-            std::vector<rg::item> xc_items;
-            for (size_t j = 0; j < n_xc; ++j) {
-                const int lg = xreq[j].lg;
-                if (lg <= 13) continue;
-                const int tt = (1 << lg) / (lg >= 14 ? 32 : 16);
-                const int M  = std::max(1, rg::NT / tt);
-                for (int b = 0; b < xreq[j].nblk; b += M) {
-                    xc_items.push_back({rg::K_XC, lg, (int)j, b, std::min(M, xreq[j].nblk - b)});
-                }
-            }
-            std::stable_sort(xc_items.begin(), xc_items.end(),
-                             [](const rg::item& x, const rg::item& y) { return x.lg > y.lg; });
-            items.insert(items.end(), xc_items.begin(), xc_items.end());
+        // 16384-point correlations last, one window per item
+        for (size_t j = 0; j < n_xc; ++j) {
+            if (xreq[j].lg <= 13) continue;
+            for (int b = 0; b < xreq[j].nblk; ++b) items.push_back({rg::K_XC, xreq[j].lg, (int)j, b, 1});
         }
         h->n_fft   = n_fft;
         h->n_items = items.size();
