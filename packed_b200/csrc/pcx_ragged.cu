@@ -57,14 +57,25 @@ constexpr int MAXLG = 32;
 // exchange buffer (one padding slot per 16 elements): 68 KB at every size.
 constexpr int STAGE = 69632;
 constexpr int RING  = ST * STAGE;
-// Behind the ring: the full stage tables of the 64..512-point sub-transforms
-// (the four-step passes of 2^13..2^18 and the correlations of 128..512
-// points), copied from global memory once per launch.
-constexpr int SUB_LO = 6, SUB_HI = 9;
+// Behind the ring: the full stage tables of the 64..1024-point sub-transforms
+// (the four-step passes of 2^13..2^18 and the correlations of 128..1024
+// points), copied from global memory once per launch.  The 1024-point table
+// also serves 512 points (the same stages, a radix-4 last stage read at every
+// other entry), so four tables are kept: 2^6, 2^7, 2^8 and 2^10.
+constexpr int SUB_LO = 6, SUB_HI = 10;
 template<int L>
-__host__ __device__ constexpr int sub_off() {    // entries before the table of 2^L points
+using sub_plan = splan<(L == 9 ? 10 : L)>;    // the plan whose table serves 2^L points
+template<int L>
+__host__ __device__ constexpr bool sub_kept() {
+    return L >= SUB_LO && L <= SUB_HI && L != 9;
+}
+template<int L>
+__host__ __device__ constexpr int sub_off() {    // entries before the kept table of 2^L points
     int o = 0;
-    if constexpr (L > SUB_LO) o = sub_off<L - 1>() + fs_full_tw_size<splan<L - 1>>();
+    if constexpr (L > SUB_LO) {
+        o = sub_off<L - 1>();
+        if constexpr (sub_kept<L - 1>()) o += fs_full_tw_size<splan<L - 1>>();
+    }
     return o;
 }
 constexpr int SUBTAB = sub_off<SUB_HI + 1>() * 8;
@@ -86,10 +97,12 @@ __host__ __device__ __forceinline__ int xc2_rows_inside(long long left) {
     return (int)(r < N1 ? r : N1);
 }
 
+// The table (of plan sub_plan<L>) that serves 2^L points.
 template<int L>
 __device__ __forceinline__ const cpx<float>* sub_tab() {
     static_assert(L >= SUB_LO && L <= SUB_HI, "table kept in shared memory");
-    return reinterpret_cast<const cpx<float>*>(rg_smem + RING) + sub_off<L>();
+    static_assert(full_tab_serves<splan<L>, sub_plan<L>>(), "the kept table serves this size");
+    return reinterpret_cast<const cpx<float>*>(rg_smem + RING) + sub_off<(L == 9 ? 10 : L)>();
 }
 
 enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3, K_XR = 4 };
@@ -120,7 +133,7 @@ struct tabs {
     cpx<float>*       scratch[MAXLG]; // the size's ring of scratch slots
     const cpx<float>* xft[MAXLG];     // correlator full stage tables
     const cpx<float>* x2tw[MAXLG];    // in-CTA four-step correlator: W_N^e (e < N/16), W_N^(TT1*n2), W_N^(TT2*k1)
-    const void*       sub;            // SUBTAB bytes: full tables of 2^6..2^9 points, in order
+    const void*       sub;            // SUBTAB bytes: full tables of 2^6, 2^7, 2^8, 2^10 points, in order
 };
 struct args {
     const item*        items;
@@ -154,8 +167,14 @@ __shared__ stage_meta s_meta[ST];
 __shared__ int        s_conj;     // inverse: conjugate in and out
 __shared__ float      s_scale;
 
-// Geometry of the four-step sizes: N = N1*N2 with N1 = 2^((lg+1)/2), tiles of
-// 8192 elements over NT threads of 16 points.
+// The four-step split N = 2^l1 * 2^(lg - l1) of a ragged transform of 2^lg
+// points (host and device use this one table).
+__host__ __device__ constexpr int split_l1(int lg) {
+    return lg == 13 ? 7 : lg == 14 ? 7 : lg == 15 ? 8 : lg == 16 ? 8 : lg == 17 ? 8 : lg == 18 ? 8 : (lg + 1) / 2;
+}
+
+// Geometry of the four-step sizes: N = N1*N2, tiles of 8192 elements over NT
+// threads of 16 points.
 template<int L1, int L2>
 struct fsg {
     static constexpr int N1 = 1 << L1, N2 = 1 << L2;
@@ -272,7 +291,8 @@ __device__ __forceinline__ bool col_item(const stage_meta& mt, unsigned char* bu
     });
     const auto* fst = sub_tab<L1>();
     stage_compute_tab<P1, 0>(v, t, fst);
-    if (run_stages_full<P1, typename F::X1, true, NT>(v, reinterpret_cast<cpx<float>*>(buf), c, t, fst, bad)) {
+    if (run_stages_full<P1, typename F::X1, true, NT, sub_plan<L1>>(v, reinterpret_cast<cpx<float>*>(buf), c, t, fst,
+                                                                   bad)) {
         return false;
     }
     // the stage is read: let the producer refill it while the tile is stored
@@ -310,7 +330,8 @@ __device__ __forceinline__ bool row_item(const stage_meta& mt, unsigned char* bu
     });
     const auto* fst = sub_tab<L2>();
     stage_compute_tab<P2, 0>(v, t, fst);
-    if (run_stages_full<P2, typename F::X2, true, NT>(v, reinterpret_cast<cpx<float>*>(buf), m, t, fst, bad)) {
+    if (run_stages_full<P2, typename F::X2, true, NT, sub_plan<L2>>(v, reinterpret_cast<cpx<float>*>(buf), m, t, fst,
+                                                                   bad)) {
         return false;
     }
     fence_proxy_async_smem();
@@ -497,13 +518,14 @@ __device__ __noinline__ bool xr_items(const args& A, const stage_meta& mt, unsig
         v[i] = t + i * TT < lim ? x : cpx<float>{0.f, 0.f};
     });
     constexpr bool TS  = LOGN <= SUB_HI;    // its table is in shared memory
+    using PT           = std::conditional_t<TS, sub_plan<(TS ? LOGN : SUB_LO)>, P>;
     const auto*    fst = [&]() {
         if constexpr (TS) return sub_tab<(TS ? LOGN : SUB_LO)>();
         else return A.tb.xft[LOGN];
     }();
     auto* xch = reinterpret_cast<cpx<float>*>(buf);
     stage_compute_tab<P, 0>(v, t, fst);
-    if (run_stages_full<P, typename G::X, TS, NT>(v, xch, m, t, fst, bad)) return false;
+    if (run_stages_full<P, typename G::X, TS, NT, PT>(v, xch, m, t, fst, bad)) return false;
     // v[i] = X[t + i*TT]: conj(X) * K, then the forward transform again
     static_for<E>([&](auto ic) {
         constexpr int    i = decltype(ic)::value;
@@ -511,7 +533,7 @@ __device__ __noinline__ bool xr_items(const args& A, const stage_meta& mt, unsig
         v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
     });
     stage_compute_tab<P, 0>(v, t, fst);
-    run_stages_full<P, typename G::X, TS, NT>(v, xch, m, t, fst);
+    run_stages_full<P, typename G::X, TS, NT, PT>(v, xch, m, t, fst);
     fence_proxy_async_smem();    // the stage is read: it may be refilled
     __syncwarp();
     if (tid % 32 == 0) mbar_arrive(empty_bar);
@@ -606,7 +628,10 @@ __device__ void issue_xc2(const args& A, const item& it, uint64_t* bar, int lane
     }
 }
 
-#define PCX_RG_FOURSTEP(X) X(13, 7, 6) X(14, 7, 7) X(15, 8, 7) X(16, 8, 8) X(17, 9, 8) X(18, 9, 9)
+#define PCX_RG_FOURSTEP(X) X(13, 7, 6) X(14, 7, 7) X(15, 8, 7) X(16, 8, 8) X(17, 8, 9) X(18, 8, 10)
+#define PCX_RG_CHECK_SPLIT(LG, A1, A2) static_assert(split_l1(LG) == A1 && LG == A1 + A2, "one split table");
+PCX_RG_FOURSTEP(PCX_RG_CHECK_SPLIT)
+#undef PCX_RG_CHECK_SPLIT
 #define PCX_RG_SINGLE(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 #define PCX_RG_XC(X) X(14)
 #define PCX_RG_XR(X) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
@@ -784,14 +809,13 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
             } else if (it.kind == K_ROW) {
                 // the rows are in shared memory: drop their L2 lines unwritten
                 const int   lg   = it.lg;
-                const int   l2   = lg / 2, l1 = lg - l2;
+                const int   l2   = lg - split_l1(lg);
                 const int   cr   = NT / ((1 << l2) / 16);
                 const long long n = 1LL << lg;
                 const char* g    = reinterpret_cast<const char*>(A.tb.scratch[lg] + (long long)A.req[it.a].slot * n +
                                                                   (long long)it.b * cr * (1LL << l2));
                 const int   lines = cr * (1 << l2) * 8 / 128;
                 for (int q = lane; q < lines; q += 32) l2_discard(g + (size_t)q * 128);
-                (void)l1;
                 __syncwarp();
                 if (lane == 0) red_release_add(A.row_done + it.a, 1);
             }
@@ -1095,9 +1119,9 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 if (!p) return fail(PCX_ERR_CUDA);
                 h->A.tb.stw[lg] = static_cast<const cpx<float>*>(p->stwL);
             } else {
-                // the four-step split (N1 = 2^((lg+1)/2)) and its twiddles; the
+                // the four-step split (split_l1) and its twiddles; the
                 // sub-transforms' stage tables are the shared ones (SUBTAB)
-                const int l1 = (lg + 1) / 2, l2 = lg / 2;
+                const int l1 = rg::split_l1(lg), l2 = lg - l1;
                 const int n1 = 1 << l1, n2 = 1 << l2;
                 void*     m  = nullptr;
                 if ((e = dev_alloc(((size_t)n1 + 2 * (size_t)n2) * 8, &m)) != cudaSuccess) return cuda_fail(e);
@@ -1119,17 +1143,16 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 h->A.scale = 1.0f / float(size_t(1) << lg);
             }
         }
-        // full stage tables of 2^6..2^9 points, copied to shared memory by every block
+        // full stage tables of 2^6, 2^7, 2^8 and 2^10 points, copied to shared memory by every block
         {
             void* sub = nullptr;
             if ((e = dev_alloc(rg::SUBTAB, &sub)) != cudaSuccess) return cuda_fail(e);
             auto*     sb   = static_cast<cpx<float>*>(sub);
-            const int offs[4] = {rg::sub_off<6>(), rg::sub_off<7>(), rg::sub_off<8>(), rg::sub_off<9>()};
-            for (int l = rg::SUB_LO; l <= rg::SUB_HI; ++l) {
+            const int kept[4][2] = {{6, rg::sub_off<6>()}, {7, rg::sub_off<7>()}, {8, rg::sub_off<8>()},
+                                    {10, rg::sub_off<10>()}};
+            for (const auto& k: kept) {
                 int fe = 0;
-                if ((e = pcx_fourstep_tables(l, sb + offs[l - rg::SUB_LO], false, 0, &fe)) != cudaSuccess) {
-                    return cuda_fail(e);
-                }
+                if ((e = pcx_fourstep_tables(k[0], sb + k[1], false, 0, &fe)) != cudaSuccess) return cuda_fail(e);
             }
             h->A.tb.sub = sub;
         }
@@ -1227,7 +1250,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
         };
         for (auto& [lg, idx]: by_lg) {
             if (lg <= 12) continue;
-            const int       l1 = (lg + 1) / 2, l2 = lg / 2;
+            const int       l1 = rg::split_l1(lg), l2 = lg - l1;
             const int       tc = h->A.col_tiles[lg], tr = h->A.row_tiles[lg];
             const long long lag = std::max<long long>(1, (in_flight + tc + tr - 1) / (tc + tr));
             // this size's ring of scratch slots: 2*lag + 2 transforms
