@@ -170,7 +170,7 @@ __shared__ float      s_scale;
 // The four-step split N = 2^l1 * 2^(lg - l1) of a ragged transform of 2^lg
 // points (host and device use this one table).
 __host__ __device__ constexpr int split_l1(int lg) {
-    return lg == 13 ? 6 : lg == 14 ? 6 : lg == 15 ? 7 : lg == 16 ? 7 : lg == 17 ? 8 : lg == 18 ? 8 : (lg + 1) / 2;
+    return lg == 13 ? 6 : lg == 14 ? 6 : lg == 15 ? 6 : lg == 16 ? 6 : lg == 17 ? 7 : lg == 18 ? 8 : (lg + 1) / 2;
 }
 
 // Geometry of the four-step sizes: N = N1*N2, tiles of 8192 elements over NT
@@ -628,7 +628,7 @@ __device__ void issue_xc2(const args& A, const item& it, uint64_t* bar, int lane
     }
 }
 
-#define PCX_RG_FOURSTEP(X) X(13, 6, 7) X(14, 6, 8) X(15, 7, 8) X(16, 7, 9) X(17, 8, 9) X(18, 8, 10)
+#define PCX_RG_FOURSTEP(X) X(13, 6, 7) X(14, 6, 8) X(15, 6, 9) X(16, 6, 10) X(17, 7, 10) X(18, 8, 10)
 #define PCX_RG_CHECK_SPLIT(LG, A1, A2) static_assert(split_l1(LG) == A1 && LG == A1 + A2, "one split table");
 PCX_RG_FOURSTEP(PCX_RG_CHECK_SPLIT)
 #undef PCX_RG_CHECK_SPLIT
