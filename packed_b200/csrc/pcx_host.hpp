@@ -68,10 +68,10 @@ struct fs_variant {
 // uneven split with the longer sub-transform in the row pass is fastest).
 constexpr fs_variant kFsVariantsF32[] = {
     {7, 6, 2, 3},  {6, 7, 2, 3},                                      // 2^13 (beside the one-pass form)
-    {7, 7, 2, 3},  {7, 7, 1, 3},                                      // 2^14
-    {7, 8, 2, 3},  {8, 7, 2, 3},                                      // 2^15
-    {8, 8, 2, 3},  {8, 8, 1, 3},  {7, 9, 2, 3},  {9, 7, 2, 3},        // 2^16
-    {8, 9, 2, 3},  {9, 8, 2, 3},  {10, 7, 1, 3}, {9, 8, 1, 3},        // 2^17
+    {7, 7, 2, 3},  {7, 7, 1, 3},  {6, 8, 2, 3},                       // 2^14
+    {7, 8, 2, 3},  {8, 7, 2, 3},  {6, 9, 2, 3},                       // 2^15
+    {8, 8, 2, 3},  {8, 8, 1, 3},  {7, 9, 2, 3},  {9, 7, 2, 3},  {6, 10, 1, 3},    // 2^16
+    {8, 9, 2, 3},  {9, 8, 2, 3},  {10, 7, 1, 3}, {9, 8, 1, 3},  {7, 10, 1, 3},    // 2^17
     {8, 10, 1, 3}, {10, 8, 1, 3}, {9, 9, 1, 3},  {9, 9, 2, 3},        // 2^18
     {9, 10, 1, 3}, {9, 10, 1, 2}, {10, 9, 1, 2}, {10, 9, 1, 3},       // 2^19
     {10, 10, 1, 3}, {10, 10, 1, 2},                                   // 2^20
