@@ -109,6 +109,14 @@ enum : int { K_SINGLE = 0, K_COL = 1, K_ROW = 2, K_XC = 3, K_XR = 4 };
 
 struct item {
     int kind, lg, a, b, c;    // SINGLE: a first transform, b count; COL/ROW: a transform, b tile; XC: a request, b first block, c count
+    // resolved on the host, so that claiming an item is one read:
+    int         tmap;         // COL: the transform's column-tile tensor map
+    int         prev;         // COL: the transform that used the slot before (-1 none)
+    int         prev_rows;    // COL: that transform's row tiles
+    const void* p0;           // COL: the scratch slot; ROW: destination; SINGLE: stage tables
+    const void* p1;           // COL: W_N^(i*N2); ROW: the scratch slot
+    const void* p2;           // COL: W_N^i
+    const void* p3;           // COL: W_{16*N2}^i
 };
 struct fft_req {
     const float* src;
@@ -152,16 +160,12 @@ struct args {
     tabs               tb;
 };
 
-// What the compute warps need of the item in each stage.  The producer fills
-// it from the queue and the requests while earlier items are computed, so
-// that no chain of dependent global loads opens an item.
+// What the compute warps need of the item in each stage, filled by the
+// producer while earlier items are computed, so that no chain of dependent
+// global loads opens an item.
 struct stage_meta {
-    item        it;
-    const void* p0;    // COL: the transform's scratch slot; ROW, SINGLE: destination / stage tables
-    const void* p1;    // COL: W_N^(i*N2)
-    const void* p2;    // COL: W_N^i
-    const void* p3;    // COL: W_{16*N2}^i
-    xc_req      xq;    // XR, XC: the correlation request
+    item   it;
+    xc_req xq;    // XR, XC: the correlation request
 };
 __shared__ stage_meta s_meta[ST];
 __shared__ int        s_conj;     // inverse: conjugate in and out
@@ -231,7 +235,7 @@ __device__ __forceinline__ bool single_items(const args& A, const stage_meta& mt
     const int     m  = tid / TT;
     const int     t  = tid - m * TT;
     const float*  in = reinterpret_cast<const float*>(buf);
-    const auto*   stw  = static_cast<const cpx<float>*>(mt.p0);
+    const auto*   stw  = static_cast<const cpx<float>*>(mt.it.p0);
     const bool    conj = s_conj != 0;
     cpx<float>    v[E];
     static_for<E>([&](auto ic) {
@@ -278,9 +282,9 @@ __device__ __forceinline__ bool col_item(const stage_meta& mt, unsigned char* bu
     const int     n2 = mt.it.b * C + c;
     // four-step twiddle inputs, used after the stages
     const uint32_t   e0 = (uint32_t)t * (uint32_t)n2;
-    const cpx<float> th = ldg_cpx(static_cast<const cpx<float>*>(mt.p1) + (e0 >> L2));
-    const cpx<float> tl = ldg_cpx(static_cast<const cpx<float>*>(mt.p2) + (e0 & (N2 - 1)));
-    const cpx<float> tu = ldg_cpx(static_cast<const cpx<float>*>(mt.p3) + n2);
+    const cpx<float> th = ldg_cpx(static_cast<const cpx<float>*>(mt.it.p1) + (e0 >> L2));
+    const cpx<float> tl = ldg_cpx(static_cast<const cpx<float>*>(mt.it.p2) + (e0 & (N2 - 1)));
+    const cpx<float> tu = ldg_cpx(static_cast<const cpx<float>*>(mt.it.p3) + n2);
     const float*     in   = reinterpret_cast<const float*>(buf);
     const bool       conj = s_conj != 0;
     cpx<float>       v[E];
@@ -301,7 +305,7 @@ __device__ __forceinline__ bool col_item(const stage_meta& mt, unsigned char* bu
     if (tid % 32 == 0) mbar_arrive(empty_bar);
     if (!slot_ready()) bad = true;
     if (!bad) {
-        cpx<float>* dst = const_cast<cpx<float>*>(static_cast<const cpx<float>*>(mt.p0)) + (long long)t * N2 + n2;
+        cpx<float>* dst = const_cast<cpx<float>*>(static_cast<const cpx<float>*>(mt.it.p0)) + (long long)t * N2 + n2;
         apply_fourstep_tw(v, cmul(th, tl), tu, [&](auto ic, cpx<float> o) {
             constexpr int i             = decltype(ic)::value;
             dst[(long long)i * TT * N2] = o;
@@ -337,7 +341,7 @@ __device__ __forceinline__ bool row_item(const stage_meta& mt, unsigned char* bu
     fence_proxy_async_smem();
     __syncwarp();
     if (tid % 32 == 0) mbar_arrive(empty_bar);
-    float*      dst = const_cast<float*>(static_cast<const float*>(mt.p0)) + pk<LPK>(t * N1 + k1);
+    float*      dst = const_cast<float*>(static_cast<const float*>(mt.it.p0)) + pk<LPK>(t * N1 + k1);
     const float sc = s_scale, sim = s_conj ? -sc : sc;
     static_for<E>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -561,7 +565,7 @@ __device__ void issue_col(const args& A, const item& it, unsigned char* buf, uin
     using F = fsg<L1, L2>;
     if (lane == 0) {
         mbar_arrive_expect_tx(bar, F::N1 * F::SEG * 4);
-        const CUtensorMap* map = A.tmaps + A.req[it.a].tmap;
+        const CUtensorMap* map = A.tmaps + it.tmap;
 #pragma unroll
         for (int y = 0; y < F::N1; y += F::BOXY) tma_load_3d_hint(buf + y * F::SEG * 4, map, 2 * it.b * F::C, y, 0, bar, pol);
     }
@@ -574,8 +578,7 @@ __device__ void issue_row(const args& A, const item& it, unsigned char* buf, uin
         mbar_arrive_expect_tx(bar, F::CR * F::N2 * 8);
     }
     __syncwarp();
-    const cpx<float>* g = A.tb.scratch[L1 + L2] + (long long)A.req[it.a].slot * (F::N1 * F::N2) +
-                          (long long)it.b * F::CR * F::N2;
+    const cpx<float>* g = static_cast<const cpx<float>*>(it.p1) + (long long)it.b * F::CR * F::N2;
     for (int q = lane; q < F::CR; q += 32) {
         bulk_g2s(reinterpret_cast<cpx<float>*>(buf) + q * F::RSI, g + (long long)q * F::N2, F::N2 * 8, bar);
     }
@@ -808,11 +811,9 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 }
             } else if (it.kind == K_ROW) {
                 // the rows are in shared memory: drop their L2 lines unwritten
-                const int   lg   = it.lg;
-                const int   l2   = lg - split_l1(lg);
+                const int   l2   = it.lg - split_l1(it.lg);
                 const int   cr   = NT / ((1 << l2) / 16);
-                const long long n = 1LL << lg;
-                const char* g    = reinterpret_cast<const char*>(A.tb.scratch[lg] + (long long)A.req[it.a].slot * n +
+                const char* g    = reinterpret_cast<const char*>(static_cast<const cpx<float>*>(it.p1) +
                                                                   (long long)it.b * cr * (1LL << l2));
                 const int   lines = cr * (1 << l2) * 8 / 128;
                 for (int q = lane; q < lines; q += 32) l2_discard(g + (size_t)q * 128);
@@ -870,18 +871,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 // published to the compute warps by this lane's arrival on full[s]
                 stage_meta& mt = s_meta[s];
                 mt.it          = it;
-                if (it.kind == K_COL) {
-                    mt.p0 = A.tb.scratch[it.lg] + (long long)A.req[it.a].slot * (1LL << it.lg);
-                    mt.p1 = A.tb.thi[it.lg];
-                    mt.p2 = A.tb.tlo[it.lg];
-                    mt.p3 = A.tb.tb[it.lg];
-                } else if (it.kind == K_ROW) {
-                    mt.p0 = A.req[it.a].dst;
-                } else if (it.kind == K_SINGLE) {
-                    mt.p0 = A.tb.stw[it.lg];
-                } else {
-                    mt.xq = A.xreq[it.a];
-                }
+                if (it.kind == K_XR || it.kind == K_XC) mt.xq = A.xreq[it.a];
                 s_item[s] = idx;
             }
             __syncwarp();
@@ -934,8 +924,7 @@ __global__ void __launch_bounds__(NT + 64, 1) k_ragged(const args* __restrict__ 
                 issued = k + 1;
                 // the slot: free once the transform that used it before has
                 // read all its rows
-                const fft_req& r = A.req[it.a];
-                if (r.prev >= 0 && !need(A.row_done + r.prev, r.prev_rows)) {
+                if (it.prev >= 0 && !need(A.row_done + it.prev, it.prev_rows)) {
                     fail = true;
                     break;
                 }
@@ -1227,7 +1216,10 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (lg > 12) continue;
             const int M = rg::NT / std::max(1, (1 << lg) / 16);
             for (size_t q = 0; q < idx.size(); q += M) {
-                fill.push_back({rg::K_SINGLE, lg, idx[q], (int)std::min<size_t>(M, idx.size() - q), 0});
+                rg::item it{rg::K_SINGLE, lg, idx[q], (int)std::min<size_t>(M, idx.size() - q), 0};
+                it.prev = -1;
+                it.p0   = h->A.tb.stw[lg];
+                fill.push_back(it);
             }
         }
         // correlations of up to 8192 points: M windows per item, on the ring
@@ -1236,7 +1228,9 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (lg > 13) continue;
             const int M = rg::NT / ((1 << lg) / 16);
             for (int b = 0; b < xreq[j].nblk; b += M) {
-                fill.push_back({rg::K_XR, lg, (int)j, b, std::min(M, xreq[j].nblk - b)});
+                rg::item it{rg::K_XR, lg, (int)j, b, std::min(M, xreq[j].nblk - b)};
+                it.prev = -1;
+                fill.push_back(it);
             }
         }
         std::vector<rg::item> items;
@@ -1278,12 +1272,22 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 r.tmap = (int)maps.size();
                 maps.push_back(map);
             }
+            auto slot_of = [&](int t) -> const void* { return h->A.tb.scratch[lg] + (size_t)req[t].slot * ((size_t)1 << lg); };
             for (size_t q = 0; q < idx.size() + (size_t)lag; ++q) {
                 if (q < idx.size()) {
-                    for (int tile = 0; tile < tc; ++tile) items.push_back({rg::K_COL, lg, idx[q], tile, 0});
+                    const rg::fft_req& r = req[idx[q]];
+                    for (int tile = 0; tile < tc; ++tile) {
+                        rg::item it{rg::K_COL, lg, idx[q], tile, 0, r.tmap, r.prev, r.prev_rows, slot_of(idx[q]),
+                                    h->A.tb.thi[lg], h->A.tb.tlo[lg], h->A.tb.tb[lg]};
+                        items.push_back(it);
+                    }
                 }
                 if (q >= (size_t)lag && q - lag < idx.size()) {
-                    for (int tile = 0; tile < tr; ++tile) items.push_back({rg::K_ROW, lg, idx[q - lag], tile, 0});
+                    const int t = idx[q - lag];
+                    for (int tile = 0; tile < tr; ++tile) {
+                        rg::item it{rg::K_ROW, lg, t, tile, 0, 0, -1, 0, req[t].dst, slot_of(t)};
+                        items.push_back(it);
+                    }
                 }
                 if (q < idx.size()) ++four_seen;
                 push_fill(nfour_total ? four_seen * fill.size() / nfour_total : fill.size());
@@ -1293,7 +1297,11 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
         // 16384-point correlations last, one window per item
         for (size_t j = 0; j < n_xc; ++j) {
             if (xreq[j].lg <= 13) continue;
-            for (int b = 0; b < xreq[j].nblk; ++b) items.push_back({rg::K_XC, xreq[j].lg, (int)j, b, 1});
+            for (int b = 0; b < xreq[j].nblk; ++b) {
+                rg::item it{rg::K_XC, xreq[j].lg, (int)j, b, 1};
+                it.prev = -1;
+                items.push_back(it);
+            }
         }
         h->n_fft   = n_fft;
         h->n_items = items.size();
