@@ -57,6 +57,7 @@ constexpr int MAXLG = 32;
 // exchange buffer (one padding slot per 16 elements): 68 KB at every size.
 constexpr int STAGE = 69632;
 constexpr int RING  = ST * STAGE;
+constexpr int XR2   = 13;    // correlations of 2^XR2 points: in-place in-CTA four-step windows
 // Behind the ring: the full stage tables of the 64..1024-point sub-transforms
 // (the four-step passes of 2^13..2^18 and the correlations of 128..1024
 // points), copied from global memory once per launch.  The 1024-point table
@@ -492,6 +493,152 @@ __device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int
     xch_sync<NT>();    // the ring is read: it may be refilled
 }
 
+// In-place exchange layouts inside a correlation window of rows of RS complex
+// (RS = 2 mod 16): a sub-FFT exchanges through its own column (or row) of the
+// window, logical slot l at position l ^ ((l / 16) & SW) -- a permutation
+// inside each run of 16 slots.  A group of SW + 1 threads writes slots 16t + j
+// and reads slots t + (SW + 1) i; the XOR keeps those on distinct banks (for
+// the columns, position p of column m sits at bank 4p + 2m mod 32).
+template<int RS, int SW>
+struct xch_in_column {    // m: the column
+    static_assert(SW < 16, "permutation inside runs of 16");
+    __device__ static __forceinline__ int idx(int m, int l) { return (l ^ ((l >> 4) & SW)) * RS + m; }
+};
+template<int RS, int SW>
+struct xch_in_row {       // m: the row
+    static_assert(SW < 16, "permutation inside runs of 16");
+    __device__ static __forceinline__ int idx(int m, int l) { return m * RS + (l ^ ((l >> 4) & SW)); }
+};
+
+// One overlap-save window of an 8192-point correlation in one ring stage: the
+// in-CTA four-step of the C3 correlator (128 x 64) with its sub-FFTs
+// exchanging in place in the window (no separate exchange rows), so the
+// window fits a stage and the ring keeps copying ahead.  The producer copied
+// the rows inside the signal (packed); the compute threads fill the others.
+template<int LOGN>
+__device__ __noinline__ bool xr2_window(const args& A, const stage_meta& mt, unsigned char* buf, bool bad, int tid,
+                                        uint64_t* empty_bar) {
+    using F            = xc2_cfg<LOGN>;
+    using P1           = typename F::P1;
+    using P2           = typename F::P2;
+    constexpr int N1   = F::N1;
+    constexpr int N2   = F::N2;
+    constexpr int TT1  = F::TT1;
+    constexpr int TT2  = F::TT2;
+    constexpr int RS   = F::RS;
+    constexpr int E    = 16;
+    using XC           = xch_in_column<RS, TT1 - 1>;
+    using XR           = xch_in_row<RS, TT2 - 1>;
+    static_assert(F::NT == NT && F::R1 == 1 && F::R2 == 1, "one column and one row per group");
+    static_assert(F::WIN <= STAGE, "the window fits a stage");
+    cpx<float>*       win  = reinterpret_cast<cpx<float>*>(buf);
+    const cpx<float>* tw1  = sub_tab<F::LOGN1>();
+    const cpx<float>* tw2  = sub_tab<F::LOGN2>();
+    const cpx<float>* fwb  = A.tb.x2tw[LOGN];
+    const cpx<float>* fwu1 = fwb + F::NB;
+    const cpx<float>* fwu2 = fwu1 + N2;
+    const xc_req&     q    = mt.xq;
+    const cpx<float>* kp   = q.kspec;    // K[k1 + N1*k2] / N at [k1*N2 + k2]
+    const long long   b0   = (long long)mt.it.b * q.step;
+    const int         rin  = xc2_rows_inside<N1, N2>(q.len - b0);
+    for (int e = tid; e < (N1 - rin) * N2; e += NT) {
+        const int       r   = rin + e / N2, c = e % N2;
+        const long long pos = b0 + (long long)r * N2 + c;
+        float           re = 0.f, im = 0.f;
+        if (pos < q.len) {
+            const long long o = ((pos >> 3) << 4) + (pos & 7);
+            re                = q.src[o];
+            im                = q.src[o + 8];
+        }
+        float* row                         = reinterpret_cast<float*>(win + r * RS);
+        row[((c >> 3) << 4) + (c & 7)]     = re;
+        row[((c >> 3) << 4) + (c & 7) + 8] = im;
+    }
+    // the first block barrier also votes on `bad`
+    if (bar1_any<NT>(bad)) return false;
+    for (int e = tid; e < N1 * N2 / 8; e += NT) {
+        const int    r  = e % N1, p = e / N1;
+        float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
+        const float4 r0 = w[0], r1 = w[1], i0 = w[2], i1 = w[3];
+        w[0]            = make_float4(r0.x, i0.x, r0.y, i0.y);
+        w[1]            = make_float4(r0.z, i0.z, r0.w, i0.w);
+        w[2]            = make_float4(r1.x, i1.x, r1.y, i1.y);
+        w[3]            = make_float4(r1.z, i1.z, r1.w, i1.w);
+    }
+    xch_sync<NT>();
+    // ---- step 1: columns, forward, times W_N^(k1*n2); group g owns column g
+    {
+        const int  n2 = tid / TT1, t = tid % TT1;
+        cpx<float> v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = win[(t + i * TT1) * RS + n2];
+        });
+        stage_compute_tab<P1, 0>(v, t, tw1);
+        run_stages_full<P1, XC, true, -1>(v, win, n2, t, tw1);
+        __syncwarp();    // the column's exchange reads are done
+        apply_fourstep_tw(v, ldg_cpx(fwb + t * n2), ldg_cpx(fwu1 + n2), [&](auto ic, cpx<float> o) {
+            constexpr int i              = decltype(ic)::value;
+            win[(t + i * TT1) * RS + n2] = o;
+        });
+    }
+    xch_sync<NT>();
+    // ---- step 2: rows; spectrum times the kernel's; inverse rows
+    {
+        constexpr int S  = TT2 / 2;    // the U groups of a half-warp take rows S apart:
+        constexpr int U  = 16 / TT2;   // their rows fall in disjoint banks (RS = 2 mod 16)
+        const int     g  = tid / TT2, t = tid % TT2;
+        const int     bb = g / U, u = g % U;
+        const int     k1 = (bb / S) * 8 + (bb % S) + u * S;
+        cpx<float>    v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = win[k1 * RS + t + i * TT2];
+        });
+        stage_compute_tab<P2, 0>(v, t, tw2);
+        run_stages_full<P2, XR, true, -1>(v, win, k1, t, tw2);
+        static_for<E>([&](auto ic) {
+            constexpr int    i = decltype(ic)::value;
+            const cpx<float> k = ldg_cpx(kp + k1 * N2 + t + i * TT2);
+            v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
+        });
+        stage_compute_tab<P2, 0>(v, t, tw2);
+        run_stages_full<P2, XR, true, -1>(v, win, k1, t, tw2);
+        __syncwarp();
+        apply_fourstep_tw(v, ldg_cpx(fwb + k1 * t), ldg_cpx(fwu2 + k1), [&](auto ic, cpx<float> o) {
+            constexpr int i            = decltype(ic)::value;
+            win[k1 * RS + t + i * TT2] = o;
+        });
+    }
+    xch_sync<NT>();
+    // ---- step 3: columns again; outputs y = conj(.) for window positions
+    // n < step inside the signal
+    {
+        const int  n2 = tid / TT1, t = tid % TT1;
+        const int  hi = (int)min((long long)q.step, q.len - b0);
+        cpx<float> v[E];
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            v[i]            = win[(t + i * TT1) * RS + n2];
+        });
+        stage_compute_tab<P1, 0>(v, t, tw1);
+        run_stages_full<P1, XC, true, -1>(v, win, n2, t, tw1);
+        // the window is read: the stage may be refilled while the outputs go out
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (tid % 32 == 0) mbar_arrive(empty_bar);
+        float* drow = q.dst + 2 * b0 + 2 * t * N2 + ((n2 >> 3) << 4) + (n2 & 7);
+        static_for<E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            if ((t + i * TT1) * N2 + n2 < hi) {
+                __stcs(drow + 2 * i * TT1 * N2, v[i].re);
+                __stcs(drow + 2 * i * TT1 * N2 + 8, -v[i].im);
+            }
+        });
+    }
+    return true;
+}
+
 // Up to M overlap-save blocks of one correlation (N_fft <= 8192) from their
 // packed windows in the stage.
 // Not inlined into its run loop: the correlation's two transforms need every
@@ -593,8 +740,28 @@ __device__ void issue_single(const args& A, const item& it, unsigned char* buf, 
     }
 }
 
+// The rows of an 8192-point correlation window inside the signal (one bulk
+// copy of N2 packed samples per row) into the stage.
+template<int LOGN>
+__device__ void issue_xr2(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    using F            = xc2_cfg<LOGN>;
+    const xc_req&   q  = A.xreq[it.a];
+    const long long b0 = (long long)it.b * q.step;
+    const int       rin = xc2_rows_inside<F::N1, F::N2>(q.len - b0);
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rin * F::N2 * 8);
+    __syncwarp();
+    cpx<float>* win = reinterpret_cast<cpx<float>*>(buf);
+    for (int r = lane; r < rin; r += 32) {
+        bulk_g2s(win + r * F::RS, q.src + 2 * (b0 + (long long)r * F::N2), F::N2 * 8, bar);
+    }
+}
+
 template<int LOGN>
 __device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    if constexpr (LOGN == XR2) {
+        issue_xr2<LOGN>(A, it, buf, bar, lane);
+        return;
+    }
     using G          = xrg<LOGN>;
     const xc_req& q  = A.xreq[it.a];
     // window m: samples [(b+m)*step, +L) of the packed signal, whole packs
@@ -749,7 +916,8 @@ __device__ __noinline__ int run_xr(const args& A, int tid, cstate& cs) {
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_XR && it.lg == LOGN; },
         [&](const stage_meta& mt, int s, unsigned char* buf) -> bool {
-            return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
+            if constexpr (LOGN == XR2) return xr2_window<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
+            else return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
         });
     cs.bad = bad;
     return r;
@@ -1164,15 +1332,16 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (!aligned16(xc_src[j]) || !aligned16(xc_dst[j])) {
                 return fail(pcx_fail(PCX_ERR_INVALID, "ragged correlation buffers must be 16-byte aligned"));
             }
-            if (lg == 14) {
-                // the in-CTA four-step window: the spectrum in its (k1, k2) order
-                // and the four-step twiddles (shared by the 16384-point requests)
-                using C  = xc2_cfg<14>;
-                void* kp = nullptr;
-                if ((e = dev_alloc(xc_nfft[j] * 8, &kp)) != cudaSuccess) return cuda_fail(e);
-                if ((e = pcx_xc2_perm_spectrum(ks, kp, C::LOGN1, C::LOGN2, 0)) != cudaSuccess) return cuda_fail(e);
-                ks = kp;
-                if (!h->A.tb.x2tw[lg]) {
+            if (lg == 14 || lg == rg::XR2) {
+                // the in-CTA four-step windows: the spectrum in their (k1, k2)
+                // order and the four-step twiddles (shared by the requests of a size)
+                auto x2 = [&](auto cfg) -> int {
+                    using C  = decltype(cfg);
+                    void* kp = nullptr;
+                    if ((e = dev_alloc(xc_nfft[j] * 8, &kp)) != cudaSuccess) return cuda_fail(e);
+                    if ((e = pcx_xc2_perm_spectrum(ks, kp, C::LOGN1, C::LOGN2, 0)) != cudaSuccess) return cuda_fail(e);
+                    ks = kp;
+                    if (h->A.tb.x2tw[lg]) return PCX_OK;
                     void* tw = nullptr;
                     if ((e = dev_alloc(((size_t)C::NB + C::N2 + C::N1) * 8, &tw)) != cudaSuccess) return cuda_fail(e);
                     auto* t = static_cast<cpx<float>*>(tw);
@@ -1182,7 +1351,9 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                         return cuda_fail(e);
                     }
                     h->A.tb.x2tw[lg] = t;
-                }
+                    return PCX_OK;
+                };
+                if (int rc2 = lg == 14 ? x2(xc2_cfg<14>{}) : x2(xc2_cfg<rg::XR2>{})) return rc2;
             } else if (!h->A.tb.xft[lg]) {
                 int   fe = 0;
                 void* ft = nullptr;
