@@ -340,7 +340,9 @@ int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int direction, in
  * FFT size xc_nfft[j] in 2^7..2^14), executed by ONE persistent launch that
  * takes work items from a device queue (four-step transforms as column and
  * row tiles with device-side dependencies), captured once as a CUDA graph.
- * Pointers are fixed at creation; each exec replays the graph.
+ * Pointers are fixed at creation; each exec replays the graph.  Every buffer
+ * (transforms and correlation signals, pack 8) must be 16-byte aligned: the
+ * data arrive by bulk copies (PCX_ERR_INVALID otherwise).
  */
 typedef struct pcx_ragged_s* pcx_ragged;
 int pcx_ragged_create(pcx_ragged* h, int dtype, size_t n_fft, const size_t* sizes, void* const* dst,

@@ -84,7 +84,7 @@ constexpr int SMEM   = RING + SUBTAB;
 static_assert(SUBTAB % 16 == 0 && SMEM <= 232448, "tables beside the ring");
 
 extern __shared__ __align__(128) unsigned char rg_smem[];
-__shared__ uint64_t s_full[ST];       // the item's copies landed (XC: the producer arrived)
+__shared__ uint64_t s_full[ST];       // the item's copies landed (or, at the end, the producer arrived)
 __shared__ uint64_t s_empty[ST];      // compute warps done with the stage, publisher past its item
 __shared__ uint64_t s_slotok[ST];     // column tile: its scratch slot may be written
 __shared__ uint64_t s_written[ST];    // column tile: compute warps wrote the slot
