@@ -129,3 +129,31 @@ def test_full_c5_scale_against_fp64():
         worst = max(worst, err)
         assert err < TOL[np.float32], (s, k, nf, err)
     print(f"full C5: worst relative L2 {worst:.3g}")
+
+
+@pytest.mark.parametrize("log_n", [10, 14, 16, 18])
+def test_ragged_inverse_one_size(log_n):
+    """An inverse ragged batch (normalised: every transform of one size, as
+    pcx_ragged_create requires) against numpy's inverse FFT."""
+    n = 1 << log_n
+    cnt = max(3, min(40, (1 << 21) // n))
+    rng = np.random.default_rng(700 + log_n)
+    z = normal_cx(rng, cnt, n)
+    src = [dev(O.pack(z[i], 8)) for i in range(cnt)]
+    dst = [torch.full_like(s, float("nan")) for s in src]
+    batch = ragged_batch([(dst[i], src[i], n) for i in range(cnt)], direction=1)
+    batch()
+    torch.cuda.synchronize()
+    batch.status()
+    for i in range(cnt):
+        assert rel_l2(O.unpack(dst[i].cpu().numpy(), n, 8), np.fft.ifft(z[i])) < TOL[np.float32], i
+
+
+def test_ragged_rejects_mixed_normalised_inverse_and_misaligned_buffers():
+    rng = np.random.default_rng(8)
+    a, b = dev(O.pack(normal_cx(rng, 256), 8)), dev(O.pack(normal_cx(rng, 512), 8))
+    with pytest.raises(NotImplementedError):
+        ragged_batch([(torch.empty_like(a), a, 256), (torch.empty_like(b), b, 512)], direction=1)
+    c = torch.zeros(2 * 1024 + 2, device="cuda")
+    with pytest.raises(ValueError):
+        ragged_batch([(c[2:], c[2:], 1024)])    # 8-byte offset: not 16-byte aligned
