@@ -112,6 +112,7 @@ struct item {
     int kind, lg, a, b, c;    // SINGLE: a first transform, b count; COL/ROW: a transform, b tile; XC: a request, b first block, c count
     // resolved on the host, so that claiming an item is one read:
     int         tmap;         // COL: the transform's column-tile tensor map
+    int         tz;           // COL: the transform's index in that map (0 for a map of its own)
     int         prev;         // COL: the transform that used the slot before (-1 none)
     int         prev_rows;    // COL: that transform's row tiles
     const void* p0;           // COL: the scratch slot; ROW: destination; SINGLE: stage tables
@@ -125,7 +126,8 @@ struct fft_req {
     int          slot;        // four-step scratch slot (in the size's own ring)
     int          prev;        // transform that used the slot before (-1 none)
     int          prev_rows;   // row tiles of that transform (its completion count)
-    int          tmap;        // its column-tile tensor map (four-step sizes)
+    int          tmap;        // its column-tile tensor map
+    int          tz;          // its index in that map (four-step sizes)
 };
 struct xc_req {
     const float*      src;
@@ -714,7 +716,9 @@ __device__ void issue_col(const args& A, const item& it, unsigned char* buf, uin
         mbar_arrive_expect_tx(bar, F::N1 * F::SEG * 4);
         const CUtensorMap* map = A.tmaps + it.tmap;
 #pragma unroll
-        for (int y = 0; y < F::N1; y += F::BOXY) tma_load_3d_hint(buf + y * F::SEG * 4, map, 2 * it.b * F::C, y, 0, bar, pol);
+        for (int y = 0; y < F::N1; y += F::BOXY) {
+            tma_load_3d_hint(buf + y * F::SEG * 4, map, 2 * it.b * F::C, y, it.tz, bar, pol);
+        }
     }
 }
 template<int L1, int L2>
@@ -1247,7 +1251,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (!aligned16(src[i]) || !aligned16(dst[i])) {
                 return fail(pcx_fail(PCX_ERR_INVALID, "ragged FFT buffers must be 16-byte aligned"));
             }
-            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1, 0, -1};
+            req[i] = {static_cast<const float*>(src[i]), static_cast<float*>(dst[i]), -1, -1, 0, -1, 0};
             by_lg[lg].push_back((int)i);
         }
         int sms = 148, dev = 0;
@@ -1423,24 +1427,47 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             void*        scr   = nullptr;
             if ((e = dev_alloc(nslot * ((size_t)8 << lg), &scr)) != cudaSuccess) return cuda_fail(e);
             h->A.tb.scratch[lg] = static_cast<cpx<float>*>(scr);
+            // column tiles read the transforms through tensor maps [n1][2*N2
+            // reals], box of 2*C reals x min(N1, 256) rows: one map over all of
+            // them when they lie at a uniform stride (one descriptor for the
+            // SMs' TMA units to cache), else a map per transform
+            const int        c      = rg::NT / std::max(1, (1 << l1) / 16);
+            const cuuint32_t box[3] = {(cuuint32_t)(2 * c), (cuuint32_t)std::min(1 << l1, 256), 1};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            long long        ustride = idx.size() > 1 ? (long long)(req[idx[1]].src - req[idx[0]].src) : 0;
+            bool             uniform = idx.size() > 1 && ustride >= (2LL << lg) && ustride % 4 == 0;
+            for (size_t q = 0; uniform && q < idx.size(); ++q) uniform = req[idx[q]].src == req[idx[0]].src + q * ustride;
+            int shared_map = -1;
+            if (uniform) {
+                CUtensorMap      map;
+                const cuuint64_t dims[3] = {(cuuint64_t)2 << l2, (cuuint64_t)1 << l1, (cuuint64_t)idx.size()};
+                const cuuint64_t strd[2] = {((cuuint64_t)2 << l2) * 4, (cuuint64_t)ustride * 4};
+                if ((e = encode_tensor_map(&map, false, 3, const_cast<float*>(req[idx[0]].src), dims, strd, box, estr)) !=
+                    cudaSuccess) {
+                    return cuda_fail(e);
+                }
+                shared_map = (int)maps.size();
+                maps.push_back(map);
+            }
             for (size_t q = 0; q < idx.size(); ++q) {
                 rg::fft_req& r = req[idx[q]];
                 r.slot         = (int)(q % nslot);
                 r.prev         = q >= nslot ? idx[q - nslot] : -1;
                 r.prev_rows    = tr;
-                // column tiles read the transform through its own tensor map:
-                // [n1][2*N2 reals], box of 2*C reals x min(N1, 256) rows
+                if (shared_map >= 0) {
+                    r.tmap = shared_map;
+                    r.tz   = (int)q;
+                    continue;
+                }
                 CUtensorMap      map;
-                const int        c      = rg::NT / std::max(1, (1 << l1) / 16);
                 const cuuint64_t dims[3] = {(cuuint64_t)2 << l2, (cuuint64_t)1 << l1, 1};
                 const cuuint64_t strd[2] = {((cuuint64_t)2 << l2) * 4, ((cuuint64_t)2 << lg) * 4};
-                const cuuint32_t box[3]  = {(cuuint32_t)(2 * c), (cuuint32_t)std::min(1 << l1, 256), 1};
-                const cuuint32_t estr[3] = {1, 1, 1};
                 if ((e = encode_tensor_map(&map, false, 3, const_cast<float*>(r.src), dims, strd, box, estr)) !=
                     cudaSuccess) {
                     return cuda_fail(e);
                 }
                 r.tmap = (int)maps.size();
+                r.tz   = 0;
                 maps.push_back(map);
             }
             auto slot_of = [&](int t) -> const void* { return h->A.tb.scratch[lg] + (size_t)req[t].slot * ((size_t)1 << lg); };
@@ -1448,7 +1475,8 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 if (q < idx.size()) {
                     const rg::fft_req& r = req[idx[q]];
                     for (int tile = 0; tile < tc; ++tile) {
-                        rg::item it{rg::K_COL, lg, idx[q], tile, 0, r.tmap, r.prev, r.prev_rows, slot_of(idx[q]),
+                        rg::item it{rg::K_COL,  lg,         idx[q],      tile,           0,
+                                    r.tmap,     r.tz,       r.prev,      r.prev_rows,    slot_of(idx[q]),
                                     h->A.tb.thi[lg], h->A.tb.tlo[lg], h->A.tb.tb[lg]};
                         items.push_back(it);
                     }
@@ -1456,7 +1484,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 if (q >= (size_t)lag && q - lag < idx.size()) {
                     const int t = idx[q - lag];
                     for (int tile = 0; tile < tr; ++tile) {
-                        rg::item it{rg::K_ROW, lg, t, tile, 0, 0, -1, 0, req[t].dst, slot_of(t)};
+                        rg::item it{rg::K_ROW, lg, t, tile, 0, 0, 0, -1, 0, req[t].dst, slot_of(t)};
                         items.push_back(it);
                     }
                 }
