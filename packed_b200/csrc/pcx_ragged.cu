@@ -367,7 +367,7 @@ __device__ __forceinline__ bool row_item(const stage_meta& mt, unsigned char* bu
 // Block barriers are named barrier 1 over the NT compute threads; each sub-FFT
 // belongs to TT threads of one warp and exchanges with warp barriers only.
 template<int LOGN>
-__device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int tid) {
+__device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int tid, uint64_t* empty_bar) {
     using F            = xc2_cfg<LOGN>;
     using P1           = typename F::P1;
     using P2           = typename F::P2;
@@ -480,6 +480,13 @@ __device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int
                 constexpr int i = decltype(ic)::value;
                 v[i]            = win[(t + i * TT1) * RS + n2];
             });
+            if (rd == F::R1 - 1) {
+                // the window is read: the next window's rows may land while
+                // this one finishes (its exchanges use the rows behind it)
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (tid % 32 == 0) mbar_arrive(empty_bar);
+            }
             stage_compute_tab<P1, 0>(v, t, tw1);
             run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
             float* drow = d + 2 * t * N2 + ((n2 >> 3) << 4) + (n2 & 7);
@@ -492,7 +499,6 @@ __device__ __noinline__ void xc2_window(const args& A, const stage_meta& mt, int
             });
         }
     }
-    xch_sync<NT>();    // the ring is read: it may be refilled
 }
 
 // In-place exchange layouts inside a correlation window of rows of RS complex
@@ -840,12 +846,6 @@ __device__ __forceinline__ int next_item(const args& A, int s, uint32_t par) {
     return s_item[s];
 }
 
-// Stage s is no longer read: it may be refilled.
-__device__ __forceinline__ void release_stage(int s, int tid) {
-    fence_proxy_async_smem();
-    __syncwarp();
-    if (tid % 32 == 0) mbar_arrive(&s_empty[s]);
-}
 
 // Runs the items from stage cs.s on while Match(item) holds, with
 // Work(stage_meta, s, stage buffer) returning false when the block leaves.
@@ -934,8 +934,7 @@ __device__ __noinline__ int run_xc(const args& A, int tid, cstate& cs) {
         A, cs, [](const item& it) { return it.kind == K_XC && it.lg == LOGN; },
         [&](const stage_meta& mt, int s, unsigned char*) -> bool {
             if (bar1_any<NT>(bad)) return false;
-            xc2_window<LOGN>(A, mt, tid);
-            release_stage(s, tid);
+            xc2_window<LOGN>(A, mt, tid, &s_empty[s]);    // releases the ring once the window is read
             return true;
         });
 }
