@@ -2,20 +2,23 @@
 // correlations, all in ONE persistent launch fed by a device work queue and
 // replayed from a CUDA graph.
 //
-// Work items (built once on the host, claimed in queue order from a device
-// counter):
+// Work items (built once on the host, each with its slot, destination, tensor
+// map and dependency resolved, claimed in queue order from a device counter):
 //   SINGLE  M whole transforms of one size N <= 4096 (M rows of 16 points per
 //           thread fill the block)
-//   COL     one column tile of a four-step transform (N = 2^13..2^18): TMA copy
-//           of the tile through the transform's own tensor map, column FFTs,
-//           four-step twiddle, written to the transform's scratch slot, then
-//           counted in col_done[t]
+//   COL     one column tile of a four-step transform (N = 2^13..2^18, split
+//           split_l1): TMA copy of the tile (one tensor map per size when the
+//           transforms lie at a uniform stride, else one per transform),
+//           column FFTs, four-step twiddle, written to the transform's
+//           scratch slot, then counted in col_done[t]
 //   ROW     one row tile: waits until col_done[t] reaches the column-tile
 //           count, bulk-copies the slot rows, row FFTs, natural-order output,
 //           counted in row_done[t] once its rows have landed
 //   XR      up to M consecutive overlap-save blocks of one correlation with
-//           N_fft <= 8192: the producer bulk-copies the M packed windows into
-//           the stage; forward FFT, times conj(K), inverse, in the stage
+//           N_fft <= 4096: the producer bulk-copies the M packed windows into
+//           the stage; forward FFT, times conj(K), inverse, in the stage.
+//           With N_fft = 8192 one window per item, as the in-CTA four-step
+//           with in-place exchanges inside the window (one stage)
 //   XC      one overlap-save window of a correlation with N_fft = 16384 on
 //           the whole ring: the producer bulk-copies the window's rows, the
 //           compute warps run the in-CTA four-step of the C3 correlator
@@ -25,14 +28,14 @@
 // transform's row tiles, or a transform's column tiles) and issues its
 // copies into a three-stage shared-memory ring, so two items are in flight
 // while one is computed; the publisher counts completions as soon as they
-// happen and never waits on another block.  Every size runs its own
-// compile-time geometry; the exchanges of the sub-transforms run in place in
-// the item's stage.  16384-point correlation items (last in the queue) use the
-// whole ring, so the producer drains the ring around them.  Every wait is on
-// an item earlier in the queue,
-// claimed by a resident block whose publisher never waits on a later item:
-// the waits always end.  They are still bounded (about one second); on
-// timeout the block records an error and leaves.
+// happen and never waits on another block.  The compute warps run one loop
+// per item kind and size (its own compile-time geometry and register
+// allocation); the exchanges of the sub-transforms run in place in the item's
+// stage.  16384-point correlation items (last in the queue) use the whole
+// ring, so the producer drains the ring around them.  Every wait is on an
+// item earlier in the queue, claimed by a resident block whose publisher
+// never waits on a later item: the waits always end.  They are still bounded
+// (about one second); on timeout the block records an error and leaves.
 #include "pcx_fft_v2.cuh"
 #include "pcx_fourstep.cuh"
 #include "pcx_fxcorr2d.cuh"
