@@ -4,6 +4,7 @@
 #include "pcxo/fft.hpp"
 #include "pcxo/fxcorr.hpp"
 #include "pcxo/mdstorage.hpp"
+#include "pcxo/ragged.hpp"
 
 #include <cmath>
 #include <complex>
@@ -113,6 +114,37 @@ int main() {
         expect(rel_err(so, y) < 2e-6, "fxcorr_unit(std::vector dest, src)", rel_err(so, y));
         xc(sv);
         expect(rel_err(sv, y) < 2e-6, "fxcorr_unit(std::vector) in place", rel_err(sv, y));
+    }
+    {    // ragged batch: FFTs of three sizes and a correlation in one persistent launch
+        const std::size_t                sizes[] = {256, 2048, 8192};
+        std::vector<pcxo::vector<float>> src, dst;
+        std::vector<std::vector<cd>>     want;
+        for (std::size_t n: sizes) {
+            src.emplace_back(n);
+            dst.emplace_back(n);
+            std::vector<cd> x(n);
+            for (std::size_t i = 0; i < n; ++i) x[i] = cd(u(rng), u(rng)), src.back()[i] = x[i];
+            want.push_back(dft(x, -1));
+        }
+        const std::size_t   k = 300, s = 5000;
+        pcxo::vector<float> g(k), x(s), yv(s);
+        std::vector<cd>     gd(k), xd(s), y(s);
+        for (std::size_t i = 0; i < k; ++i) gd[i] = cd(u(rng), u(rng)), g[i] = gd[i];
+        for (std::size_t i = 0; i < s; ++i) xd[i] = cd(u(rng), u(rng)), x[i] = xd[i];
+        for (std::size_t i = 0; i < s; ++i) {
+            cd acc = 0;
+            for (std::size_t j = 0; j < k && i + j < s; ++j) acc += xd[i + j] * std::conj(gd[j]);
+            y[i] = acc;
+        }
+        pcxo::ragged_batch batch;
+        for (std::size_t q = 0; q < 3; ++q) batch.add_fft(dst[q], src[q]);
+        batch.add_xcorr(yv, x, g, pcxo::correlation_fft_size(k));
+        batch();
+        double worst = 0;
+        for (std::size_t q = 0; q < 3; ++q) worst = std::max(worst, rel_err(dst[q], want[q]));
+        expect(worst < 2e-6, "ragged_batch FFTs (256, 2048, 8192)", worst);
+        expect(rel_err(yv, y) < 2e-6, "ragged_batch correlation", rel_err(yv, y));
+        expect(batch.items() > 3, "ragged_batch work items");
     }
     {    // md::dynamic_storage (mdstorage.hpp): rows as vectors and batched row transforms
         enum class ax { x, y, z };
