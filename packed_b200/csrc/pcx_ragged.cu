@@ -15,10 +15,11 @@
 //           count, bulk-copies the slot rows, row FFTs, natural-order output,
 //           counted in row_done[t] once its rows have landed
 //   XR      up to M consecutive overlap-save blocks of one correlation with
-//           N_fft <= 4096: the producer bulk-copies the M packed windows into
+//           N_fft <= 2048: the producer bulk-copies the M packed windows into
 //           the stage; forward FFT, times conj(K), inverse, in the stage.
-//           With N_fft = 8192 one window per item, as the in-CTA four-step
-//           with in-place exchanges inside the window (one stage)
+//           With N_fft = 4096 (two windows per item) and 8192 (one) the
+//           windows' rows are copied and each window runs as the in-CTA
+//           four-step with in-place exchanges inside the window (one stage)
 //   XC      one overlap-save window of a correlation with N_fft = 16384 on
 //           the whole ring: the producer bulk-copies the window's rows, the
 //           compute warps run the in-CTA four-step of the C3 correlator
@@ -60,10 +61,11 @@ constexpr int MAXLG = 32;
 // exchange buffer (one padding slot per 16 elements): 68 KB at every size.
 constexpr int STAGE = 69632;
 constexpr int RING  = ST * STAGE;
-constexpr int XR2   = 13;    // correlations of 2^XR2 points: in-place in-CTA four-step windows
+constexpr int XRW   = 12;    // correlations of 2^XRW..2^13 points: in-place in-CTA four-step windows
 // Behind the ring: the full stage tables of the 64..1024-point sub-transforms
-// (the four-step passes of 2^13..2^18 and the correlations of 128..1024
-// points), copied from global memory once per launch.  The 1024-point table
+// (the four-step passes of 2^13..2^18, the correlations of 128..1024 points
+// and the sub-transforms of the 4096..16384-point correlation windows),
+// copied from global memory once per launch.  The 1024-point table
 // also serves 512 points (the same stages, a radix-4 last stage read at every
 // other entry), so four tables are kept: 2^6, 2^7, 2^8 and 2^10.
 constexpr int SUB_LO = 6, SUB_HI = 10;
@@ -224,6 +226,31 @@ struct xrg {
     static constexpr int WS = 2 * L + single3_pad<TT>();
     using X                 = xch_blocked<L, M>;
     static_assert(M * WS * 4 <= STAGE && X::size * 8 <= STAGE, "windows and exchange fit a stage");
+};
+
+// Correlation windows of N = N1 x N2 = 2^LOGN points (4096, 8192) as the
+// in-CTA four-step with in-place exchanges: W = 8192 / N windows per item,
+// stacked as W*N1 rows of RS complex in one stage.  RS keeps a half-warp's
+// column groups and row groups on distinct banks (2 mod 16 for 8-thread
+// columns, 4 mod 16 for 4-thread ones).
+template<int LOGN>
+struct xrw_cfg {
+    static constexpr int LOGN1 = (LOGN + 1) / 2;
+    static constexpr int LOGN2 = LOGN / 2;
+    static constexpr int N1    = 1 << LOGN1;
+    static constexpr int N2    = 1 << LOGN2;
+    static constexpr int N     = N1 * N2;
+    using P1                   = splan<LOGN1>;
+    using P2                   = splan<LOGN2>;
+    static constexpr int TT1   = P1::TT;
+    static constexpr int TT2   = P2::TT;
+    static constexpr int W     = 8192 / N;
+    static constexpr int RS    = N2 + (TT1 == 8 ? 2 : 4);
+    static constexpr int NB    = N / 16;    // W_N^e, e < N/16 (= TT1*N2 = TT2*N1)
+    static constexpr int WIN   = W * N1 * RS * 8;
+    static_assert(P1::E == 16 && P2::E == 16 && TT1 <= 8 && TT2 <= 4, "groups inside a warp");
+    static_assert(W * N2 * TT1 == NT && W * N1 * TT2 == NT, "one column and one row per group");
+    static_assert(TT1 * N2 == NB && TT2 * N1 == NB, "twiddle split");
 };
 
 // ---------------------------------------------------------------- compute
@@ -521,15 +548,17 @@ struct xch_in_row {       // m: the row
     __device__ static __forceinline__ int idx(int m, int l) { return m * RS + (l ^ ((l >> 4) & SW)); }
 };
 
-// One overlap-save window of an 8192-point correlation in one ring stage: the
-// in-CTA four-step of the C3 correlator (128 x 64) with its sub-FFTs
-// exchanging in place in the window (no separate exchange rows), so the
-// window fits a stage and the ring keeps copying ahead.  The producer copied
-// the rows inside the signal (packed); the compute threads fill the others.
+// Overlap-save windows of a 4096- or 8192-point correlation in one ring stage
+// (W = 8192 / N windows of the item, stacked): the in-CTA four-step of the C3
+// correlator with its sub-FFTs exchanging in place in the window (no separate
+// exchange rows), so the windows fit a stage and the ring keeps copying ahead.
+// The producer copied the rows inside the signal (packed); the compute threads
+// fill the others.  Windows past the request's last block (in its last item)
+// are zeros and store nothing.
 template<int LOGN>
-__device__ __noinline__ bool xr2_window(const args& A, const stage_meta& mt, unsigned char* buf, bool bad, int tid,
+__device__ __noinline__ bool xrw_window(const args& A, const stage_meta& mt, unsigned char* buf, bool bad, int tid,
                                         uint64_t* empty_bar) {
-    using F            = xc2_cfg<LOGN>;
+    using F            = xrw_cfg<LOGN>;
     using P1           = typename F::P1;
     using P2           = typename F::P2;
     constexpr int N1   = F::N1;
@@ -537,11 +566,11 @@ __device__ __noinline__ bool xr2_window(const args& A, const stage_meta& mt, uns
     constexpr int TT1  = F::TT1;
     constexpr int TT2  = F::TT2;
     constexpr int RS   = F::RS;
+    constexpr int W    = F::W;
     constexpr int E    = 16;
     using XC           = xch_in_column<RS, TT1 - 1>;
     using XR           = xch_in_row<RS, TT2 - 1>;
-    static_assert(F::NT == NT && F::R1 == 1 && F::R2 == 1, "one column and one row per group");
-    static_assert(F::WIN <= STAGE, "the window fits a stage");
+    static_assert(F::WIN <= STAGE, "the windows fit a stage");
     cpx<float>*       win  = reinterpret_cast<cpx<float>*>(buf);
     const cpx<float>* tw1  = sub_tab<F::LOGN1>();
     const cpx<float>* tw2  = sub_tab<F::LOGN2>();
@@ -550,91 +579,106 @@ __device__ __noinline__ bool xr2_window(const args& A, const stage_meta& mt, uns
     const cpx<float>* fwu2 = fwu1 + N2;
     const xc_req&     q    = mt.xq;
     const cpx<float>* kp   = q.kspec;    // K[k1 + N1*k2] / N at [k1*N2 + k2]
-    const long long   b0   = (long long)mt.it.b * q.step;
-    const int         rin  = xc2_rows_inside<N1, N2>(q.len - b0);
-    for (int e = tid; e < (N1 - rin) * N2; e += NT) {
-        const int       r   = rin + e / N2, c = e % N2;
-        const long long pos = b0 + (long long)r * N2 + c;
-        float           re = 0.f, im = 0.f;
-        if (pos < q.len) {
-            const long long o = ((pos >> 3) << 4) + (pos & 7);
-            re                = q.src[o];
-            im                = q.src[o + 8];
+    // rows of each window past the copied ones: packed samples, zeros past the signal
+    for (int w = 0; w < W; ++w) {
+        const long long b0  = (long long)(mt.it.b + w) * q.step;
+        const bool      in  = w < mt.it.c;
+        const int       rin = in ? xc2_rows_inside<N1, N2>(q.len - b0) : 0;
+        for (int e = tid; e < (N1 - rin) * N2; e += NT) {
+            const int       r   = rin + e / N2, c = e % N2;
+            const long long pos = b0 + (long long)r * N2 + c;
+            float           re = 0.f, im = 0.f;
+            if (in && pos < q.len) {
+                const long long o = ((pos >> 3) << 4) + (pos & 7);
+                re                = q.src[o];
+                im                = q.src[o + 8];
+            }
+            float* row                         = reinterpret_cast<float*>(win + (w * N1 + r) * RS);
+            row[((c >> 3) << 4) + (c & 7)]     = re;
+            row[((c >> 3) << 4) + (c & 7) + 8] = im;
         }
-        float* row                         = reinterpret_cast<float*>(win + r * RS);
-        row[((c >> 3) << 4) + (c & 7)]     = re;
-        row[((c >> 3) << 4) + (c & 7) + 8] = im;
     }
     // the first block barrier also votes on `bad`
     if (bar1_any<NT>(bad)) return false;
-    for (int e = tid; e < N1 * N2 / 8; e += NT) {
-        const int    r  = e % N1, p = e / N1;
-        float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
-        const float4 r0 = w[0], r1 = w[1], i0 = w[2], i1 = w[3];
-        w[0]            = make_float4(r0.x, i0.x, r0.y, i0.y);
-        w[1]            = make_float4(r0.z, i0.z, r0.w, i0.w);
-        w[2]            = make_float4(r1.x, i1.x, r1.y, i1.y);
-        w[3]            = make_float4(r1.z, i1.z, r1.w, i1.w);
+    for (int e = tid; e < W * N1 * N2 / 8; e += NT) {
+        const int    r  = e % (W * N1), p = e / (W * N1);
+        float4*      wp = reinterpret_cast<float4*>(win + r * RS + p * 8);
+        const float4 r0 = wp[0], r1 = wp[1], i0 = wp[2], i1 = wp[3];
+        wp[0]           = make_float4(r0.x, i0.x, r0.y, i0.y);
+        wp[1]           = make_float4(r0.z, i0.z, r0.w, i0.w);
+        wp[2]           = make_float4(r1.x, i1.x, r1.y, i1.y);
+        wp[3]           = make_float4(r1.z, i1.z, r1.w, i1.w);
     }
     xch_sync<NT>();
-    // ---- step 1: columns, forward, times W_N^(k1*n2); group g owns column g
+    // ---- step 1: columns, forward, times W_N^(k1*n2); group g owns column g % N2 of window g / N2
     {
-        const int  n2 = tid / TT1, t = tid % TT1;
-        cpx<float> v[E];
+        const int   g   = tid / TT1, t = tid % TT1;
+        const int   n2  = g % N2;
+        cpx<float>* col = win + (g / N2) * N1 * RS;
+        cpx<float>  v[E];
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            v[i]            = win[(t + i * TT1) * RS + n2];
+            v[i]            = col[(t + i * TT1) * RS + n2];
         });
         stage_compute_tab<P1, 0>(v, t, tw1);
-        run_stages_full<P1, XC, true, -1>(v, win, n2, t, tw1);
+        run_stages_full<P1, XC, true, -1>(v, col, n2, t, tw1);
         __syncwarp();    // the column's exchange reads are done
         apply_fourstep_tw(v, ldg_cpx(fwb + t * n2), ldg_cpx(fwu1 + n2), [&](auto ic, cpx<float> o) {
             constexpr int i              = decltype(ic)::value;
-            win[(t + i * TT1) * RS + n2] = o;
+            col[(t + i * TT1) * RS + n2] = o;
         });
     }
     xch_sync<NT>();
     // ---- step 2: rows; spectrum times the kernel's; inverse rows
     {
-        constexpr int S  = TT2 / 2;    // the U groups of a half-warp take rows S apart:
-        constexpr int U  = 16 / TT2;   // their rows fall in disjoint banks (RS = 2 mod 16)
-        const int     g  = tid / TT2, t = tid % TT2;
-        const int     bb = g / U, u = g % U;
-        const int     k1 = (bb / S) * 8 + (bb % S) + u * S;
-        cpx<float>    v[E];
+        const int g = tid / TT2, t = tid % TT2;
+        int       R = g;    // the row: a half-warp's row groups take consecutive rows (RS = 4 mod 16) ...
+        if constexpr (RS % 16 == 2) {
+            // ... or rows S apart, S = TT2 / 2 (RS = 2 mod 16), to stay on distinct banks
+            constexpr int S  = TT2 / 2;
+            constexpr int U  = 16 / TT2;
+            const int     bb = g / U, u = g % U;
+            R                = (bb / S) * 8 + (bb % S) + u * S;
+        }
+        const int   k1  = R % N1;
+        cpx<float>* row = win + (R / N1) * N1 * RS;
+        cpx<float>  v[E];
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            v[i]            = win[k1 * RS + t + i * TT2];
+            v[i]            = row[k1 * RS + t + i * TT2];
         });
         stage_compute_tab<P2, 0>(v, t, tw2);
-        run_stages_full<P2, XR, true, -1>(v, win, k1, t, tw2);
+        run_stages_full<P2, XR, true, -1>(v, row, k1, t, tw2);
         static_for<E>([&](auto ic) {
             constexpr int    i = decltype(ic)::value;
             const cpx<float> k = ldg_cpx(kp + k1 * N2 + t + i * TT2);
             v[i]               = cmul(cpx<float>{v[i].re, -v[i].im}, k);
         });
         stage_compute_tab<P2, 0>(v, t, tw2);
-        run_stages_full<P2, XR, true, -1>(v, win, k1, t, tw2);
+        run_stages_full<P2, XR, true, -1>(v, row, k1, t, tw2);
         __syncwarp();
         apply_fourstep_tw(v, ldg_cpx(fwb + k1 * t), ldg_cpx(fwu2 + k1), [&](auto ic, cpx<float> o) {
-            constexpr int i            = decltype(ic)::value;
-            win[k1 * RS + t + i * TT2] = o;
+            constexpr int i             = decltype(ic)::value;
+            row[k1 * RS + t + i * TT2] = o;
         });
     }
     xch_sync<NT>();
     // ---- step 3: columns again; outputs y = conj(.) for window positions
     // n < step inside the signal
     {
-        const int  n2 = tid / TT1, t = tid % TT1;
-        const int  hi = (int)min((long long)q.step, q.len - b0);
-        cpx<float> v[E];
+        const int       g   = tid / TT1, t = tid % TT1;
+        const int       w   = g / N2, n2 = g % N2;
+        cpx<float>*     col = win + w * N1 * RS;
+        const long long b0  = (long long)(mt.it.b + w) * q.step;
+        const int       hi  = w < mt.it.c ? (int)min((long long)q.step, q.len - b0) : 0;
+        cpx<float>      v[E];
         static_for<E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            v[i]            = win[(t + i * TT1) * RS + n2];
+            v[i]            = col[(t + i * TT1) * RS + n2];
         });
         stage_compute_tab<P1, 0>(v, t, tw1);
-        run_stages_full<P1, XC, true, -1>(v, win, n2, t, tw1);
-        // the window is read: the stage may be refilled while the outputs go out
+        run_stages_full<P1, XC, true, -1>(v, col, n2, t, tw1);
+        // the windows are read: the stage may be refilled while the outputs go out
         fence_proxy_async_smem();
         __syncwarp();
         if (tid % 32 == 0) mbar_arrive(empty_bar);
@@ -753,26 +797,34 @@ __device__ void issue_single(const args& A, const item& it, unsigned char* buf, 
     }
 }
 
-// The rows of an 8192-point correlation window inside the signal (one bulk
-// copy of N2 packed samples per row) into the stage.
+// The rows of a 4096- or 8192-point correlation item's windows that lie
+// inside the signal (one bulk copy of N2 packed samples per row) into the
+// stage, window w at rows [w*N1, (w+1)*N1).
 template<int LOGN>
-__device__ void issue_xr2(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
-    using F            = xc2_cfg<LOGN>;
-    const xc_req&   q  = A.xreq[it.a];
-    const long long b0 = (long long)it.b * q.step;
-    const int       rin = xc2_rows_inside<F::N1, F::N2>(q.len - b0);
-    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rin * F::N2 * 8);
+__device__ void issue_xrw(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
+    using F            = xrw_cfg<LOGN>;
+    const xc_req& q    = A.xreq[it.a];
+    int           rin[F::W];
+    uint32_t      rows = 0;
+    for (int w = 0; w < F::W; ++w) {
+        rin[w] = w < it.c ? xc2_rows_inside<F::N1, F::N2>(q.len - (long long)(it.b + w) * q.step) : 0;
+        rows += (uint32_t)rin[w];
+    }
+    if (lane == 0) mbar_arrive_expect_tx(bar, rows * F::N2 * 8);
     __syncwarp();
     cpx<float>* win = reinterpret_cast<cpx<float>*>(buf);
-    for (int r = lane; r < rin; r += 32) {
-        bulk_g2s(win + r * F::RS, q.src + 2 * (b0 + (long long)r * F::N2), F::N2 * 8, bar);
+    for (int w = 0; w < F::W; ++w) {
+        const long long b0 = (long long)(it.b + w) * q.step;
+        for (int r = lane; r < rin[w]; r += 32) {
+            bulk_g2s(win + (w * F::N1 + r) * F::RS, q.src + 2 * (b0 + (long long)r * F::N2), F::N2 * 8, bar);
+        }
     }
 }
 
 template<int LOGN>
 __device__ void issue_xr(const args& A, const item& it, unsigned char* buf, uint64_t* bar, int lane) {
-    if constexpr (LOGN == XR2) {
-        issue_xr2<LOGN>(A, it, buf, bar, lane);
+    if constexpr (LOGN >= XRW) {
+        issue_xrw<LOGN>(A, it, buf, bar, lane);
         return;
     }
     using G          = xrg<LOGN>;
@@ -923,7 +975,7 @@ __device__ __noinline__ int run_xr(const args& A, int tid, cstate& cs) {
     const int r   = run_loop(
         A, cs, [](const item& it) { return it.kind == K_XR && it.lg == LOGN; },
         [&](const stage_meta& mt, int s, unsigned char* buf) -> bool {
-            if constexpr (LOGN == XR2) return xr2_window<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
+            if constexpr (LOGN >= XRW) return xrw_window<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
             else return xr_items<LOGN>(A, mt, buf, bad, tid, &s_empty[s]);
         });
     cs.bad = bad;
@@ -1338,7 +1390,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             if (!aligned16(xc_src[j]) || !aligned16(xc_dst[j])) {
                 return fail(pcx_fail(PCX_ERR_INVALID, "ragged correlation buffers must be 16-byte aligned"));
             }
-            if (lg == 14 || lg == rg::XR2) {
+            if (lg == 14 || lg >= rg::XRW) {
                 // the in-CTA four-step windows: the spectrum in their (k1, k2)
                 // order and the four-step twiddles (shared by the requests of a size)
                 auto x2 = [&](auto cfg) -> int {
@@ -1359,7 +1411,7 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                     h->A.tb.x2tw[lg] = t;
                     return PCX_OK;
                 };
-                if (int rc2 = lg == 14 ? x2(xc2_cfg<14>{}) : x2(xc2_cfg<rg::XR2>{})) return rc2;
+                if (int rc2 = lg == 14 ? x2(xc2_cfg<14>{}) : lg == 13 ? x2(rg::xrw_cfg<13>{}) : x2(rg::xrw_cfg<12>{})) return rc2;
             } else if (!h->A.tb.xft[lg]) {
                 int   fe = 0;
                 void* ft = nullptr;

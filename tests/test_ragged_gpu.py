@@ -27,11 +27,15 @@ def test_ragged_batch_matches_oracle(seed):
         ffts.append((torch.full((2 * n,), float("nan"), device="cuda"), dev(O.pack(z, 8)), n))
     xcs, xin = [], []
     # correlations of 128..8192 points (on the ring) and one of 16384 points
-    # (its own path through the whole ring)
-    for q in range(7):
-        s = int(2 ** rng.uniform(12, 17)) if q < 6 else 50000
-        k = int(2 ** rng.uniform(6, 12)) if q < 6 else 5000
-        nf = max(128, 1 << int(np.ceil(np.log2(2 * k))))
+    # (its own path through the whole ring); the fixed ones give 4096-point
+    # items with a zero second window (3 blocks; 1 block) and an 8192-point one
+    fixed = [(50000, 5000, 16384), (7676, 1500, 4096), (1200, 1100, 4096), (20000, 3000, 8192)]
+    for q in range(6 + len(fixed)):
+        if q < 6:
+            s, k = int(2 ** rng.uniform(12, 17)), int(2 ** rng.uniform(6, 12))
+            nf = max(128, 1 << int(np.ceil(np.log2(2 * k))))
+        else:
+            s, k, nf = fixed[q - 6]
         x, g = normal_cx(rng, s), normal_cx(rng, k)
         xin.append((x, g, nf))
         xcs.append((torch.full((len(O.pack(x, 8)),), float("nan"), device="cuda"), dev(O.pack(x, 8)), s,
