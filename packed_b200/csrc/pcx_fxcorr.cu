@@ -250,8 +250,14 @@ int run_xc(pcx_fxcorr_s* h, void* dst, const void* src, size_t len, int pack, si
     a.step        = (int)step;
     a.nblk        = (int)nblk;
     a.total       = (long long)total;
-    a.in_shift    = convolve ? (int)(h->k - 1) : 0;
-    a.out_shift   = convolve ? (int)(h->k - 1) : 0;
+    // convolution (the adjoint): window b starts `shift` samples before
+    // output b*step, and output m of the block is circular index m + shift.
+    // Any shift >= K-1 with step + shift <= N gives the same outputs; at pack 8
+    // K-1 rounded up to whole packs is one (step = N - shift), and it keeps
+    // the windows on whole packs, as the four-step form below needs.
+    const size_t shift = pack == 8 ? (h->k - 1 + 7) / 8 * 8 : h->k - 1;
+    a.in_shift    = convolve ? (int)shift : 0;
+    a.out_shift   = convolve ? (int)shift : 0;
     a.conj_kernel = convolve ? 0 : 1;
     a.inplace     = inplace ? 1 : 0;
     a.hwait       = (int)((n + step - 1) / step) - 1;

@@ -274,3 +274,33 @@ def test_four_step_form_matches_general_kernel(n, s, k, ch, inplace, monkeypatch
         assert rel_l2(got[c], want) < TOL[np.float32]
         assert rel_l2(ref[c], want) < TOL[np.float32]
         assert rel_l2(got[c], ref[c]) < TOL[np.float32]
+
+
+@pytest.mark.parametrize("n,s,k,ch", [(16384, 40000, 4096, 2), (16384, 30001, 4097, 1), (16384, 9000, 12000, 3),
+                                      (8192, 30000, 4000, 2), (8192, 20000, 9, 1), (16384, 16384, 1, 1)])
+def test_adjoint_signal_gradient_four_step_form(n, s, k, ch, monkeypatch):
+    """The signal gradient (a convolution with the kernel) at 2^13 and 2^14
+    points runs in the in-CTA four-step form, its windows starting K-1
+    rounded up to whole packs before each block: it must agree with the
+    general kernel (PCX_XC_GENERAL at creation) and the direct-sum oracle."""
+    rng = np.random.default_rng(n + s + k + 1)
+    z = normal_cx(rng, ch, s).astype(np.complex64)
+    g = normal_cx(rng, k, sigma=1 / 64).astype(np.complex64)
+    gy = normal_cx(rng, ch, s).astype(np.complex64)
+    dz, dgy = dev(np.stack([O.pack(r, 8) for r in z])), dev(np.stack([O.pack(r, 8) for r in gy]))
+
+    def grad_x():
+        unit = fxcorr_unit(vector.from_complex(g), n)
+        gx, _ = unit.vjp(dgy, dz, s, channels=ch, want_kernel_grad=False)
+        torch.cuda.synchronize()
+        unit.status()
+        return [O.unpack(r, s, 8) for r in gx.cpu().numpy()]
+
+    got = grad_x()
+    monkeypatch.setenv("PCX_XC_GENERAL", "1")
+    ref = grad_x()
+    for c in range(ch):
+        want, _ = O.xcorr_vjp_direct(z[c], g, gy[c])
+        assert rel_l2(got[c], want) < TOL[np.float32], c
+        assert rel_l2(ref[c], want) < TOL[np.float32], c
+        assert rel_l2(got[c], ref[c]) < TOL[np.float32], c
