@@ -389,6 +389,9 @@ class C3Fxcorr:
         from packed_b200 import fxcorr_unit, vector
         g = torch.Generator(device=dev).manual_seed(2 + rank)
         self.x = torch.randn(self.channels * 2 * self.length, device=dev, generator=g)
+        # the adjoint's inputs: an output cotangent (the gradient of the
+        # weighted |y|^2 loss has this shape and distribution class)
+        self.gy = torch.randn(self.channels * 2 * self.length, device=dev, generator=g)
         rng = np.random.default_rng(3)
         taps = (rng.standard_normal(self.k) + 1j * rng.standard_normal(self.k)) / 64
         self.unit = fxcorr_unit(vector.from_complex(taps, device=dev), self.n_fft)
@@ -397,22 +400,32 @@ class C3Fxcorr:
         return self.channels * self.length * B_PT
 
     def parts(self):
-        return ["fxcorr"]
+        # the forward correlator (the line's value) and the two halves of its
+        # adjoint, timed beside it: the signal gradient (a convolution of gy
+        # with the kernel) and the kernel gradient (block spectra of x and gy)
+        return ["fxcorr", "vjp_x", "vjp_g"]
 
     def run_part(self, key):
-        self.unit.exec(self.x, self.x, self.length, channels=self.channels, check=False)
+        if key == "fxcorr":
+            self.unit.exec(self.x, self.x, self.length, channels=self.channels, check=False)
+        else:
+            self.unit.vjp(self.gy, self.x, self.length, channels=self.channels, want_signal_grad=key == "vjp_x",
+                          want_kernel_grad=key == "vjp_g")
 
     def check_status(self):
         self.unit.status()
 
     def part_work(self, key):
-        """Two N_fft-point transforms per overlap-save block (forward, inverse)."""
+        """Two N_fft-point transforms per overlap-save block (forward and
+        inverse; the kernel gradient: two forward, and one inverse in all)."""
         step = self.n_fft - self.k + 1
         blocks = self.channels * -(-self.length // step)
         lg = self.n_fft.bit_length() - 1
-        return 2 * blocks, 2 * blocks * 5 * self.n_fft * lg
+        tf = 2 * blocks + (1 if key == "vjp_g" else 0)
+        return tf, tf * 5 * self.n_fft * lg
 
     def part_bytes(self, key):
+        """16 B per signal sample: x in and y out; gy in and gx out; x and gy in."""
         return self.bytes_per_step()
 
     def e2e(self, torch, stream):
@@ -432,7 +445,9 @@ class C3Fxcorr:
                 "d2h_bytes_per_step": nb, "ms_per_step": ms}
 
     def launches(self):
-        return 1
+        # forward: one kernel; signal gradient: one; kernel gradient: the
+        # per-block spectra, their reduction, the inverse FFT and the repack
+        return 1 + 1 + 4
 
     def cpu_reference(self, budget_s=12.0):
         import ctypes
@@ -859,12 +874,16 @@ def main() -> None:
     pk = peaks()
     ms_step = res["ms"] / args.steps
     value = whole_job_gbs(wl.bytes_per_step(), world, ms_step)
-    if wl.name in ("c1", "c4", "c5"):
-        # the step runs several alternative forms of the same work: report the
-        # headline form's own time (c5: the ragged graph; c4: the fastest form)
+    if wl.name in ("c1", "c3", "c4", "c5"):
+        # the step runs several alternative forms of the same work, or work
+        # beside the headline: report the headline form's own time (c5: the
+        # ragged graph; c4: the fastest form; c3: the forward correlator)
         means = {p: statistics.mean(v) for p, v in res["per"].items()}
         if wl.name == "c5":
             ms_step = means["ragged_graph"]
+            nbytes  = wl.bytes_per_step()
+        elif wl.name == "c3":
+            ms_step = means["fxcorr"]
             nbytes  = wl.bytes_per_step()
         elif wl.name == "c1":
             ms_step = means["1024"]
@@ -879,9 +898,11 @@ def main() -> None:
     # the parts `value` counts (for c1/c4/c5 only the headline form of each
     # piece of work); throughput in the other units, transforms/s and
     # 5 N log2 N GFLOP/s, is whole job (all ranks) over the same device time
-    if wl.name in ("c1", "c4", "c5"):
+    if wl.name in ("c1", "c3", "c4", "c5"):
         if wl.name == "c5":
             counted = ["ragged_graph"]
+        elif wl.name == "c3":
+            counted = ["fxcorr"]
         elif wl.name == "c1":
             counted = ["1024"]
         else:

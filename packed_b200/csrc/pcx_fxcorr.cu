@@ -163,6 +163,19 @@ int launch_xc2(const xc2_args& a, cudaStream_t st, int sms, bool attr_only) {
     return PCX_OK;
 }
 
+template<int LOGN>
+int launch_xc2_kg(const xc2_kg_args& a, cudaStream_t st, int grid, bool attr_only) {
+    using C   = xc2_cfg<LOGN>;
+    auto kern = k_fxcorr2d_kgrad<LOGN>;
+    if (attr_only) {
+        PCX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        return PCX_OK;
+    }
+    kern<<<(unsigned)grid, C::NT, C::SMEM, st>>>(a);
+    PCX_CUDA_TRY(cudaGetLastError());
+    return PCX_OK;
+}
+
 // Tables of the in-CTA four-step form; false when it does not apply.
 template<int LOGN>
 int init_xc2(pcx_fxcorr_s* h) {
@@ -191,6 +204,7 @@ int init_xc2(pcx_fxcorr_s* h) {
     h->x2_stw1  = s1;
     h->x2_stw2  = s2;
     h->x2_tws   = tws;
+    if (int rc = launch_xc2_kg<LOGN>(xc2_kg_args{}, 0, 0, true)) return rc;
     return launch_xc2<LOGN>(xc2_args{}, 0, 0, true);
 }
 
@@ -421,12 +435,27 @@ extern "C" int pcx_fxcorr_vjp(pcx_fxcorr h, void* gx, void* gg, const void* gy, 
         a.nblk    = (int)nblk;
         a.total   = (long long)total;
         a.counter = h->ctl;
+        a.error   = reinterpret_cast<int*>(h->ctl + 1);
         a.acc     = base;
         a.xspec   = base + (size_t)grid * n * eb;
         void* sum = base + (size_t)grid * 2 * n * eb;
         void* inv = base + ((size_t)grid * 2 + 1) * n * eb;
-        int   rc  = h->dtype == PCX_F64 ? dispatch_kg<double>(h->log_n, a, h->tw, st, grid, false)
-                                        : dispatch_kg<float>(h->log_n, a, h->tw, st, grid, false);
+        // FP32 2^13 / 2^14 at pack 8 on 16-byte aligned rows: the in-CTA
+        // four-step form with the per-thread spectra in tensor memory
+        const bool x2 = h->x2d && pack == 8 && (channels == 1 || stride % 4 == 0) &&
+                        (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(gy)) % 16 == 0;
+        int rc;
+        if (x2) {
+            xc2_kg_args b{};
+            b.base = a;
+            b.stw1 = h->x2_stw1;
+            b.stw2 = h->x2_stw2;
+            b.tws  = h->x2_tws;
+            rc     = h->log_n == 14 ? launch_xc2_kg<14>(b, st, grid, false) : launch_xc2_kg<13>(b, st, grid, false);
+        } else {
+            rc = h->dtype == PCX_F64 ? dispatch_kg<double>(h->log_n, a, h->tw, st, grid, false)
+                                     : dispatch_kg<float>(h->log_n, a, h->tw, st, grid, false);
+        }
         if (rc) return rc;
         if (h->dtype == PCX_F64) {
             k_kgrad_reduce<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(

@@ -31,6 +31,7 @@
 
 #include "pcx_fft_v2.cuh"
 #include "pcx_fxcorr_kernels.cuh"
+#include "pcx_tmem.cuh"
 
 namespace pcxg {
 
@@ -348,6 +349,260 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel-gradient pass in the same form (the counterpart of k_fxcorr_kgrad for
+// FP32 N = 2^13 / 2^14, pack 8): per block, the gy block (zero-padded to N)
+// and then the x window land in the window rows, and steps 1-2 of the forward
+// four-step leave each thread the spectrum values of its rows k1 at columns
+// k2 = t + i*TT2 -- the same (k1, k2) every block.  So each thread keeps its
+// share of FFT(gy block) and of the running sum of FFT(x window) *
+// conj(FFT(gy block)) in tensor memory: per row round 32 columns of each (at
+// 16384 points the SM's 512 TMEM columns hold the spectrum twice; the four
+// warps that share a lane quarter take a quarter of the columns each).  At the end every CTA
+// writes its sum in natural order (k = k1 + N1*k2) to acc[blockIdx.x]; the
+// reduction over CTAs and the inverse FFT follow as for the general kernel.
+struct xc2_kg_args {
+    kg_args     base;
+    const void* stw1;    // as xc2_args
+    const void* stw2;
+    const void* tws;
+};
+
+template<int LOGN>
+__global__ void __launch_bounds__(512, 1) k_fxcorr2d_kgrad(xc2_kg_args A) {
+    using F            = xc2_cfg<LOGN>;
+    using P1           = typename F::P1;
+    using P2           = typename F::P2;
+    constexpr int N1   = F::N1;
+    constexpr int N2   = F::N2;
+    constexpr int NT   = F::NT;
+    constexpr int TT1  = F::TT1;
+    constexpr int TT2  = F::TT2;
+    constexpr int RS   = F::RS;
+    constexpr int E    = 16;
+    // per thread, 32 TMEM columns per row round for FFT(gy) and as many for the sum;
+    // the four warps that share a lane quarter take CPT columns each
+    constexpr uint32_t CPT   = 64 * F::R2;
+    constexpr uint32_t TCOLS = 4 * CPT;
+    static_assert(TCOLS == 256 || TCOLS == 512, "a power-of-two TMEM allocation");
+    const kg_args& a   = A.base;
+    extern __shared__ __align__(128) unsigned char smem[];
+    cpx<float>*          win  = reinterpret_cast<cpx<float>*>(smem);
+    cpx<float>*          xch  = reinterpret_cast<cpx<float>*>(smem + F::WIN);
+    cpx<float>*          tw1  = reinterpret_cast<cpx<float>*>(smem + F::WIN + F::XB);
+    cpx<float>*          tw2  = tw1 + F::TB1 / 8;
+    cpx<float>*          fwb  = tw2 + F::TB2 / 8;
+    cpx<float>*          fwu1 = fwb + F::NBP;
+    __shared__ uint64_t  full;
+    __shared__ long long s_item;
+    __shared__ int       s_rhi;
+    __shared__ uint32_t  s_tmem;
+    const int            tid  = threadIdx.x;
+    const int            warp = tid / 32;
+
+    copy_table_to_smem<F::TB1>(tw1, A.stw1, tid, NT);
+    copy_table_to_smem<F::TB2>(tw2, A.stw2, tid, NT);
+    const cpx<float>* tws = reinterpret_cast<const cpx<float>*>(A.tws);
+    for (int e = tid; e < F::NB; e += NT) fwb[e + (e >> 4)] = ldg_cpx(tws + e);
+    for (int i = tid; i < (N2 + N1) / 2; i += NT) {
+        reinterpret_cast<uint4*>(fwu1)[i] = __ldg(reinterpret_cast<const uint4*>(tws + F::NB) + i);
+    }
+    if (warp == 0) {
+        tmem_alloc(&s_tmem, TCOLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&full, 1);
+        fence_barrier_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = s_tmem;
+    // this thread's columns: FFT(gy) of round rd at 32*rd, the sum at SUM + 32*rd
+    constexpr uint32_t SUM  = 32 * F::R2;
+    const uint32_t     tcol = tbase + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(warp / 4) * CPT;
+    {
+        uint32_t z[32];
+        static_for<32>([&](auto jc) { z[decltype(jc)::value] = 0u; });
+        for (int rd = 0; rd < F::R2; ++rd) tmem_st32(tcol + SUM + 32 * rd, z);
+    }
+
+    // window `ph` of an item: 0 the gy block [b*step, b*step + step), 1 the x
+    // window [b*step, b*step + N); samples past the block or the signal are zero
+    auto item_pos = [&](long long item, long long& ch, long long& b0) {
+        ch = item / a.nblk;
+        b0 = (item - ch * a.nblk) * a.step;
+    };
+    auto valid_of = [&](int ph, long long b0) -> long long {
+        const long long v = a.len - b0;
+        return ph == 0 ? (v < a.step ? v : (long long)a.step) : v;
+    };
+    // warp 0: the bulk copies of the whole rows that lie inside the valid
+    // samples (thread 0 first claims the next item when ph == 0)
+    auto copy_window = [&](int ph) {
+        if (tid == 0) {
+            if (ph == 0) s_item = (long long)atomicAdd(a.counter, 1u);
+            const long long item = s_item;
+            if (item < a.total) {
+                long long ch, b0;
+                item_pos(item, ch, b0);
+                long long r_hi = valid_of(ph, b0) / N2;
+                r_hi           = r_hi < 0 ? 0 : (r_hi > N1 ? N1 : r_hi);
+                s_rhi          = (int)r_hi;
+                mbar_arrive_expect_tx(&full, (uint32_t)r_hi * (N2 * 8));
+            }
+        }
+        __syncwarp();
+        const long long item = s_item;
+        if (item >= a.total) return;
+        long long ch, b0;
+        item_pos(item, ch, b0);
+        const float* base = reinterpret_cast<const float*>(ph == 0 ? a.gy : a.x) + ch * a.stride + 2 * b0;
+        for (int r = tid; r < s_rhi; r += 32) bulk_g2s(win + r * RS, base + 2LL * r * N2, N2 * 8, &full);
+    };
+
+    __syncthreads();
+    if (tid < 32) copy_window(0);
+    uint32_t phase   = 0;
+    bool     aborted = false;
+    // step 2's row groups (as k_fxcorr2d): the U groups of a half-warp take
+    // rows S apart
+    constexpr int S  = TT2 / 2;
+    constexpr int U  = 16 / TT2;
+    const int     g2 = tid / TT2, t2 = tid % TT2;
+    const int     r0 = ((g2 / U) / S) * 8 + ((g2 / U) % S) + (g2 % U) * S;
+    for (;;) {
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= a.total) break;
+        long long ch, b0;
+        item_pos(item, ch, b0);
+        for (int ph = 0; ph < 2; ++ph) {
+            if (ph == 1) __syncthreads();    // warp 0 has set this window's copies going
+            const int       r_hi  = s_rhi;
+            const long long valid = valid_of(ph, b0);
+            const float*    sp    = reinterpret_cast<const float*>(ph == 0 ? a.gy : a.x) + ch * a.stride;
+            // rows past the copied ones: the samples of a partial row, zeros after
+            for (int q = r_hi * N2 + tid; q < N1 * N2; q += NT) {
+                const int r = q / N2, c = q - r * N2;
+                float     re = 0.f, im = 0.f;
+                if (q < valid) {
+                    const long long pos = b0 + q;
+                    const long long o   = ((pos >> 3) << 4) + (pos & 7);
+                    re                  = sp[o];
+                    im                  = sp[o + 8];
+                }
+                float* row                         = reinterpret_cast<float*>(win + r * RS);
+                row[((c >> 3) << 4) + (c & 7)]     = re;
+                row[((c >> 3) << 4) + (c & 7) + 8] = im;
+            }
+            const bool ok = mbar_wait_bounded(&full, phase);
+            if (__syncthreads_or(!ok)) {
+                // give up: record it and let the copies in flight land first
+                if (tid == 0) {
+                    atomicExch(a.error, 1);
+                    mbar_wait_bounded(&full, phase, 100000000ull);
+                }
+                aborted = true;
+                break;
+            }
+            phase ^= 1;
+            for (int q = tid; q < N1 * N2 / 8; q += NT) {
+                const int    r  = q % N1, p = q / N1;
+                float4*      w  = reinterpret_cast<float4*>(win + r * RS + p * 8);
+                const float4 r0v = w[0], r1v = w[1], i0v = w[2], i1v = w[3];
+                w[0]             = make_float4(r0v.x, i0v.x, r0v.y, i0v.y);
+                w[1]             = make_float4(r0v.z, i0v.z, r0v.w, i0v.w);
+                w[2]             = make_float4(r1v.x, i1v.x, r1v.y, i1v.y);
+                w[3]             = make_float4(r1v.z, i1v.z, r1v.w, i1v.w);
+            }
+            __syncthreads();
+            // ---------------- step 1: columns, forward, times W_N^(k1*n2)
+            {
+                const int g = tid / TT1, t = tid % TT1;
+                for (int rd = 0; rd < F::R1; ++rd) {
+                    const int  n2 = rd * F::G1 + g;
+                    cpx<float> v[E];
+                    static_for<E>([&](auto ic) {
+                        constexpr int i = decltype(ic)::value;
+                        v[i]            = win[(t + i * TT1) * RS + n2];
+                    });
+                    stage_compute_tab<P1, 0>(v, t, tw1);
+                    run_stages_full<P1, typename F::X1, true, -1>(v, xch, g, t, tw1);
+                    const int e = t * n2;
+                    apply_fourstep_tw(v, fwb[e + (e >> 4)], fwu1[n2], [&](auto ic, cpx<float> o) {
+                        constexpr int i              = decltype(ic)::value;
+                        win[(t + i * TT1) * RS + n2] = o;
+                    });
+                }
+            }
+            __syncthreads();
+            // ---------------- step 2: rows; the spectrum to tensor memory
+            for (int rd = 0; rd < F::R2; ++rd) {
+                const int  k1 = rd * F::G2 + r0;
+                cpx<float> v[E];
+                static_for<E>([&](auto ic) {
+                    constexpr int i = decltype(ic)::value;
+                    v[i]            = win[k1 * RS + t2 + i * TT2];
+                });
+                if (rd == F::R2 - 1) {
+                    // the window is read: start the next window's copies (the
+                    // x window of this block, or the next block's gy block)
+                    fence_proxy_async_smem();
+                    __syncthreads();
+                    if (tid < 32) copy_window(ph ^ 1);
+                }
+                stage_compute_tab<P2, 0>(v, t2, tw2);
+                run_stages_full<P2, typename F::X2, true, -1>(v, xch, g2, t2, tw2);
+                // v[i] = spectrum at k1 + N1*k2, k2 = t2 + i*TT2
+                if (ph == 0) {
+                    uint32_t r[32];
+                    static_for<E>([&](auto ic) {
+                        constexpr int i = decltype(ic)::value;
+                        r[2 * i]        = __float_as_uint(v[i].re);
+                        r[2 * i + 1]    = __float_as_uint(v[i].im);
+                    });
+                    tmem_st32(tcol + 32 * rd, r);
+                } else {
+                    // sum += X * conj(GY), eight values at a time
+                    static_for<2>([&](auto hc) {
+                        constexpr int h = decltype(hc)::value;
+                        uint32_t      gq[16], sq[16];
+                        tmem_ld16(tcol + 32 * rd + 16 * h, gq);
+                        tmem_ld16(tcol + SUM + 32 * rd + 16 * h, sq);
+                        static_for<8>([&](auto jc) {
+                            constexpr int    j = decltype(jc)::value;
+                            const cpx<float> p = cmulc(v[8 * h + j], cpx<float>{__uint_as_float(gq[2 * j]),
+                                                                                 __uint_as_float(gq[2 * j + 1])});
+                            sq[2 * j]          = __float_as_uint(__uint_as_float(sq[2 * j]) + p.re);
+                            sq[2 * j + 1]      = __float_as_uint(__uint_as_float(sq[2 * j + 1]) + p.im);
+                        });
+                        tmem_st16(tcol + SUM + 32 * rd + 16 * h, sq);
+                    });
+                }
+            }
+        }
+        if (aborted) break;
+    }
+    if (!aborted) {
+        // this CTA's sum, natural order
+        cpx<float>* acc = reinterpret_cast<cpx<float>*>(a.acc) + (long long)blockIdx.x * (N1 * N2);
+        for (int rd = 0; rd < F::R2; ++rd) {
+            const int k1 = rd * F::G2 + r0;
+            uint32_t  sq[32];
+            tmem_ld32(tcol + SUM + 32 * rd, sq);
+            static_for<E>([&](auto ic) {
+                constexpr int i                = decltype(ic)::value;
+                acc[k1 + N1 * (t2 + i * TT2)] = {__uint_as_float(sq[2 * i]), __uint_as_float(sq[2 * i + 1])};
+            });
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tbase, TCOLS);
 }
 
 }    // namespace pcxg

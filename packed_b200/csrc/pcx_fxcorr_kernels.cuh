@@ -200,6 +200,7 @@ struct kg_args {
     unsigned*   counter;
     void*       acc;          // [gridDim.x][N] complex
     void*       xspec;        // [gridDim.x][N] complex, per-CTA spectrum scratch
+    int*        error;        // set when a bounded wait gave up (forms with bulk copies)
 };
 
 template<class T, int LOGN, int EPT>

@@ -505,14 +505,17 @@ class fxcorr_unit:
         self.exec(dest.data, source.data, dest.size(), pack=dest.pack_size)
 
     def vjp(self, gy: torch.Tensor, x: torch.Tensor, length: int, *, channels: int = 1, pack: int | None = None,
-            want_kernel_grad: bool = True, stream=None) -> tuple[torch.Tensor, torch.Tensor | None]:
+            want_kernel_grad: bool = True, want_signal_grad: bool = True,
+            stream=None) -> tuple[torch.Tensor | None, torch.Tensor | None]:
+        """Cotangents of the signal and the kernel given the output's, `gy`
+        (pcx_fxcorr_vjp); either may be skipped (returned as None)."""
         p = pack or default_pack_size(self._dtype)
-        gx = torch.empty_like(gy)
+        gx = torch.empty_like(gy) if want_signal_grad else None
         gg = (torch.empty(real_size(self._k, self._pack_g), dtype=self._dtype, device=gy.device)
               if want_kernel_grad else None)
-        _lib.check(_lib.lib().pcx_fxcorr_vjp(self._h, _ptr(gx), _ptr(gg) if gg is not None else None, _ptr(gy),
-                                             _ptr(x), length, p, channels, real_size(length, p),
-                                             _stream_ptr(stream)))
+        _lib.check(_lib.lib().pcx_fxcorr_vjp(self._h, _ptr(gx) if gx is not None else None,
+                                             _ptr(gg) if gg is not None else None, _ptr(gy), _ptr(x), length, p,
+                                             channels, real_size(length, p), _stream_ptr(stream)))
         return gx, gg
 
 

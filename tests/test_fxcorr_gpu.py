@@ -277,30 +277,38 @@ def test_four_step_form_matches_general_kernel(n, s, k, ch, inplace, monkeypatch
 
 
 @pytest.mark.parametrize("n,s,k,ch", [(16384, 40000, 4096, 2), (16384, 30001, 4097, 1), (16384, 9000, 12000, 3),
-                                      (8192, 30000, 4000, 2), (8192, 20000, 9, 1), (16384, 16384, 1, 1)])
-def test_adjoint_signal_gradient_four_step_form(n, s, k, ch, monkeypatch):
-    """The signal gradient (a convolution with the kernel) at 2^13 and 2^14
-    points runs in the in-CTA four-step form, its windows starting K-1
-    rounded up to whole packs before each block: it must agree with the
-    general kernel (PCX_XC_GENERAL at creation) and the direct-sum oracle."""
+                                      (8192, 30000, 4000, 2), (8192, 20000, 9, 1), (16384, 16384, 1, 1),
+                                      (16384, 100, 300, 2)])
+def test_adjoint_four_step_form(n, s, k, ch, monkeypatch):
+    """Both halves of the adjoint at 2^13 and 2^14 points run in the in-CTA
+    four-step form: the signal gradient (a convolution with the kernel, its
+    windows starting K-1 rounded up to whole packs before each block) and the
+    kernel gradient (per-thread block spectra kept in tensor memory).  They
+    must agree with the general kernels (PCX_XC_GENERAL at creation) and the
+    direct-sum oracle."""
     rng = np.random.default_rng(n + s + k + 1)
     z = normal_cx(rng, ch, s).astype(np.complex64)
     g = normal_cx(rng, k, sigma=1 / 64).astype(np.complex64)
     gy = normal_cx(rng, ch, s).astype(np.complex64)
     dz, dgy = dev(np.stack([O.pack(r, 8) for r in z])), dev(np.stack([O.pack(r, 8) for r in gy]))
 
-    def grad_x():
+    def grads():
         unit = fxcorr_unit(vector.from_complex(g), n)
-        gx, _ = unit.vjp(dgy, dz, s, channels=ch, want_kernel_grad=False)
+        gx, gg = unit.vjp(dgy, dz, s, channels=ch)
         torch.cuda.synchronize()
         unit.status()
-        return [O.unpack(r, s, 8) for r in gx.cpu().numpy()]
+        return [O.unpack(r, s, 8) for r in gx.cpu().numpy()], O.unpack(gg.cpu().numpy(), k, 8)
 
-    got = grad_x()
+    got_x, got_g = grads()
     monkeypatch.setenv("PCX_XC_GENERAL", "1")
-    ref = grad_x()
+    ref_x, ref_g = grads()
+    want_g = np.zeros(k, complex)
     for c in range(ch):
-        want, _ = O.xcorr_vjp_direct(z[c], g, gy[c])
-        assert rel_l2(got[c], want) < TOL[np.float32], c
-        assert rel_l2(ref[c], want) < TOL[np.float32], c
-        assert rel_l2(got[c], ref[c]) < TOL[np.float32], c
+        want_x, wg = O.xcorr_vjp_direct(z[c], g, gy[c])
+        want_g += wg
+        assert rel_l2(got_x[c], want_x) < TOL[np.float32], c
+        assert rel_l2(ref_x[c], want_x) < TOL[np.float32], c
+        assert rel_l2(got_x[c], ref_x[c]) < TOL[np.float32], c
+    assert rel_l2(got_g, want_g) < TOL[np.float32]
+    assert rel_l2(ref_g, want_g) < TOL[np.float32]
+    assert rel_l2(got_g, ref_g) < TOL[np.float32]
