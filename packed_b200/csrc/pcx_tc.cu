@@ -22,6 +22,7 @@
 #include "pcx_host.hpp"
 #include "pcx_tmem.cuh"
 
+#include <algorithm>
 #include <cuda_bf16.h>
 
 namespace pcxg {
@@ -501,6 +502,356 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     if (warp == 0) tmem_dealloc(taddr, 32);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of mode 0 (N = 2^8..2^12, whole rows): each CTA of 256
+// threads takes items of 4096 points (T = 4096 / N rows) in turn, so the DFT
+// matrix and the TMEM columns are set up once per CTA, not once per row group.
+// A radix-16 stage is one round: every thread builds the operand row of one
+// of the item's 256 butterflies, thread 0 issues two M = 128 products (rows
+// 0..127 and 128..255 into TMEM columns 0..31 and 32..63), and every thread
+// reads its own butterfly's 32 outputs back from its TMEM lane (warps 0-3 the
+// first block, warps 4-7 the second, each in its own lane quarter).  The
+// work buffer is updated in place (all of a stage's reads land in the
+// operands before the first write), so three CTAs fit on an SM in the bfloat16
+// form.  Work element p sits at p + 2*(p/16): the strided reads of the
+// operand build, the Stockham writes and the packs of 8 contiguous elements
+// of the row copies are all conflict-free, and the first stage's 16
+// contiguous outputs per thread go out as 16-byte stores.
+// The same kernel runs a list of items of mixed sizes (the ragged batch's
+// transforms of up to 4096 points), each with its own rows.
+constexpr int TP_NT  = 256;
+constexpr int TP_PTS = 4096;    // points per item
+constexpr int TP_MAXR = TP_PTS / 256;    // rows per item at N = 256
+
+struct tcp_item {
+    int          lg;      // log2 N, 8..12
+    int          rows;    // 1 .. 4096 / N
+    const float* src[TP_MAXR];
+    float*       dst[TP_MAXR];
+};
+
+struct tcp_args {
+    // uniform form: `batch` rows of 2^lg points at src/dst (2N reals apart)
+    const float*    src;
+    float*          dst;
+    long long       batch;
+    int             lg;
+    // list form (when items != nullptr)
+    const tcp_item* items;
+    int             nitems;
+    int             conj;     // inputs and outputs conjugated (the inverse)
+    float           scale;    // on the outputs
+    const void*     tw;       // W_M^i, i < M = 2^tw_lg (tw_lg >= every item's lg)
+    int             tw_lg;
+    int*            error;
+};
+
+template<int PREC>
+struct tcp_cfg {
+    using O                    = op_traits<PREC>;
+    static constexpr int NS    = O::NS;
+    static constexpr int OPB   = (int)sizeof(typename O::elem);
+    static constexpr int WORK  = TP_PTS + TP_PTS / 8;           // complex, padded
+    static constexpr int ABYTE = TP_NT * 32 * OPB;              // one part of the 256 x 32 operand
+    static constexpr int BBYTE = 32 * 32 * OPB;
+    static constexpr int SMEM  = WORK * 8 + NS * ABYTE + NS * BBYTE;
+    static constexpr int MINB  = SMEM <= 74 * 1024 ? 3 : 2;    // CTAs per SM the shared memory allows
+};
+
+__device__ __forceinline__ int tcp_wp(int p) { return p + 2 * (p >> 4); }
+
+// One item of N = 2^LOGN points: rows s_src[r] -> s_dst[r], r < rows.  False
+// when the bounded wait for the products gave up (the CTA then leaves).
+template<int LOGN, int PREC>
+__device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float* const* s_src, float* const* s_dst,
+                                        cpx<float>* work, unsigned char* const (&opA)[op_traits<PREC>::NS],
+                                        unsigned char* const (&opB)[op_traits<PREC>::NS], uint32_t taddr,
+                                        uint64_t* mbar, uint32_t& phase) {
+    using O           = op_traits<PREC>;
+    using E           = typename O::elem;
+    constexpr int NS  = O::NS;
+    constexpr int N   = 1 << LOGN;
+    constexpr int T   = TP_PTS / N;
+    constexpr int R0B = LOGN % 4;
+    constexpr int NTC = LOGN / 4;
+    const int     tid = threadIdx.x;
+    const int     warp = tid / 32;
+    const float   cj   = a.conj ? -1.f : 1.f;
+    const auto*   tw   = reinterpret_cast<const cpx<float>*>(a.tw);
+    const int  tr = tid / (N / 16), bl = tid % (N / 16);
+    // the first tensor-core stage's twiddle factors (W_{16 ns}^(qk), q =
+    // 1,2,3,4,8,12, from the W_M table); each later stage's are requested
+    // while the previous stage's products run
+    cpx<float> fn[6] = {};
+    auto       load_f = [&](int nsx) {
+        if (nsx > 1) {
+            const int k  = bl & (nsx - 1);
+            const int sh = a.tw_lg - 4 - (__ffs(nsx) - 1);
+            fn[0]        = ldg_cpx(tw + ((k) << sh));
+            fn[1]        = ldg_cpx(tw + ((2 * k) << sh));
+            fn[2]        = ldg_cpx(tw + ((3 * k) << sh));
+            fn[3]        = ldg_cpx(tw + ((4 * k) << sh));
+            fn[4]        = ldg_cpx(tw + ((8 * k) << sh));
+            fn[5]        = ldg_cpx(tw + ((12 * k) << sh));
+        }
+    };
+    load_f(1 << R0B);
+    // rows in natural order (conjugated for the inverse); missing rows are
+    // zero.  Two 8-point packs per thread, all loads first.
+    static_assert(T * N / 8 == 2 * TP_NT, "two packs per thread");
+    {
+        float4 v[2][4];
+        static_for<2>([&](auto uc) {
+            constexpr int u   = decltype(uc)::value;
+            const int     q   = tid + u * TP_NT;
+            const int     r   = q / (N / 8), pk8 = q % (N / 8);
+            v[u][0] = v[u][1] = v[u][2] = v[u][3] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (r < rows) {
+                const float4* s = reinterpret_cast<const float4*>(s_src[r] + pk8 * 16);
+                static_for<4>([&](auto hc) { v[u][decltype(hc)::value] = __ldg(s + decltype(hc)::value); });
+            }
+        });
+        static_for<2>([&](auto uc) {
+            constexpr int u   = decltype(uc)::value;
+            const int     q   = tid + u * TP_NT;
+            const int     r   = q / (N / 8), pk8 = q % (N / 8);
+            const float4 &r0 = v[u][0], &r1 = v[u][1], &i0 = v[u][2], &i1 = v[u][3];
+            float4*       w   = reinterpret_cast<float4*>(work + tcp_wp(r * N + pk8 * 8));    // 8 contiguous elements
+            w[0]              = make_float4(r0.x, cj * i0.x, r0.y, cj * i0.y);
+            w[1]              = make_float4(r0.z, cj * i0.z, r0.w, cj * i0.w);
+            w[2]              = make_float4(r1.x, cj * i1.x, r1.y, cj * i1.y);
+            w[3]              = make_float4(r1.z, cj * i1.z, r1.w, cj * i1.w);
+        });
+    }
+    __syncthreads();
+    int ns = 1;
+    // remainder stage (radix 2, 4 or 8) on the CUDA cores, in place
+    if constexpr (R0B > 0) {
+        constexpr int R = 1 << R0B;
+        constexpr int U = 16 / R;    // butterflies per thread
+        cpx<float>    x[16];
+        static_for<U>([&](auto uc) {
+            constexpr int u  = decltype(uc)::value;
+            const int     b  = tid + u * TP_NT;
+            const int     tr = b / (N / R), bl = b % (N / R);
+            static_for<R>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                x[u * R + j]    = work[tcp_wp(tr * N + bl + j * (N / R))];
+            });
+        });
+        __syncthreads();
+        static_for<U>([&](auto uc) {
+            constexpr int u  = decltype(uc)::value;
+            const int     b  = tid + u * TP_NT;
+            const int     tr = b / (N / R), bl = b % (N / R);
+            dft<R, 1, u * R>(x);
+            static_for<R>([&](auto jc) {
+                constexpr int j                     = decltype(jc)::value;
+                work[tcp_wp(tr * N + bl * R + j)] = x[u * R + j];
+            });
+        });
+        ns = R;
+        __syncthreads();
+    }
+    for (int st = 0; st < NTC; ++st) {
+        const int  k = bl & (ns - 1);
+        cpx<float> x[16];
+        // twiddle j of the butterfly: W_{16 ns}^(jk), from the six factors
+        static_for<16>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            cpx<float>    v = work[tcp_wp(tr * N + bl + j * (N / 16))];
+            if constexpr (j > 0) {
+                if (ns > 1) v = cmul(v, stw_factor<4, j>(fn));
+            }
+            x[j] = v;
+        });
+        // operand row tid: reals 0..15 then imaginaries 16..31, one 16-byte
+        // core-matrix row per store
+        static_for<32 / O::PER_CHUNK>([&](auto cc) {
+            constexpr int c = decltype(cc)::value;
+            E             part[NS][O::PER_CHUNK];
+            static_for<O::PER_CHUNK>([&](auto qc) {
+                constexpr int q  = decltype(qc)::value;
+                constexpr int kk = c * O::PER_CHUNK + q;
+                const float   xv = kk < 16 ? x[kk & 15].re : x[kk & 15].im;
+                E             e[NS];
+                O::split(xv, e);
+                static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
+            });
+            static_for<NS>([&](auto ic) {
+                constexpr int i = decltype(ic)::value;
+                uint4         pv;
+                memcpy(&pv, part[i], 16);
+                *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, TP_NT>(tid, c * O::PER_CHUNK)) = pv;
+            });
+        });
+        fence_proxy_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            constexpr uint32_t LBO_A = (TP_NT / 8) * 128, LBO_B = (32 / 8) * 128, SBO = 128;
+            constexpr uint32_t BLK   = (128 / 8) * 128;    // rows 128..255
+            constexpr int      KS    = 32 / O::K_PER_MMA;
+            constexpr int      CH    = O::K_PER_MMA / O::PER_CHUNK;
+            using SP                 = split_products<NS>;
+            static_for<2>([&](auto bc) {
+                constexpr int blk = decltype(bc)::value;
+                uint32_t      acc = 0;
+                static_for<SP::NP>([&](auto pc) {
+                    constexpr int        p  = decltype(pc)::value;
+                    const unsigned char* xa = opA[SP::x(p)] + blk * BLK;
+                    const unsigned char* ab = opB[SP::a(p)];
+                    for (int ks = 0; ks < KS; ++ks) {
+                        umma<PREC>(taddr + 32 * blk, sdesc(xa + ks * CH * LBO_A, LBO_A, SBO),
+                                   sdesc(ab + ks * CH * LBO_B, LBO_B, SBO), O::IDESC, acc);
+                        acc = 1;
+                    }
+                });
+            });
+            umma_commit(mbar);
+        }
+        if (st + 1 < NTC) load_f(ns * 16);
+        const bool ok = mbar_wait_bounded(mbar, phase);
+        if (__syncthreads_or(!ok)) {
+            // give up: record it and let the products in flight finish before TMEM is freed
+            if (tid == 0) {
+                atomicExch(a.error, 1);
+                mbar_wait_bounded(mbar, phase, 100000000ull);
+            }
+            return false;
+        }
+        phase ^= 1;
+        tc_fence_after();
+        uint32_t r[32];
+        tmem_ld32(taddr + ((uint32_t)(32 * (warp % 4)) << 16) + 32 * (warp / 4), r);
+        // outputs of this butterfly, Stockham placement, in place
+        const int base = tr * N + (bl / ns) * ns * 16 + k;
+        if (ns == 1) {
+            // sixteen contiguous outputs: eight 16-byte stores
+            float4* w = reinterpret_cast<float4*>(work + tcp_wp(base));
+            static_for<8>([&](auto jc) {
+                constexpr int j = decltype(jc)::value;
+                w[j]            = make_float4(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 16]),
+                                              __uint_as_float(r[2 * j + 1]), __uint_as_float(r[2 * j + 17]));
+            });
+        } else {
+            static_for<16>([&](auto jc) {
+                constexpr int j                = decltype(jc)::value;
+                work[tcp_wp(base + j * ns)] = {__uint_as_float(r[j]), __uint_as_float(r[j + 16])};
+            });
+        }
+        tc_fence_before();
+        __syncthreads();    // operands, accumulator and work free for the next stage
+        ns *= 16;
+    }
+    // natural order out (conjugated and scaled for the inverse)
+    const float sc = a.scale, sim = a.conj ? -a.scale : a.scale;
+    static_for<2>([&](auto uc) {
+        const int q = tid + decltype(uc)::value * TP_NT;
+        const int r = q / (N / 8), pk8 = q % (N / 8);
+        if (r < rows) {
+            const float4* w  = reinterpret_cast<const float4*>(work + tcp_wp(r * N + pk8 * 8));
+            const float4  w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+            float4*       d  = reinterpret_cast<float4*>(s_dst[r] + pk8 * 16);
+            d[0]             = make_float4(w0.x * sc, w0.z * sc, w1.x * sc, w1.z * sc);
+            d[1]             = make_float4(w2.x * sc, w2.z * sc, w3.x * sc, w3.z * sc);
+            d[2]             = make_float4(w0.y * sim, w0.w * sim, w1.y * sim, w1.w * sim);
+            d[3]             = make_float4(w2.y * sim, w2.w * sim, w3.y * sim, w3.w * sim);
+        }
+    });
+    __syncthreads();    // the work buffer and row pointers are free for the next item
+    return true;
+}
+
+template<int PREC>
+__global__ void __launch_bounds__(TP_NT, tcp_cfg<PREC>::MINB) k_tcp(tcp_args a) {
+    using C          = tcp_cfg<PREC>;
+    using O          = op_traits<PREC>;
+    using E          = typename O::elem;
+    constexpr int NS = O::NS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    cpx<float>*    work = reinterpret_cast<cpx<float>*>(smem);
+    unsigned char* opA[NS];
+    unsigned char* opBw[NS];
+    static_for<NS>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        opA[i]          = smem + C::WORK * 8 + i * C::ABYTE;
+        opBw[i]         = smem + C::WORK * 8 + NS * C::ABYTE + i * C::BBYTE;
+    });
+    __shared__ uint64_t     mbar;
+    __shared__ uint32_t     tslot;
+    __shared__ const float* s_src[TP_MAXR];
+    __shared__ float*       s_dst[TP_MAXR];
+    const int               tid  = threadIdx.x;
+    const int               warp = tid / 32;
+    if (warp == 0) {
+        tmem_alloc(&tslot, 64);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        fence_barrier_init();
+    }
+    // constant operand, once per CTA: the 32 x 32 real DFT matrix, split
+    for (int q = tid; q < 32 * 32; q += TP_NT) {
+        const int n = q / 32, k = q % 32;
+        const int nn = n % 16, kk = k % 16;
+        double    s, c;
+        sincospi(2.0 * (double)((nn * kk) % 16) / 16.0, &s, &c);
+        double v;
+        if (n < 16) v = k < 16 ? c : s;
+        else v = k < 16 ? -s : c;
+        E part[NS];
+        O::split_exact(v, part);
+        static_for<NS>([&](auto ic) {
+            constexpr int i                                        = decltype(ic)::value;
+            *reinterpret_cast<E*>(opBw[i] + op_off<PREC, 32>(n, k)) = part[i];
+        });
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t  taddr  = tslot;
+    uint32_t        phase  = 0;
+    const long long nitems = a.items ? (long long)a.nitems : (a.batch + (TP_PTS >> a.lg) - 1) / (TP_PTS >> a.lg);
+    for (long long j = blockIdx.x; j < nitems; j += gridDim.x) {
+        int lg, rows;
+        if (a.items) {
+            const tcp_item& it = a.items[j];
+            lg                 = it.lg;
+            rows               = it.rows;
+            if (tid < rows) {
+                s_src[tid] = it.src[tid];
+                s_dst[tid] = it.dst[tid];
+            }
+        } else {
+            const int       T  = TP_PTS >> a.lg;
+            const long long r0 = j * T;
+            lg                 = a.lg;
+            rows               = (int)min((long long)T, a.batch - r0);
+            if (tid < rows) {
+                s_src[tid] = a.src + (r0 + tid) * (2LL << lg);
+                s_dst[tid] = a.dst + (r0 + tid) * (2LL << lg);
+            }
+        }
+        __syncthreads();
+        bool ok = true;
+        switch (lg) {
+        case 8: ok = tcp_run<8, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        case 9: ok = tcp_run<9, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        case 10: ok = tcp_run<10, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        case 11: ok = tcp_run<11, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        case 12: ok = tcp_run<12, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        default: break;
+        }
+        if (!ok) break;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, 64);
+}
+
 }    // namespace tc
 }    // namespace pcxg
 
@@ -519,16 +870,19 @@ cudaError_t launch_tc(const tc::tc_args& a, cudaStream_t st) {
     kern<<<(unsigned)grid, tc::NT, C::SMEM, st>>>(a);
     return cudaGetLastError();
 }
+// The persistent whole-row form: resident CTAs, at most one per item.
 template<int PREC>
-cudaError_t dispatch_tc(int log_n, const tc::tc_args& a, cudaStream_t st) {
-    switch (log_n) {
-    case 8: return launch_tc<8, PREC, 0>(a, st);
-    case 9: return launch_tc<9, PREC, 0>(a, st);
-    case 10: return launch_tc<10, PREC, 0>(a, st);
-    case 11: return launch_tc<11, PREC, 0>(a, st);
-    case 12: return launch_tc<12, PREC, 0>(a, st);
-    default: return cudaErrorNotSupported;
-    }
+cudaError_t launch_tcp(const tc::tcp_args& a, long long nitems, int sms, cudaStream_t st) {
+    using C   = tc::tcp_cfg<PREC>;
+    auto kern = tc::k_tcp<PREC>;
+    cudaError_t e = smem_attr_cached(reinterpret_cast<const void*>(kern), C::SMEM);
+    if (e != cudaSuccess) return e;
+    if (nitems <= 0) return cudaSuccess;
+    // C::MINB CTAs per SM (its shared memory and the register bound of
+    // __launch_bounds__); the occupancy query reports one for this kernel
+    const long long grid = std::max<long long>(1, std::min<long long>(nitems, (long long)C::MINB * sms));
+    kern<<<(unsigned)grid, tc::TP_NT, C::SMEM, st>>>(a);
+    return cudaGetLastError();
 }
 // passes of the two-pass form: sub-transforms of 2^6..2^8 points
 template<int PREC, int MODE>
@@ -604,18 +958,22 @@ extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int di
             }
             return PCX_OK;
         }
-        // full W_N table (the plan's single-pass table)
-        tc::tc_args a{};
-        a.src   = static_cast<const float*>(src);
-        a.dst   = static_cast<float*>(dst);
-        a.batch = (long long)batch;
-        a.conj  = direction == PCX_INVERSE;
-        a.scale = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
-        a.twN   = plan->twL;
-        a.error = plan->err;
-        cudaError_t  e  = precision == 0   ? dispatch_tc<tc::PREC_BF16>(plan->log_n, a, st)
-                          : precision == 1 ? dispatch_tc<tc::PREC_TF32>(plan->log_n, a, st)
-                                           : dispatch_tc<tc::PREC_BF16X6>(plan->log_n, a, st);
+        // whole rows: the persistent form, items of 4096 points, the plan's
+        // full W_N table
+        tc::tcp_args a{};
+        a.src    = static_cast<const float*>(src);
+        a.dst    = static_cast<float*>(dst);
+        a.batch  = (long long)batch;
+        a.lg     = plan->log_n;
+        a.conj   = direction == PCX_INVERSE;
+        a.scale  = (direction == PCX_INVERSE && normalize) ? 1.0f / (float)plan->n : 1.0f;
+        a.tw     = plan->twL;
+        a.tw_lg  = plan->log_n;
+        a.error  = plan->err;
+        const long long items = ((long long)batch + (tc::TP_PTS >> plan->log_n) - 1) / (tc::TP_PTS >> plan->log_n);
+        cudaError_t     e     = precision == 0   ? launch_tcp<tc::PREC_BF16>(a, items, plan->sms, st)
+                                : precision == 1 ? launch_tcp<tc::PREC_TF32>(a, items, plan->sms, st)
+                                                 : launch_tcp<tc::PREC_BF16X6>(a, items, plan->sms, st);
         PCX_CUDA_TRY(e);
         return PCX_OK;
     });

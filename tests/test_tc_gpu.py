@@ -76,3 +76,23 @@ def test_tc_sizes_outside_the_form_are_refused():
         x = torch.zeros(2 * n, device="cuda")
         with pytest.raises(NotImplementedError, match="tensor-core form"):
             unit.exec_tensor_core(x, x, batch=1)
+
+
+@pytest.mark.parametrize("log_n,b", [(8, 20000), (10, 3001), (12, 1500)])
+def test_tc_persistent_many_items_per_cta(log_n, b):
+    """Whole-row sizes run as a persistent launch: with a batch of several
+    items per resident CTA (items of 4096 points, the last one partial) every
+    row must match the plain FP32 transform to the split form's accuracy."""
+    n = 1 << log_n
+    x = torch.randn(b, 2 * n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(log_n + b))
+    unit = fft_unit(n)
+    want = torch.empty_like(x)
+    unit.exec(want, x, batch=b)
+    for precision in ("bf16x6", "tf32"):
+        y = torch.full_like(x, float("nan"))
+        unit.exec_tensor_core(y, x, batch=b, precision=precision)
+        torch.cuda.synchronize()
+        unit.status()
+        d = (y - want).double()
+        rel = (d.norm(dim=1) / want.double().norm(dim=1)).max().item()
+        assert rel < TOL[np.float32], (precision, rel)
