@@ -667,6 +667,9 @@ class C5Ragged:
             self.xcs.append((y, x, int(s), taps, nf))
             self.xunits.append(fxcorr_unit(taps, nf))
         self.batch = ragged_batch(ffts, self.xcs)
+        # the same batch with the transforms of 2^8..2^12 points in the
+        # tensor-core form (bf16 x6, FP32-level accuracy), timed beside it
+        self.batch_tc = ragged_batch(ffts, self.xcs, tensor_core="bf16x6")
         self.fft_points = sum(cnt << lg for lg, (cnt, _, _, _) in self.groups.items())
         self.fft_flops = sum(cnt * 5 * (lg << lg) for lg, (cnt, _, _, _) in self.groups.items())
         self.xc_ffts, self.xc_flops = 0, 0
@@ -676,11 +679,13 @@ class C5Ragged:
             self.xc_flops += 2 * blocks * 5 * nf * (nf.bit_length() - 1)
 
     def parts(self):
-        return ["ragged_graph", "plain_per_size"]
+        return ["ragged_graph", "ragged_graph_tc", "plain_per_size"]
 
     def run_part(self, key):
         if key == "ragged_graph":
             self.batch()
+        elif key == "ragged_graph_tc":
+            self.batch_tc()
         else:
             for lg, (cnt, src, dst, u) in self.groups.items():
                 u.exec(dst, src, batch=cnt, check=False)
@@ -696,6 +701,7 @@ class C5Ragged:
 
     def check_status(self):
         self.batch.status()
+        self.batch_tc.status()
         for _, _, _, u in self.groups.values():
             u.status()
         for u in self.xunits:
@@ -717,16 +723,27 @@ class C5Ragged:
         def rel(got, want):
             return torch.linalg.vector_norm(got - want, dim=-1) / torch.linalg.vector_norm(want, dim=-1)
 
+        def worst_fft(lgs):
+            w = 0.0
+            for lg in lgs:
+                cnt, src, dst, _ = self.groups[lg]
+                n = 1 << lg
+                for r0 in range(0, cnt, 128):
+                    r1 = min(cnt, r0 + 128)
+                    e = rel(rows(dst[r0 * 2 * n:r1 * 2 * n], n), torch.fft.fft(rows(src[r0 * 2 * n:r1 * 2 * n], n)))
+                    w = max(w, float(e.max()))
+            return w
+
+        # the tensor-core batch first (same outputs), its transforms of 2^8..2^12
+        self.batch_tc()
+        torch.cuda.synchronize()
+        self.batch_tc.status()
+        w_tc = worst_fft([lg for lg in self.groups if 8 <= lg <= 12])
         self.batch()
         torch.cuda.synchronize()
         self.batch.status()
-        w_fft = w_xc = 0.0
-        for lg, (cnt, src, dst, _) in self.groups.items():
-            n = 1 << lg
-            for r0 in range(0, cnt, 128):
-                r1 = min(cnt, r0 + 128)
-                e = rel(rows(dst[r0 * 2 * n:r1 * 2 * n], n), torch.fft.fft(rows(src[r0 * 2 * n:r1 * 2 * n], n)))
-                w_fft = max(w_fft, float(e.max()))
+        w_xc = 0.0
+        w_fft = worst_fft(list(self.groups))
         for y, x, s, taps, _ in self.xcs:
             k = taps.size()
             kp = (k + 7) // 8 * 8
@@ -735,13 +752,16 @@ class C5Ragged:
             want = torch.fft.ifft(torch.fft.fft(rows(x, s)[0], L) * torch.conj(torch.fft.fft(g, L)))[:s]
             w_xc = max(w_xc, float(rel(rows(y, s)[0], want)))
         return {"ragged_fft_max_rel_l2": w_fft, "ragged_xcorr_max_rel_l2": w_xc,
+                "ragged_tc_bf16x6_fft_max_rel_l2": w_tc,
                 "transforms": sum(c for c, _, _, _ in self.groups.values()), "correlations": len(self.xcs)}
 
     def e2e(self, torch, stream):
         return None
 
     def launches(self):
-        return 1 + len(self.groups) + self.n_xc
+        # the ragged graph; the tensor-core graph (ragged launch + tensor-core
+        # launch); per-size plain launches and one per correlation
+        return 1 + 2 + len(self.groups) + self.n_xc
 
     def cpu_reference(self, budget_s=12.0):
         c2 = C2Sweep()

@@ -349,6 +349,16 @@ int pcx_ragged_create(pcx_ragged* h, int dtype, size_t n_fft, const size_t* size
                       const void* const* src, int direction, int normalize, size_t n_xc, const size_t* xc_len,
                       const size_t* xc_k, const void* const* xc_g, const size_t* xc_nfft, void* const* xc_dst,
                       const void* const* xc_src);
+/*
+ * As pcx_ragged_create, with the transforms of 2^8..2^12 points run by the
+ * tensor-core form (a second persistent launch in the same graph, items of
+ * 4096 points; the precision as pcx_tc_fft_exec: 0 bf16 x3, 1 tf32 x3,
+ * 2 bf16 x6); tensor_core = -1 is pcx_ragged_create.
+ */
+int pcx_ragged_create_tc(pcx_ragged* h, int dtype, size_t n_fft, const size_t* sizes, void* const* dst,
+                         const void* const* src, int direction, int normalize, size_t n_xc, const size_t* xc_len,
+                         const size_t* xc_k, const void* const* xc_g, const size_t* xc_nfft, void* const* xc_dst,
+                         const void* const* xc_src, int tensor_core);
 int pcx_ragged_exec(pcx_ragged h, void* stream);
 /* PCX_ERR_TIMEOUT if a work item gave up waiting for a dependency (synchronises). */
 int pcx_ragged_status(pcx_ragged h);

@@ -14,7 +14,9 @@
 // Every buffer must reach the GPU (device or managed memory, as pcxo::vector's
 // default allocator gives) and be 16-byte aligned; its storage is used in
 // place, so the objects must outlive the batch.  All FFTs are forward, or all
-// inverse (normalised: then of one size).
+// inverse (normalised: then of one size).  With tensor_core (0 bf16 x3,
+// 1 tf32 x3, 2 bf16 x6) the transforms of 2^8..2^12 points run in the
+// tensor-core form, a second persistent launch in the same graph.
 #ifndef PCXO_RAGGED_HPP
 #define PCXO_RAGGED_HPP
 
@@ -54,9 +56,10 @@ inline uZ correlation_fft_size(uZ k, uZ max_size = 16384) {
 
 class ragged_batch {
 public:
-    explicit ragged_batch(bool inverse = false, bool normalized = true)
+    explicit ragged_batch(bool inverse = false, bool normalized = true, int tensor_core = -1)
     : m_inverse(inverse)
-    , m_normalized(normalized) {}
+    , m_normalized(normalized)
+    , m_tensor_core(tensor_core) {}
     ragged_batch(const ragged_batch&)            = delete;
     ragged_batch& operator=(const ragged_batch&) = delete;
 
@@ -100,10 +103,10 @@ public:
     void build() {
         if (m_handle) return;
         pcx_ragged h = nullptr;
-        detail_::check(pcx_ragged_create(&h, PCX_F32, m_sizes.size(), m_sizes.data(), m_dst.data(), m_src.data(),
-                                         m_inverse ? PCX_INVERSE : PCX_FORWARD, m_normalized ? 1 : 0, m_xlen.size(),
-                                         m_xlen.data(), m_xk.data(), m_xg.data(), m_xn.data(), m_xdst.data(),
-                                         m_xsrc.data()));
+        detail_::check(pcx_ragged_create_tc(&h, PCX_F32, m_sizes.size(), m_sizes.data(), m_dst.data(),
+                                            m_src.data(), m_inverse ? PCX_INVERSE : PCX_FORWARD, m_normalized ? 1 : 0,
+                                            m_xlen.size(), m_xlen.data(), m_xk.data(), m_xg.data(), m_xn.data(),
+                                            m_xdst.data(), m_xsrc.data(), m_tensor_core));
         m_handle.reset(h, [](pcx_ragged q) { pcx_ragged_destroy(q); });
     }
 
@@ -125,6 +128,7 @@ private:
 
     bool                                               m_inverse;
     bool                                               m_normalized;
+    int                                                m_tensor_core;
     std::vector<std::size_t>                           m_sizes;
     std::vector<void*>                                 m_dst;
     std::vector<const void*>                           m_src;

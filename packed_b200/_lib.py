@@ -59,6 +59,10 @@ SIGNATURES: dict[str, tuple] = {
     "pcx_ragged_create": (_i, [ctypes.POINTER(_vp), _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_vp),
                                ctypes.POINTER(_vp), _i, _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                ctypes.POINTER(_vp), ctypes.POINTER(_sz), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "pcx_ragged_create_tc": (_i, [ctypes.POINTER(_vp), _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_vp),
+                                  ctypes.POINTER(_vp), _i, _i, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
+                                  ctypes.POINTER(_vp), ctypes.POINTER(_sz), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                  _i]),
     "pcx_ragged_exec": (_i, [_vp, _vp]),
     "pcx_ragged_status": (_i, [_vp]),
     "pcx_ragged_items": (_sz, [_vp]),

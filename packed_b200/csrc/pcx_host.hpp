@@ -186,6 +186,24 @@ cudaError_t pcx_gen_twiddles(void* out, int count, int log_n, long long mult, bo
 // for the in-CTA four-step correlator (pcx_fxcorr.cu).
 cudaError_t pcx_xc2_perm_spectrum(const void* ks, void* kp, int log_n1, int log_n2, cudaStream_t st);
 
+namespace pcxg {
+// One work item of the persistent tensor-core FFT (pcx_tc.cu): `rows`
+// transforms of 2^lg points (8 <= lg <= 12, rows <= 2^(12 - lg)), complex64
+// pack 8, each from its own source row to its own destination row.
+struct tc_item {
+    int          lg;
+    int          rows;
+    const float* src[16];
+    float*       dst[16];
+};
+}    // namespace pcxg
+// The persistent tensor-core FFT over a device list of items (precision 0
+// bf16 x3, 1 tf32 x3, 2 bf16 x6): conj = 1 conjugates inputs and outputs (the
+// inverse), scale multiplies the outputs; tw = W_M^i (i < M = 2^tw_lg >= every
+// item's size).  Resident CTAs, at most one per item.
+cudaError_t pcx_tc_list_launch(int precision, const pcxg::tc_item* items, int nitems, int conj, float scale,
+                               const void* tw, int tw_lg, int* error, int sms, cudaStream_t st);
+
 // Hot-path launches (pcx_v2_*.cu); cudaErrorNotSupported when no variant exists.
 cudaError_t pcx_v2_single(bool f64, int log_n, const pcxg::v2_args& a, cudaStream_t st, bool attr_only);
 cudaError_t pcx_v3_single(bool f64, int log_n, const pcxg::v3_args& a, cudaStream_t st, int sms, bool attr_only);

@@ -1283,10 +1283,22 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                                  const void* const* src, int direction, int normalize, size_t n_xc,
                                  const size_t* xc_len, const size_t* xc_k, const void* const* xc_g,
                                  const size_t* xc_nfft, void* const* xc_dst, const void* const* xc_src) {
+    return pcx_ragged_create_tc(out, dtype, n_fft, sizes, dst, src, direction, normalize, n_xc, xc_len, xc_k, xc_g,
+                                xc_nfft, xc_dst, xc_src, -1);
+}
+
+extern "C" int pcx_ragged_create_tc(pcx_ragged* out, int dtype, size_t n_fft, const size_t* sizes, void* const* dst,
+                                    const void* const* src, int direction, int normalize, size_t n_xc,
+                                    const size_t* xc_len, const size_t* xc_k, const void* const* xc_g,
+                                    const size_t* xc_nfft, void* const* xc_dst, const void* const* xc_src,
+                                    int tensor_core) {
     return pcx_guard([&]() -> int {
         if (!out) return pcx_fail(PCX_ERR_INVALID, "handle pointer is null");
         *out = nullptr;
         if (dtype != PCX_F32) return pcx_fail(PCX_ERR_UNSUPPORTED, "ragged batches are built for complex64");
+        if (tensor_core < -1 || tensor_core > 2) {
+            return pcx_fail(PCX_ERR_INVALID, "tensor_core: -1 off, 0 bf16x3, 1 tf32x3, 2 bf16x6");
+        }
         auto  h    = new pcx_ragged_s{};
         auto  fail = [&](int rc) {
             pcx_ragged_destroy(h);
@@ -1313,6 +1325,24 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         h->A.conj  = direction == PCX_INVERSE;
         h->A.scale = 1.0f;
+        // the tensor-core form takes the transforms of 2^8..2^12 points
+        std::map<int, std::vector<int>> tc_by_lg;
+        if (tensor_core >= 0) {
+            for (int lg = 8; lg <= 12; ++lg) {
+                auto it = by_lg.find(lg);
+                if (it == by_lg.end()) continue;
+                tc_by_lg[lg] = std::move(it->second);
+                by_lg.erase(it);
+            }
+        }
+        if (normalize && direction == PCX_INVERSE) {
+            // one scale per launch: every transform of an inverse batch must share N
+            if (by_lg.size() + tc_by_lg.size() > 1) {
+                return fail(pcx_fail(PCX_ERR_UNSUPPORTED, "a normalised inverse ragged batch needs one size"));
+            }
+            const int lg = by_lg.empty() ? (tc_by_lg.empty() ? 0 : tc_by_lg.begin()->first) : by_lg.begin()->first;
+            h->A.scale = 1.0f / float(size_t(1) << lg);
+        }
         std::map<int, pcx_plan> plan_of;
         auto get_plan = [&](int lg) -> pcx_plan {
             auto it = plan_of.find(lg);
@@ -1349,13 +1379,6 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
                 if ((e = pcx_gen_twiddles(b + n1 + n2, n2, l2 + 4, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
                 h->A.col_tiles[lg] = n2 / (rg::NT / std::max(1, n1 / 16));
                 h->A.row_tiles[lg] = n1 / (rg::NT / std::max(1, n2 / 16));
-            }
-            if (normalize && direction == PCX_INVERSE) {
-                // one scale per launch: every transform of an inverse batch must share N
-                if (by_lg.size() > 1) {
-                    return fail(pcx_fail(PCX_ERR_UNSUPPORTED, "a normalised inverse ragged batch needs one size"));
-                }
-                h->A.scale = 1.0f / float(size_t(1) << lg);
             }
         }
         // full stage tables of 2^6, 2^7, 2^8 and 2^10 points, copied to shared memory by every block
@@ -1557,7 +1580,31 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
             }
         }
         h->n_fft   = n_fft;
-        h->n_items = items.size();
+        // tensor-core items: 4096 points each (2^(12 - lg) transforms of one size)
+        std::vector<tc_item> tc_items;
+        for (auto& [lg, idx]: tc_by_lg) {
+            const size_t per = size_t(1) << (12 - lg);
+            for (size_t q = 0; q < idx.size(); q += per) {
+                tc_item ti{};
+                ti.lg   = lg;
+                ti.rows = (int)std::min(per, idx.size() - q);
+                for (int r = 0; r < ti.rows; ++r) {
+                    ti.src[r] = static_cast<const float*>(src[idx[q + r]]);
+                    ti.dst[r] = static_cast<float*>(dst[idx[q + r]]);
+                }
+                tc_items.push_back(ti);
+            }
+        }
+        const tc_item* d_tc = nullptr;
+        void*          tc_tw = nullptr;
+        if (!tc_items.empty()) {
+            d_tc = static_cast<const tc_item*>(upload(h, tc_items, &e));
+            if (e != cudaSuccess) return cuda_fail(e);
+            // W_4096^i, i < 4096: every item size reads it at a stride
+            if ((e = dev_alloc(4096 * 8, &tc_tw)) != cudaSuccess) return cuda_fail(e);
+            if ((e = pcx_gen_twiddles(tc_tw, 4096, 12, 1, false, 0)) != cudaSuccess) return cuda_fail(e);
+        }
+        h->n_items = items.size() + tc_items.size();
         // ---- device state
         h->A.items = static_cast<const rg::item*>(upload(h, items, &e));
         if (e == cudaSuccess) h->A.req = static_cast<const rg::fft_req*>(upload(h, req, &e));
@@ -1603,6 +1650,10 @@ extern "C" int pcx_ragged_create(pcx_ragged* out, int dtype, size_t n_fft, const
         if (e == cudaSuccess) {
             rg::k_ragged<<<h->grid, rg::NT + 64, rg::SMEM, cs>>>(d_args);
             e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && !tc_items.empty()) {
+            e = pcx_tc_list_launch(tensor_core, d_tc, (int)tc_items.size(), h->A.conj, h->A.scale, tc_tw, 12,
+                                   h->A.error, sms, cs);
         }
         cudaError_t e2 = cudaStreamEndCapture(cs, &h->graph);
         if (e == cudaSuccess) e = e2;

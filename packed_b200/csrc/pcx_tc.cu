@@ -523,12 +523,8 @@ constexpr int TP_NT  = 256;
 constexpr int TP_PTS = 4096;    // points per item
 constexpr int TP_MAXR = TP_PTS / 256;    // rows per item at N = 256
 
-struct tcp_item {
-    int          lg;      // log2 N, 8..12
-    int          rows;    // 1 .. 4096 / N
-    const float* src[TP_MAXR];
-    float*       dst[TP_MAXR];
-};
+using tcp_item = tc_item;    // lg 8..12, rows 1 .. 4096 / N, one source and destination row each
+static_assert(sizeof(((tc_item*)nullptr)->src) / sizeof(const float*) == TP_MAXR, "rows per item");
 
 struct tcp_args {
     // uniform form: `batch` rows of 2^lg points at src/dst (2N reals apart)
@@ -895,6 +891,21 @@ cudaError_t dispatch_tc_pass(int log_n, const tc::tc_args& a, cudaStream_t st) {
     }
 }
 }    // namespace
+
+cudaError_t pcx_tc_list_launch(int precision, const pcxg::tc_item* items, int nitems, int conj, float scale,
+                               const void* tw, int tw_lg, int* error, int sms, cudaStream_t st) {
+    tc::tcp_args a{};
+    a.items  = items;
+    a.nitems = nitems;
+    a.conj   = conj;
+    a.scale  = scale;
+    a.tw     = tw;
+    a.tw_lg  = tw_lg;
+    a.error  = error;
+    return precision == 0   ? launch_tcp<tc::PREC_BF16>(a, nitems, sms, st)
+           : precision == 1 ? launch_tcp<tc::PREC_TF32>(a, nitems, sms, st)
+                            : launch_tcp<tc::PREC_BF16X6>(a, nitems, sms, st);
+}
 
 // Tensor-core transform of `batch` contiguous rows (pack 8, natural order).
 extern "C" int pcx_tc_fft_exec(pcx_plan plan, void* dst, const void* src, int direction, int normalize,

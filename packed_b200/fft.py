@@ -549,9 +549,13 @@ class ragged_batch:
     (``n`` in 2^5..2^18).  ``xcorrs``: list of ``(dst, src, length, g, n_fft)``
     with ``g`` a :class:`vector` of kernel taps (out of place).  Pointers are
     fixed at construction; calling the object replays the graph.
+    ``tensor_core`` ("bf16", "tf32" or "bf16x6", as ``fft_unit.exec_tensor_core``)
+    runs the transforms of 2^8..2^12 points in the tensor-core form, a second
+    persistent launch in the same graph (pcx_ragged_create_tc).
     """
 
-    def __init__(self, ffts, xcorrs=(), direction: int = 0, normalize: bool = True):
+    def __init__(self, ffts, xcorrs=(), direction: int = 0, normalize: bool = True,
+                 tensor_core: str | None = None):
         n = len(ffts)
         m = len(xcorrs)
         sz = (ctypes.c_size_t * max(n, 1))(*[int(f[2]) for f in ffts])
@@ -565,8 +569,9 @@ class ragged_batch:
         xs = (ctypes.c_void_p * max(m, 1))(*[x[1].data_ptr() for x in xcorrs])
         self._keep = (ffts, xcorrs)
         self._h = ctypes.c_void_p()
-        _lib.check(_lib.lib().pcx_ragged_create(ctypes.byref(self._h), _lib.PCX_F32, n, sz, dsts, srcs, direction,
-                                                int(normalize), m, xl, xk, xg, xn, xd, xs))
+        tc = -1 if tensor_core is None else {"bf16": 0, "tf32": 1, "bf16x6": 2}[tensor_core]
+        _lib.check(_lib.lib().pcx_ragged_create_tc(ctypes.byref(self._h), _lib.PCX_F32, n, sz, dsts, srcs,
+                                                   direction, int(normalize), m, xl, xk, xg, xn, xd, xs, tc))
 
     def __call__(self, stream=None) -> None:
         _lib.check(_lib.lib().pcx_ragged_exec(self._h, _stream_ptr(stream)))

@@ -145,6 +145,15 @@ int main() {
         expect(worst < 2e-6, "ragged_batch FFTs (256, 2048, 8192)", worst);
         expect(rel_err(yv, y) < 2e-6, "ragged_batch correlation", rel_err(yv, y));
         expect(batch.items() > 3, "ragged_batch work items");
+        // the tensor-core form (bf16 x6) for the 256- and 2048-point transforms
+        for (std::size_t q = 0; q < 3; ++q)
+            for (std::size_t i = 0; i < dst[q].size(); ++i) dst[q][i] = std::complex<float>(0, 0);
+        pcxo::ragged_batch tc(false, true, 2);
+        for (std::size_t q = 0; q < 3; ++q) tc.add_fft(dst[q], src[q]);
+        tc();
+        worst = 0;
+        for (std::size_t q = 0; q < 3; ++q) worst = std::max(worst, rel_err(dst[q], want[q]));
+        expect(worst < 2e-6, "ragged_batch tensor-core form (256, 2048 on tcgen05; 8192)", worst);
     }
     {    // md::dynamic_storage (mdstorage.hpp): rows as vectors and batched row transforms
         enum class ax { x, y, z };

@@ -161,3 +161,41 @@ def test_ragged_rejects_mixed_normalised_inverse_and_misaligned_buffers():
     c = torch.zeros(2 * 1024 + 2, device="cuda")
     with pytest.raises(ValueError):
         ragged_batch([(c[2:], c[2:], 1024)])    # 8-byte offset: not 16-byte aligned
+
+
+@pytest.mark.parametrize("precision", ["bf16x6", "tf32"])
+def test_ragged_tensor_core_form(precision):
+    """With tensor_core set, the transforms of 2^8..2^12 points run in the
+    persistent tensor-core form beside the ragged launch (one graph): every
+    transform of a mixed batch (all sizes 2^5..2^14, ragged counts per size,
+    plus correlations) and a normalised inverse of one size against the
+    oracle at the FP32 bar."""
+    rng = np.random.default_rng(900)
+    sizes = [1 << int(v) for v in rng.integers(5, 15, 70)] + [256] * 17 + [4096] * 3
+    zs, ffts = [], []
+    for n in sizes:
+        z = normal_cx(rng, n)
+        zs.append(z)
+        ffts.append((torch.full((2 * n,), float("nan"), device="cuda"), dev(O.pack(z, 8)), n))
+    x, g = normal_cx(rng, 20000), normal_cx(rng, 700)
+    xc = (torch.full((len(O.pack(x, 8)),), float("nan"), device="cuda"), dev(O.pack(x, 8)), 20000,
+          vector.from_complex(g), 2048)
+    batch = ragged_batch(ffts, [xc], tensor_core=precision)
+    for replay in range(2):
+        batch()
+        torch.cuda.synchronize()
+        batch.status()
+        for (d, _, n), z in zip(ffts, zs):
+            assert rel_l2(O.unpack(d.cpu().numpy(), n, 8), np.fft.fft(z)) < TOL[np.float32], (replay, n)
+        assert rel_l2(O.unpack(xc[0].cpu().numpy(), 20000, 8), O.xcorr_ols(x, g, 2048)) < TOL[np.float32]
+    # inverse, normalised, one size in the tensor-core range
+    n = 1024
+    z = normal_cx(rng, 11, n)
+    src = [dev(O.pack(z[i], 8)) for i in range(11)]
+    dst = [torch.full_like(s, float("nan")) for s in src]
+    inv = ragged_batch([(dst[i], src[i], n) for i in range(11)], direction=1, tensor_core=precision)
+    inv()
+    torch.cuda.synchronize()
+    inv.status()
+    for i in range(11):
+        assert rel_l2(O.unpack(dst[i].cpu().numpy(), n, 8), np.fft.ifft(z[i])) < TOL[np.float32], i
