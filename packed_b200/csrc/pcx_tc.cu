@@ -84,6 +84,21 @@ struct op_traits<PREC_BF16> {
         p[0] = __bfloat16_as_ushort(__double2bfloat16(v));
         p[1] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0])));
     }
+    // two adjacent K elements (lo, hi) rounded together into one 32-bit word
+    // (the same round-to-nearest per element as bf()), and back to floats
+    __device__ static uint32_t pk2(float lo, float hi) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+    __device__ static float2 unpk2(uint32_t w) {
+        return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+    }
+    // split() of two adjacent elements, parts packed in pairs
+    __device__ static void split2(float lo, float hi, uint32_t (&w)[NS]) {
+        w[0]           = pk2(lo, hi);
+        const float2 f = unpk2(w[0]);
+        w[1]           = pk2(lo - f.x, hi - f.y);
+    }
 };
 template<>
 struct op_traits<PREC_BF16X6> : op_traits<PREC_BF16> {
@@ -98,6 +113,14 @@ struct op_traits<PREC_BF16X6> : op_traits<PREC_BF16> {
         p[0] = __bfloat16_as_ushort(__double2bfloat16(v));
         p[1] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0])));
         p[2] = __bfloat16_as_ushort(__double2bfloat16(v - (double)fl(p[0]) - (double)fl(p[1])));
+    }
+    __device__ static void split2(float lo, float hi, uint32_t (&w)[NS]) {
+        w[0]            = pk2(lo, hi);
+        const float2 f0 = unpk2(w[0]);
+        const float  rl = lo - f0.x, rh = hi - f0.y;    // exact
+        w[1]            = pk2(rl, rh);
+        const float2 f1 = unpk2(w[1]);
+        w[2]            = pk2(rl - f1.x, rh - f1.y);
     }
 };
 template<>
@@ -665,20 +688,30 @@ __device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float
         // core-matrix row per store
         static_for<32 / O::PER_CHUNK>([&](auto cc) {
             constexpr int c = decltype(cc)::value;
-            E             part[NS][O::PER_CHUNK];
-            static_for<O::PER_CHUNK>([&](auto qc) {
-                constexpr int q  = decltype(qc)::value;
-                constexpr int kk = c * O::PER_CHUNK + q;
-                const float   xv = kk < 16 ? x[kk & 15].re : x[kk & 15].im;
-                E             e[NS];
-                O::split(xv, e);
-                static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
-            });
+            uint32_t      part[NS][4];
+            if constexpr (PREC == PREC_TF32) {
+                static_for<4>([&](auto qc) {
+                    constexpr int q  = decltype(qc)::value;
+                    constexpr int kk = c * 4 + q;
+                    E             e[NS];
+                    O::split(kk < 16 ? x[kk & 15].re : x[kk & 15].im, e);
+                    static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
+                });
+            } else {
+                // bfloat16: adjacent pairs rounded together, one word per pair and part
+                static_for<4>([&](auto qc) {
+                    constexpr int q  = decltype(qc)::value;
+                    constexpr int kk = c * 8 + 2 * q;
+                    uint32_t      w[NS];
+                    O::split2(kk < 16 ? x[kk & 15].re : x[kk & 15].im,
+                              kk + 1 < 16 ? x[(kk + 1) & 15].re : x[(kk + 1) & 15].im, w);
+                    static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = w[decltype(ic)::value]; });
+                });
+            }
             static_for<NS>([&](auto ic) {
                 constexpr int i = decltype(ic)::value;
-                uint4         pv;
-                memcpy(&pv, part[i], 16);
-                *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, TP_NT>(tid, c * O::PER_CHUNK)) = pv;
+                *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, TP_NT>(tid, c * O::PER_CHUNK)) =
+                    make_uint4(part[i][0], part[i][1], part[i][2], part[i][3]);
             });
         });
         fence_proxy_async_smem();
