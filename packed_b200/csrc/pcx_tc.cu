@@ -392,20 +392,30 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             // core-matrix row per store
             static_for<32 / O::PER_CHUNK>([&](auto cc) {
                 constexpr int c = decltype(cc)::value;
-                E             part[NS][O::PER_CHUNK];
-                static_for<O::PER_CHUNK>([&](auto qc) {
-                    constexpr int q  = decltype(qc)::value;
-                    constexpr int kk = c * O::PER_CHUNK + q;
-                    const float   xv = kk < 16 ? x[kk & 15].re : x[kk & 15].im;
-                    E             e[NS];
-                    O::split(xv, e);
-                    static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
-                });
+                uint32_t      part[NS][4];
+                if constexpr (PREC == PREC_TF32) {
+                    static_for<4>([&](auto qc) {
+                        constexpr int q  = decltype(qc)::value;
+                        constexpr int kk = c * 4 + q;
+                        E             e[NS];
+                        O::split(kk < 16 ? x[kk & 15].re : x[kk & 15].im, e);
+                        static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = e[decltype(ic)::value]; });
+                    });
+                } else {
+                    // bfloat16: adjacent pairs rounded together, one word per pair and part
+                    static_for<4>([&](auto qc) {
+                        constexpr int q  = decltype(qc)::value;
+                        constexpr int kk = c * 8 + 2 * q;
+                        uint32_t      w[NS];
+                        O::split2(kk < 16 ? x[kk & 15].re : x[kk & 15].im,
+                                  kk + 1 < 16 ? x[(kk + 1) & 15].re : x[(kk + 1) & 15].im, w);
+                        static_for<NS>([&](auto ic) { part[decltype(ic)::value][q] = w[decltype(ic)::value]; });
+                    });
+                }
                 static_for<NS>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
-                    uint4         pv;
-                    memcpy(&pv, part[i], 16);
-                    *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) = pv;
+                    *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) =
+                        make_uint4(part[i][0], part[i][1], part[i][2], part[i][3]);
                 });
             });
             fence_proxy_async_smem();
