@@ -14,8 +14,10 @@
 // The dropped lo*lo term and the representation error of hi + lo set the
 // accuracy (about 2^-16 per stage for bfloat16, 2^-21 for tf32).
 //
-// One CTA of 128 threads transforms T rows; thread i owns TMEM lane i (one
-// butterfly per 128-row block).  Twiddles, the remainder radix-2/4/8 stage and
+// k_tcfft (the two passes of 2^13..2^16 points): one CTA of 128 threads
+// transforms T rows; thread i owns TMEM lane i (one butterfly per 128-row
+// block).  k_tcp (whole rows of 2^8..2^12 points): persistent CTAs of 256
+// threads, one round of products per radix-16 stage.  Twiddles, the remainder radix-2/4/8 stage and
 // the data movement stay on the CUDA cores; one elected thread issues the
 // MMAs and commits them to an mbarrier.  Every mbarrier wait is bounded.
 #include "pcx_fft_v2.cuh"
@@ -187,8 +189,8 @@ struct tc_args {
     const void*  tw_lo;       // W_M^i, i < 2^lg_other (mode 1)
 };
 
-// Modes of one launch:
-//   0: `batch` contiguous rows of N points, natural order in and out;
+// The two passes of a transform of 2^13..2^16 points (whole rows of 2^8..2^12
+// points run in k_tcp below), one launch each:
 //   1: column pass of a two-pass transform of M = N * C points laid out as
 //      N rows of C (C = 2^lg_other): each CTA transforms T adjacent columns
 //      of one transform, multiplies output k of column c by W_M^(c k) and
@@ -218,7 +220,8 @@ struct tc_cfg {
 
 template<int LOGN, int PREC, int MODE>
 __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
-    static_assert(MODE == 0 || tc_cfg<LOGN, PREC>::T % 8 == 0, "two-pass modes move whole packs of columns");
+    static_assert((MODE == 1 || MODE == 2) && tc_cfg<LOGN, PREC>::T % 8 == 0,
+                  "the two passes move whole packs of columns (whole rows: k_tcp)");
     using C  = tc_cfg<LOGN, PREC>;
     using O  = op_traits<PREC>;
     using E  = typename O::elem;
@@ -517,17 +520,6 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
             d[1] = make_float4(w(4).re * sc, w(5).re * sc, w(6).re * sc, w(7).re * sc);
             d[2] = make_float4(w(0).im * sim, w(1).im * sim, w(2).im * sim, w(3).im * sim);
             d[3] = make_float4(w(4).im * sim, w(5).im * sim, w(6).im * sim, w(7).im * sim);
-        }
-    } else if (!aborted) {
-        const float sc = a.scale, sim = conj_out ? -a.scale : a.scale;
-        for (int q = tid; q < rows * N / 8; q += NT) {
-            const int         r = q / (N / 8), pk8 = q % (N / 8);
-            const cpx<float>* w = in + wp(r * N + pk8 * 8);    // 8 elements, no pad inside
-            float4*           d = reinterpret_cast<float4*>(a.dst + (row0 + r) * (2 * N) + pk8 * 16);
-            d[0] = make_float4(w[0].re * sc, w[1].re * sc, w[2].re * sc, w[3].re * sc);
-            d[1] = make_float4(w[4].re * sc, w[5].re * sc, w[6].re * sc, w[7].re * sc);
-            d[2] = make_float4(w[0].im * sim, w[1].im * sim, w[2].im * sim, w[3].im * sim);
-            d[3] = make_float4(w[4].im * sim, w[5].im * sim, w[6].im * sim, w[7].im * sim);
         }
     }
     tc_fence_before();
