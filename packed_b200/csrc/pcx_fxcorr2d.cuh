@@ -442,8 +442,11 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d_kgrad(xc2_kg_args A) {
     };
     // warp 0: the bulk copies of the whole rows that lie inside the valid
     // samples (thread 0 first claims the next item when ph == 0)
-    auto copy_window = [&](int ph) {
-        if (tid == 0) {
+    // rows [lo, hi) of the window (the part of them inside the valid samples);
+    // `claim` first sets the window up (the whole window's bytes expected on
+    // `full`), so a window may arrive in two batches of rows
+    auto copy_window = [&](int ph, bool claim, int lo, int hi) {
+        if (claim && tid == 0) {
             if (ph == 0) s_item = (long long)atomicAdd(a.counter, 1u);
             const long long item = s_item;
             if (item < a.total) {
@@ -461,11 +464,12 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d_kgrad(xc2_kg_args A) {
         long long ch, b0;
         item_pos(item, ch, b0);
         const float* base = reinterpret_cast<const float*>(ph == 0 ? a.gy : a.x) + ch * a.stride + 2 * b0;
-        for (int r = tid; r < s_rhi; r += 32) bulk_g2s(win + r * RS, base + 2LL * r * N2, N2 * 8, &full);
+        const int    rhi  = s_rhi < hi ? s_rhi : hi;
+        for (int r = lo + tid; r < rhi; r += 32) bulk_g2s(win + r * RS, base + 2LL * r * N2, N2 * 8, &full);
     };
 
     __syncthreads();
-    if (tid < 32) copy_window(0);
+    if (tid < 32) copy_window(0, true, 0, N1);
     uint32_t phase   = 0;
     bool     aborted = false;
     // step 2's row groups (as k_fxcorr2d): the U groups of a half-warp take
@@ -548,12 +552,17 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d_kgrad(xc2_kg_args A) {
                     constexpr int i = decltype(ic)::value;
                     v[i]            = win[k1 * RS + t2 + i * TT2];
                 });
-                if (rd == F::R2 - 1) {
-                    // the window is read: start the next window's copies (the
-                    // x window of this block, or the next block's gy block)
+                // round rd has read rows [rd*G2, (rd+1)*G2): the next window's
+                // copies into them (the x window of this block, or the next
+                // block's gy block) start now, the rest after the last round
+                if (F::R2 == 1 || rd == 0 || rd == F::R2 - 1) {
                     fence_proxy_async_smem();
                     __syncthreads();
-                    if (tid < 32) copy_window(ph ^ 1);
+                    if (tid < 32) {
+                        const int lo = F::R2 == 1 || rd == 0 ? 0 : F::G2;
+                        const int hi = F::R2 == 1 || rd == F::R2 - 1 ? N1 : F::G2;
+                        copy_window(ph ^ 1, rd == 0, lo, hi);
+                    }
                 }
                 stage_compute_tab<P2, 0>(v, t2, tw2);
                 run_stages_full<P2, typename F::X2, true, -1>(v, xch, g2, t2, tw2);
