@@ -50,6 +50,25 @@ __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_
             : "memory");
     }
 }
+// The same product with A read from tensor memory (a_tmem: its first column;
+// row m of A in lane m, K along the columns, 32 bits per column).
+template<int PREC>
+__device__ __forceinline__ void umma_ta(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    if constexpr (PREC != PREC_TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d),
+            "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d),
+            "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+            : "memory");
+    }
+}
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
@@ -573,10 +592,15 @@ struct tcp_cfg {
     static constexpr int NS    = O::NS;
     static constexpr int OPB   = (int)sizeof(typename O::elem);
     static constexpr int WORK  = TP_PTS + TP_PTS / 8;           // complex, padded
-    static constexpr int ABYTE = TP_NT * 32 * OPB;              // one part of the 256 x 32 operand
     static constexpr int BBYTE = 32 * 32 * OPB;
-    static constexpr int SMEM  = WORK * 8 + NS * ABYTE + NS * BBYTE;
-    static constexpr int MINB  = SMEM <= 74 * 1024 ? 3 : 2;    // CTAs per SM the shared memory allows
+    static constexpr int SMEM  = WORK * 8 + NS * BBYTE;
+    // tensor memory: the two accumulators (columns 0..63), then the operand
+    // rows, one 32-element K row per block and part (ACOLS 32-bit columns)
+    static constexpr int ACOLS = 32 * OPB / 4;
+    static constexpr int USED  = 64 + 2 * NS * ACOLS;
+    static constexpr int TCOLS = USED <= 128 ? 128 : 256;
+    static constexpr int MINB  = TCOLS <= 128 ? 3 : 2;    // CTAs per SM (tensor memory, registers)
+    static_assert(USED <= TCOLS && MINB * TCOLS <= 512, "tensor memory of the resident CTAs");
 };
 
 __device__ __forceinline__ int tcp_wp(int p) { return p + 2 * (p >> 4); }
@@ -585,10 +609,11 @@ __device__ __forceinline__ int tcp_wp(int p) { return p + 2 * (p >> 4); }
 // when the bounded wait for the products gave up (the CTA then leaves).
 template<int LOGN, int PREC>
 __device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float* const* s_src, float* const* s_dst,
-                                        cpx<float>* work, unsigned char* const (&opA)[op_traits<PREC>::NS],
-                                        unsigned char* const (&opB)[op_traits<PREC>::NS], uint32_t taddr,
+                                        cpx<float>* work, unsigned char* const (&opB)[op_traits<PREC>::NS],
+                                        uint32_t taddr,
                                         uint64_t* mbar, uint32_t& phase) {
     using O           = op_traits<PREC>;
+    using C           = tcp_cfg<PREC>;
     using E           = typename O::elem;
     constexpr int NS  = O::NS;
     constexpr int N   = 1 << LOGN;
@@ -598,6 +623,8 @@ __device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float
     const int     tid = threadIdx.x;
     const int     warp = tid / 32;
     const float   cj   = a.conj ? -1.f : 1.f;
+    // this thread's operand row: lane tid % 128 (its warp's quarter), block tid / 128
+    const uint32_t arow = taddr + ((uint32_t)(32 * (warp % 4)) << 16) + 64 + (uint32_t)((warp / 4) * NS * C::ACOLS);
     const auto*   tw   = reinterpret_cast<const cpx<float>*>(a.tw);
     const int  tr = tid / (N / 16), bl = tid % (N / 16);
     // the first tensor-core stage's twiddle factors (W_{16 ns}^(qk), q =
@@ -686,8 +713,8 @@ __device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float
             }
             x[j] = v;
         });
-        // operand row tid: reals 0..15 then imaginaries 16..31, one 16-byte
-        // core-matrix row per store
+        // operand row tid (reals 0..15 then imaginaries 16..31) into this
+        // thread's tensor-memory lane, four columns at a time
         static_for<32 / O::PER_CHUNK>([&](auto cc) {
             constexpr int c = decltype(cc)::value;
             uint32_t      part[NS][4];
@@ -712,30 +739,30 @@ __device__ __forceinline__ bool tcp_run(const tcp_args& a, int rows, const float
             }
             static_for<NS>([&](auto ic) {
                 constexpr int i = decltype(ic)::value;
-                *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, TP_NT>(tid, c * O::PER_CHUNK)) =
-                    make_uint4(part[i][0], part[i][1], part[i][2], part[i][3]);
+                tmem_st4_nowait(arow + (uint32_t)(i * C::ACOLS + 4 * c), part[i][0], part[i][1], part[i][2],
+                                part[i][3]);
             });
         });
-        fence_proxy_async_smem();
+        tmem_wait_st();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
         if (tid == 0) {
-            constexpr uint32_t LBO_A = (TP_NT / 8) * 128, LBO_B = (32 / 8) * 128, SBO = 128;
-            constexpr uint32_t BLK   = (128 / 8) * 128;    // rows 128..255
+            constexpr uint32_t LBO_B = (32 / 8) * 128, SBO = 128;
             constexpr int      KS    = 32 / O::K_PER_MMA;
             constexpr int      CH    = O::K_PER_MMA / O::PER_CHUNK;
+            constexpr uint32_t KCOL  = O::K_PER_MMA * C::OPB / 4;    // A columns per product's K
             using SP                 = split_products<NS>;
             static_for<2>([&](auto bc) {
                 constexpr int blk = decltype(bc)::value;
                 uint32_t      acc = 0;
                 static_for<SP::NP>([&](auto pc) {
                     constexpr int        p  = decltype(pc)::value;
-                    const unsigned char* xa = opA[SP::x(p)] + blk * BLK;
+                    const uint32_t       xa = taddr + 64 + (uint32_t)((blk * NS + SP::x(p)) * C::ACOLS);
                     const unsigned char* ab = opB[SP::a(p)];
                     for (int ks = 0; ks < KS; ++ks) {
-                        umma<PREC>(taddr + 32 * blk, sdesc(xa + ks * CH * LBO_A, LBO_A, SBO),
-                                   sdesc(ab + ks * CH * LBO_B, LBO_B, SBO), O::IDESC, acc);
+                        umma_ta<PREC>(taddr + 32 * blk, xa + ks * KCOL, sdesc(ab + ks * CH * LBO_B, LBO_B, SBO),
+                                      O::IDESC, acc);
                         acc = 1;
                     }
                 });
@@ -803,12 +830,10 @@ __global__ void __launch_bounds__(TP_NT, tcp_cfg<PREC>::MINB) k_tcp(tcp_args a) 
     constexpr int NS = O::NS;
     extern __shared__ __align__(128) unsigned char smem[];
     cpx<float>*    work = reinterpret_cast<cpx<float>*>(smem);
-    unsigned char* opA[NS];
     unsigned char* opBw[NS];
     static_for<NS>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        opA[i]          = smem + C::WORK * 8 + i * C::ABYTE;
-        opBw[i]         = smem + C::WORK * 8 + NS * C::ABYTE + i * C::BBYTE;
+        opBw[i]         = smem + C::WORK * 8 + i * C::BBYTE;
     });
     __shared__ uint64_t     mbar;
     __shared__ uint32_t     tslot;
@@ -817,7 +842,7 @@ __global__ void __launch_bounds__(TP_NT, tcp_cfg<PREC>::MINB) k_tcp(tcp_args a) 
     const int               tid  = threadIdx.x;
     const int               warp = tid / 32;
     if (warp == 0) {
-        tmem_alloc(&tslot, 64);
+        tmem_alloc(&tslot, C::TCOLS);
         tmem_relinquish();
     }
     if (tid == 0) {
@@ -840,6 +865,7 @@ __global__ void __launch_bounds__(TP_NT, tcp_cfg<PREC>::MINB) k_tcp(tcp_args a) 
             *reinterpret_cast<E*>(opBw[i] + op_off<PREC, 32>(n, k)) = part[i];
         });
     }
+    fence_proxy_async_smem();    // B is read by the products (async proxy)
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -869,18 +895,18 @@ __global__ void __launch_bounds__(TP_NT, tcp_cfg<PREC>::MINB) k_tcp(tcp_args a) 
         __syncthreads();
         bool ok = true;
         switch (lg) {
-        case 8: ok = tcp_run<8, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
-        case 9: ok = tcp_run<9, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
-        case 10: ok = tcp_run<10, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
-        case 11: ok = tcp_run<11, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
-        case 12: ok = tcp_run<12, PREC>(a, rows, s_src, s_dst, work, opA, opBw, taddr, &mbar, phase); break;
+        case 8: ok = tcp_run<8, PREC>(a, rows, s_src, s_dst, work, opBw, taddr, &mbar, phase); break;
+        case 9: ok = tcp_run<9, PREC>(a, rows, s_src, s_dst, work, opBw, taddr, &mbar, phase); break;
+        case 10: ok = tcp_run<10, PREC>(a, rows, s_src, s_dst, work, opBw, taddr, &mbar, phase); break;
+        case 11: ok = tcp_run<11, PREC>(a, rows, s_src, s_dst, work, opBw, taddr, &mbar, phase); break;
+        case 12: ok = tcp_run<12, PREC>(a, rows, s_src, s_dst, work, opBw, taddr, &mbar, phase); break;
         default: break;
         }
         if (!ok) break;
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(taddr, 64);
+    if (warp == 0) tmem_dealloc(taddr, C::TCOLS);
 }
 
 }    // namespace tc

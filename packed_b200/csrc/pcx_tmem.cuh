@@ -72,4 +72,13 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// Four columns of this thread's lane from registers, without waiting (a run of
+// such stores ends with tmem_wait_st()).
+__device__ __forceinline__ void tmem_st4_nowait(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(a), "r"(b), "r"(c),
+                 "r"(d)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 }    // namespace pcxg
