@@ -219,7 +219,9 @@ struct tc_args {
 //      j to element k * R + j, the transform's natural order (the output
 //      conjugated and scaled for the inverse).
 // Modes 1 and 2 read and write whole 8-point packs of T >= 8 adjacent columns.
-// Smem plan: work[2][T*N] complex | A_hi | A_lo (128 x 32) | B_hi | B_lo (32 x 32)
+// Smem plan: work[2][T*N] complex | B parts (32 x 32).  Tensor memory: the
+// accumulator (columns 0..31), then the operand rows, one 32-element K row per
+// part (ACOLS 32-bit columns each).
 template<int LOGN, int PREC>
 struct tc_cfg {
     static constexpr int N     = 1 << LOGN;
@@ -228,13 +230,15 @@ struct tc_cfg {
     static constexpr int NTC   = LOGN / 4;                    // radix-16 tensor-core stages
     static constexpr int OPB   = (int)sizeof(typename op_traits<PREC>::elem);
     static constexpr int NS    = op_traits<PREC>::NS;
-    static constexpr int ABYTE = 128 * 32 * OPB;
     static constexpr int BBYTE = 32 * 32 * OPB;
+    static constexpr int ACOLS = 32 * OPB / 4;
+    static constexpr int TCOLS = 32 + NS * ACOLS <= 64 ? 64 : 128;
     // padded work layout (one pad element per 8): faster wherever it keeps
     // three CTAs per SM or there is no remainder stage (measured per form)
     static constexpr bool PAD  = PREC != PREC_TF32 || LOGN % 4 == 0;
     static constexpr int  WORK = T * N + (PAD ? T * N / 8 : 0);    // complex per work buffer
-    static constexpr int  SMEM = 2 * WORK * 8 + NS * ABYTE + NS * BBYTE;
+    static constexpr int  SMEM = 2 * WORK * 8 + NS * BBYTE;
+    static_assert(32 + NS * ACOLS <= TCOLS, "accumulator and operand rows in the allocation");
 };
 
 template<int LOGN, int PREC, int MODE>
@@ -255,12 +259,10 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     cpx<float>* work0 = reinterpret_cast<cpx<float>*>(smem);
     cpx<float>* work1 = work0 + C::WORK;
     constexpr int  NS = C::NS;    // parts of each split operand
-    unsigned char* opA[NS];       // the twiddled inputs X, part by part
-    unsigned char* opB[NS];       // the DFT matrix A
+    unsigned char* opB[NS];       // the DFT matrix A (the twiddled inputs X go to tensor memory)
     static_for<NS>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        opA[i]          = reinterpret_cast<unsigned char*>(work1 + C::WORK) + i * C::ABYTE;
-        opB[i]          = reinterpret_cast<unsigned char*>(work1 + C::WORK) + NS * C::ABYTE + i * C::BBYTE;
+        opB[i]          = reinterpret_cast<unsigned char*>(work1 + C::WORK) + i * C::BBYTE;
     });
     __shared__ uint64_t mbar;
     __shared__ uint32_t tslot;
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     const int       rows = MODE == 1 ? T : (int)min((long long)T, a.batch - row0);
 
     if (warp == 0) {
-        tmem_alloc(&tslot, 32);
+        tmem_alloc(&tslot, C::TCOLS);
         tmem_relinquish();
     }
     if (tid == 0) {
@@ -344,6 +346,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
         w[6] = {r1.z, cj * i1.z};
         w[7] = {r1.w, cj * i1.w};
     }
+    fence_proxy_async_smem();    // B is read by the products (async proxy)
     __syncthreads();
     tc_fence_after();
     const uint32_t taddr = tslot;
@@ -436,27 +439,27 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
                 }
                 static_for<NS>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
-                    *reinterpret_cast<uint4*>(opA[i] + op_off<PREC, 128>(tid, c * O::PER_CHUNK)) =
-                        make_uint4(part[i][0], part[i][1], part[i][2], part[i][3]);
+                    tmem_st4_nowait(taddr + ((uint32_t)(32 * warp) << 16) + 32 + (uint32_t)(i * C::ACOLS + 4 * c),
+                                    part[i][0], part[i][1], part[i][2], part[i][3]);
                 });
             });
-            fence_proxy_async_smem();
+            tmem_wait_st();
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
             if (tid == 0) {
-                constexpr uint32_t LBO_A = (128 / 8) * 128, LBO_B = (32 / 8) * 128, SBO = 128;
+                constexpr uint32_t LBO_B = (32 / 8) * 128, SBO = 128;
                 constexpr int      KS    = 32 / O::K_PER_MMA;               // MMAs per product
                 constexpr int      CH    = O::K_PER_MMA / O::PER_CHUNK;     // chunks per MMA (2)
+                constexpr uint32_t KCOL  = O::K_PER_MMA * C::OPB / 4;       // A columns per product's K
                 using SP                 = split_products<NS>;
                 uint32_t           acc   = 0;
                 static_for<SP::NP>([&](auto pc) {
                     constexpr int        p  = decltype(pc)::value;
-                    const unsigned char* xa = opA[SP::x(p)];
+                    const uint32_t       xa = taddr + 32 + (uint32_t)(SP::x(p) * C::ACOLS);
                     const unsigned char* ab = opB[SP::a(p)];
                     for (int ks = 0; ks < KS; ++ks) {
-                        umma<PREC>(taddr, sdesc(xa + ks * CH * LBO_A, LBO_A, SBO), sdesc(ab + ks * CH * LBO_B, LBO_B, SBO),
-                                   O::IDESC, acc);
+                        umma_ta<PREC>(taddr, xa + ks * KCOL, sdesc(ab + ks * CH * LBO_B, LBO_B, SBO), O::IDESC, acc);
                         acc = 1;
                     }
                 });
@@ -543,7 +546,7 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(taddr, 32);
+    if (warp == 0) tmem_dealloc(taddr, C::TCOLS);
 }
 
 // ---------------------------------------------------------------------------
