@@ -550,17 +550,19 @@ __global__ void __launch_bounds__(NT, 1) k_tcfft(tc_args a) {
 }
 
 // ---------------------------------------------------------------------------
-// Persistent form of mode 0 (N = 2^8..2^12, whole rows): each CTA of 256
-// threads takes items of 4096 points (T = 4096 / N rows) in turn, so the DFT
-// matrix and the TMEM columns are set up once per CTA, not once per row group.
-// A radix-16 stage is one round: every thread builds the operand row of one
-// of the item's 256 butterflies, thread 0 issues two M = 128 products (rows
-// 0..127 and 128..255 into TMEM columns 0..31 and 32..63), and every thread
-// reads its own butterfly's 32 outputs back from its TMEM lane (warps 0-3 the
-// first block, warps 4-7 the second, each in its own lane quarter).  The
-// work buffer is updated in place (all of a stage's reads land in the
-// operands before the first write), so three CTAs fit on an SM in the bfloat16
-// form.  Work element p sits at p + 2*(p/16): the strided reads of the
+// Persistent form for whole rows (N = 2^8..2^12): each CTA of 256 threads
+// takes items of 4096 points (T = 4096 / N rows) in turn, so the DFT matrix
+// and the TMEM columns are set up once per CTA, not once per row group.  A
+// radix-16 stage is one round: every thread builds the operand row of one of
+// the item's 256 butterflies and writes it to its own TMEM lane (warps 0-3 the
+// first block of 128 rows, warps 4-7 the second, each in its own lane
+// quarter), thread 0 issues two M = 128 products with A read from tensor
+// memory (into TMEM columns 0..31 and 32..63), and every thread reads its own
+// butterfly's 32 outputs back from its lane.  The work buffer is updated in
+// place (all of a stage's reads land in the operands before the first write);
+// shared memory holds only it and the DFT matrix, and the CTAs per SM are set
+// by tensor memory and registers (three in the bfloat16 form, two in the
+// others).  Work element p sits at p + 2*(p/16): the strided reads of the
 // operand build, the Stockham writes and the packs of 8 contiguous elements
 // of the row copies are all conflict-free, and the first stage's 16
 // contiguous outputs per thread go out as 16-byte stores.
