@@ -940,8 +940,8 @@ cudaError_t launch_tcp(const tc::tcp_args& a, long long nitems, int sms, cudaStr
     cudaError_t e = smem_attr_cached(reinterpret_cast<const void*>(kern), C::SMEM);
     if (e != cudaSuccess) return e;
     if (nitems <= 0) return cudaSuccess;
-    // C::MINB CTAs per SM (its shared memory and the register bound of
-    // __launch_bounds__); the occupancy query reports one for this kernel
+    // C::MINB CTAs per SM (the tensor memory each allocates and the register
+    // bound of __launch_bounds__); more would wait in tcgen05.alloc
     const long long grid = std::max<long long>(1, std::min<long long>(nitems, (long long)C::MINB * sms));
     kern<<<(unsigned)grid, tc::TP_NT, C::SMEM, st>>>(a);
     return cudaGetLastError();
