@@ -197,7 +197,7 @@ __device__ __forceinline__ uint32_t op_off(int row, int k) {
 struct tc_args {
     const float* src;
     float*       dst;
-    long long    batch;    // rows (mode 0 and 2) or transforms (mode 1)
+    long long    batch;    // rows (mode 2) or transforms (mode 1)
     int          conj;
     float        scale;
     const void*  twN;    // W_N^i
