@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
     __shared__ int       s_rlo;
     __shared__ int       s_rhi;
     __shared__ int       s_abort;
+    __shared__ uint32_t  s_tmem;
     const int            tid  = threadIdx.x;
     const float*         src  = reinterpret_cast<const float*>(a.src);
     float*               dst  = reinterpret_cast<float*>(a.dst);
@@ -121,6 +122,38 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
     if (tid == 0) {
         mbar_init(&full, 1);
         fence_barrier_init();
+    }
+    // step 2's row groups: the U groups of a half-warp take rows S apart, so
+    // their window rows fall in disjoint banks (RS = 2 mod 16)
+    constexpr int S2 = TT2 / 2;
+    constexpr int U2 = 16 / TT2;
+    const int     g2 = tid / TT2, t2 = tid % TT2;
+    const int     r2 = ((g2 / U2) / S2) * 8 + ((g2 / U2) % S2) + (g2 % U2) * S2;
+    // The kernel spectrum values a thread multiplies by are the same for every
+    // block (its rows k1 = rd*G2 + r2, columns k2 = t2 + i*TT2): they are read
+    // once into the thread's tensor-memory lane (otherwise idle in this kernel),
+    // 32 columns per row round, instead of from global memory in every block.
+    constexpr uint32_t TCOLS = 128 * F::R2;    // four warps share each lane quarter
+    static_assert(TCOLS == 128 || TCOLS == 256, "a power-of-two TMEM allocation");
+    if (tid < 32) {
+        tmem_alloc(&s_tmem, TCOLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = s_tmem;
+    const uint32_t tcol  = tbase + ((uint32_t)(32 * ((tid / 32) % 4)) << 16) + (uint32_t)((tid / 128) * 32 * F::R2);
+    for (int rd = 0; rd < F::R2; ++rd) {
+        const int k1 = rd * F::G2 + r2;
+        uint32_t  kr[32];
+        static_for<E>([&](auto ic) {
+            constexpr int    i = decltype(ic)::value;
+            const cpx<float> k = ldg_cpx(kp + k1 * N2 + t2 + i * TT2);
+            kr[2 * i]          = __float_as_uint(k.re);
+            kr[2 * i + 1]      = __float_as_uint(k.im);
+        });
+        tmem_st32(tcol + 32 * rd, kr);
     }
 
     // channel and window start (samples) of an item
@@ -191,7 +224,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 mbar_wait_bounded(&full, phase, 100000000ull);
             }
             __syncthreads();
-            return;
+            break;    // every thread leaves the loop together; TMEM is freed below
         }
         phase ^= 1;
         if (a.inplace && tid == 0) {
@@ -245,15 +278,9 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
         }
         // ---------------- step 2: rows; spectrum times conj(K) or K; inverse rows
         {
-            // the U groups of a half-warp take rows S apart, so their window
-            // rows fall in disjoint banks (RS = 2 mod 16)
-            constexpr int S  = TT2 / 2;
-            constexpr int U  = 16 / TT2;
-            const int     g  = tid / TT2, t = tid % TT2;
-            const int     bb = g / U, u = g % U;
-            const int     r0 = (bb / S) * 8 + (bb % S) + u * S;
+            const int g = g2, t = t2;
             for (int rd = 0; rd < F::R2; ++rd) {
-                const int  k1 = rd * F::G2 + r0;
+                const int  k1 = rd * F::G2 + r2;
                 cpx<float> v[E];
                 static_for<E>([&](auto ic) {
                     constexpr int i = decltype(ic)::value;
@@ -261,12 +288,18 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 });
                 stage_compute_tab<P2, 0>(v, t, tw2);
                 run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
-                // v[i] = X[k1 + N1*k2], k2 = t + i*TT2: conj(X * conj(K)) or conj(X * K)
-                static_for<E>([&](auto ic) {
-                    constexpr int    i = decltype(ic)::value;
-                    const cpx<float> k = ldg_cpx(kp + k1 * N2 + t + i * TT2);
-                    const cpx<float> c = {v[i].re, -v[i].im};
-                    v[i]               = a.conj_kernel ? cmul(c, k) : cmulc(c, k);
+                // v[i] = X[k1 + N1*k2], k2 = t + i*TT2: conj(X * conj(K)) or conj(X * K),
+                // K from tensor memory eight values at a time
+                static_for<2>([&](auto hc) {
+                    constexpr int h = decltype(hc)::value;
+                    uint32_t      kq[16];
+                    tmem_ld16(tcol + 32 * rd + 16 * h, kq);
+                    static_for<8>([&](auto jc) {
+                        constexpr int    i = 8 * h + decltype(jc)::value;
+                        const cpx<float> k = {__uint_as_float(kq[2 * (i - 8 * h)]), __uint_as_float(kq[2 * (i - 8 * h) + 1])};
+                        const cpx<float> c = {v[i].re, -v[i].im};
+                        v[i]               = a.conj_kernel ? cmul(c, k) : cmulc(c, k);
+                    });
                 });
                 stage_compute_tab<P2, 0>(v, t, tw2);
                 run_stages_full<P2, typename F::X2, true, -1>(v, xch, g, t, tw2);
@@ -309,7 +342,7 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
                 }
             }
             __syncthreads();
-            if (s_abort) return;    // every thread leaves together; no copy is in flight
+            if (s_abort) break;    // every thread leaves together; no copy is in flight
         }
         {
             const int       g    = tid / TT1, t = tid % TT1;
@@ -349,6 +382,9 @@ __global__ void __launch_bounds__(512, 1) k_fxcorr2d(xc2_args A) {
             }
         }
     }
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) tmem_dealloc(tbase, TCOLS);
 }
 
 // ---------------------------------------------------------------------------
